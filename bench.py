@@ -1,0 +1,303 @@
+#!/usr/bin/env python
+"""Throughput of the hotspin hot path on B200: two-temperature model + LLB at 512x512x4.
+
+Workload (the configuration the headline metric is quoted on): 512 x 512 x 4 cells of
+4 nm, demag padded to 1024 x 1024 x 8, Ms0 = 8e5 A/m, A = 1.3e-11 J/m, lambda = 0.02,
+Tc = 630 K, J = 1/2, Philox thermal field (seed 3), electrons Ce = 700 Te J/m^3K, lattice
+Cl = 3e6 J/m^3K, G = 6e17 W/m^3K, ke = 90 W/mK, Gaussian laser 100 fs FWHM, 5e20 W/m^3,
+sigma = 400 nm, T0 = 300 K, adaptive Dormand-Prince 4(5) at rtol 1e-5.  One "step" is one
+accepted DP45 step of the whole grid; value = cells x accepted steps / device time
+(Mcell-steps/s), summed over ranks (independent replicas: the path does not shard).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s (TTM+LLB, DP45 rtol 1e-5) at 512x512x4"
+UNIT = "Mcell-steps/s"
+MU0 = 4e-7 * math.pi
+MUB = 9.27400968202020202e-24
+
+
+def workload():
+    """Program order: (N0, N1, N2) = (z, y, x)."""
+    ms = 8e5
+    lex = math.sqrt(2 * 1.3e-11 / (MU0 * ms * ms))
+    return dict(size=(4, 512, 512), cellsize=(4e-9, 4e-9, 4e-9), msat0T0=ms, lex=lex,
+                gamma_ll=2.211e5 / (1 + 0.02 ** 2), alpha=(0.02, 0.02, 0.02), b_ext=(0.0, 0.0, 0.02),
+                demag=True, llb=True, tc=630.0, spin_j=0.5, n_spins=ms / (2 * MUB * 0.5), temperature=300.0,
+                thermal=True, seed=3, ttm=True, gamma_e=700.0, c_l=3e6, g_ep=6e17, k_e=90.0, k_l=0.0,
+                laser_p0=5e20, laser_t0=2.5e-13, laser_fwhm=1e-13, laser_sigma=400e-9)
+
+
+def initial_state(kw):
+    """m = m_e(300 K) along user x with a seeded 5 degree random tilt; Te = Tl = 300 K."""
+    import ctypes
+    from hotspin_b200 import _lib
+    size = kw["size"]
+    me_c = ctypes.c_double()
+    _lib.check(_lib.load().hsb_mfa_equilibrium(300.0, kw["tc"], kw["spin_j"], ctypes.byref(me_c)), "m_e")
+    me = me_c.value
+    rng = np.random.default_rng(3)
+    th = np.deg2rad(5.0) * rng.random(size)
+    ph = 2 * np.pi * rng.random(size)
+    m = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)])  # around program Z
+    return {"m": me * m, "Te": np.full(size, 300.0), "Tl": np.full(size, 300.0)}
+
+
+def algorithmic_bytes(kw, fused=True):
+    """Unique bytes each kernel family must move per launch (inputs once, outputs once)."""
+    n0, n1, n2 = kw["size"]
+    ncell = n0 * n1 * n2
+    L0, L1, L2 = [2 * s if s > 1 else s for s in kw["size"]]
+    c2 = L2 // 2 + 1
+    spec = 3 * n0 * c2 * n1 * 8                  # X1: complex FP32 after the x pass
+    kern = c2 * (L1 // 2 + 1) * (L0 // 2 + 1) * 6 * 4
+    nch = 5 if kw.get("ttm") else 3
+    # DP45 attempt with a thermal field: stage 1 + stages 2..6 + stage 7
+    stage = 0
+    stage += ncell * (nch * 4 + 12 + nch * 4 + nch * 4)               # s1: ys, hd, write k1, y2
+    for s in range(2, 7):
+        stage += ncell * (nch * 4 + 12 + nch * 4 + nch * 4 * (s - 1) + nch * 4 + nch * 4)
+    stage += ncell * (nch * 4 + 12 + nch * 4 + nch * 4 * 6 + nch * 4)  # s7: ys, hd, y0(T), k1..k6, k7
+    return {"xfwd": ncell * 12 + spec, "yz": 2 * spec + kern, "xinv": spec + ncell * 12,
+            "stage_attempt": stage, "stage_launches": 7, "demag_per_attempt": 6}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                out, _ = self.p.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(kw, state):
+    """The FP64 oracle (NumPy, all host cores through numpy's own threading) timed on one
+    DP45 step of the same workload."""
+    from oracle.model import Model, Spec
+    from oracle.solvers import Integrator
+    spec = Spec(**kw)
+    model = Model(spec)
+    it = Integrator(model, state, "dp45", 2e-16, rtol=1e-5, mindt=1e-20, maxdt=1e-13)
+    t0 = time.perf_counter()
+    it.step()
+    dtw = time.perf_counter() - t0
+    ncell = int(np.prod(kw["size"]))
+    return {"value": ncell * it.step_count / dtw / 1e6, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": "1 accepted DP45 step (%d RHS evaluations) of the 512x512x4 workload by the FP64 "
+                      "NumPy oracle, %.1f s" % (7 * (1 + it.bad_steps), dtw)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ours(args):
+    import torch
+    from hotspin_b200 import _lib
+    from hotspin_b200.sim import Simulation
+    world, rank, local, pg = dist_setup()
+    kw = workload()
+    ncell = int(np.prod(kw["size"]))
+    st0 = initial_state(kw)
+    sim = Simulation(**kw, solver="dp45", dt=2e-16, rtol=1e-5, mindt=1e-20, maxdt=1e-13)
+    for k, v in st0.items():
+        sim.set(k, v)
+    stream = torch.cuda.ExternalStream(sim._lib.hsb_sim_stream(sim._h))
+    sim.step(args.warmup)
+    s0 = sim.status()
+    barrier(pg)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        sim.step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(pg)
+    ms = max_over_ranks(pg, e0.elapsed_time(e1))
+    s1 = sim.status()
+    attempts = s1["attempts"] - s0["attempts"]
+    nl = ctypes_int()
+    _lib.check(sim._lib.hsb_sim_launches_per_attempt(sim._h, nl), "launches")
+    launches = attempts * nl.value
+    value = world * ncell * args.steps / (ms / 1e3) / 1e6
+    # ---- live per-kernel timing of one attempt (eager launches between CUDA events)
+    prof = (ctypes_double * 7)()
+    _lib.check(sim._lib.hsb_sim_profile(sim._h, 3, prof), "profile")
+    cats = {"stage": prof[0], "xfwd": prof[1], "yz": prof[2], "xinv": prof[3], "other": prof[4]}
+    ab = algorithmic_bytes(kw)
+    per_launch = {"stage": (ab["stage_attempt"], prof[0], ab["stage_launches"]),
+                  "yz": (ab["yz"] * ab["demag_per_attempt"], prof[2], ab["demag_per_attempt"]),
+                  "xfwd": (ab["xfwd"] * ab["demag_per_attempt"], prof[1], ab["demag_per_attempt"]),
+                  "xinv": (ab["xinv"] * ab["demag_per_attempt"], prof[3], ab["demag_per_attempt"])}
+    dom = max(per_launch, key=lambda k: per_launch[k][1])
+    byt, tms, nlaunch = per_launch[dom]
+    peak, kind = peaks()
+    achieved = (byt / nlaunch) / ((tms / nlaunch) / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(dom)
+    names = {"stage": "k_stage<5> (fused RHS + DP45 stage)", "yz": "k_fft_yz_conv<8> (y/z FFT + tensor multiply)",
+             "xfwd": "k_fft_x_fwd<float> (R2C + transpose)", "xinv": "k_fft_x_inv (C2R)"}
+    roof = {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1), "peak": peak,
+            "peak_kind": kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+            "algorithmic_bytes_per_launch": int(byt / nlaunch),
+            "avg_launch_ms": round(tms / nlaunch, 5),
+            "attempt_ms_by_family": {k: round(v, 4) for k, v in cats.items()}}
+    # ---- end to end through the C-ABI with host buffers
+    host_state = {k: np.ascontiguousarray(v) for k, v in st0.items()}
+    barrier(pg)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k, v in host_state.items():
+        sim.set(k, v)
+    per_step_d2h = 0
+    for _ in range(args.steps):
+        sim.step(1)
+        st = sim.status()          # the step's result read back: t, dt, steps, err, status
+        per_step_d2h += 8 * 7
+    mout = sim.get("m")
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(pg, time.perf_counter() - t0)
+    h2d = sum(v.nbytes for v in host_state.values())
+    d2h = mout.nbytes + per_step_d2h
+    e2e = {"value": round(world * ncell * args.steps / e2e_s / 1e6, 3), "unit": UNIT,
+           "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+           "note": "per run: FP64 host state uploaded, K steps each followed by a status read, m downloaded"}
+    out = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "TTM+LLB 512x512x4 (demag 1024x1024x8), DP45 rtol 1e-5, thermal field",
+                      "cells": ncell, "parallelism": "replicas" if world > 1 else "single",
+                      "l2": "working set %d MB > 126 MB L2" % int((ncell * 4 * (5 * 13 + 12) + 3 * 4 * 513 * 512 * 8
+                                                                     + 31.6e6) / 1e6),
+                      "attempts": attempts, "rejected": s1["rejects"] - s0["rejects"],
+                      "sim_time_ps": round(s1["t"] * 1e12, 4)},
+           "roofline": roof, "gpu_launches": int(launches), "e2e": e2e, "clocks": clk.summary()}
+    sim.close()
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(kw, st0)
+        print(json.dumps(out))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def ctypes_int():
+    import ctypes
+    return ctypes.c_int()
+
+
+ctypes_double = __import__("ctypes").c_double
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        from oracle.replay import bench_reference
+        bench_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,664 @@
+// Zero-padded FFT demagnetising convolution for sm_100a (hand-written FFTs, no cuFFT).
+//
+// Replaces hotspin's MaxwellPlan (src/hotspin-core/modules/maxwell_convolution.go:103-131):
+// memset + copyPad3D + cuFFT D2Z per component, tensSYMMVecMul, cuFFT Z2D + copyUnPad3D
+// per component (gpu/fftplanX.go:76-104, copypad.cu, mul.cu:31-90).
+//
+// Axes: program order a0 (slowest, user z), a1 (user y), a2 (fastest, user x); logic size
+// L = 2N for open non-unit axes, N otherwise (engine/zeropad.go:12-22).  The real-to-complex
+// axis is a2, packed as a length L2/2 complex FFT; C2 = L2/2 + 1 frequencies are kept.
+//
+// Forward path (FP32):
+//   x-pass   m (SoA, [c][a0][a1][a2]) * msat mask -> X1[c][a0<N0][kx<C2][a1<N1]   (transposed)
+//   yz-pass  per kx column: y FFT (N1 -> L1), z FFT (N0 -> L0), symmetric tensor multiply,
+//            inverse z (keep a0 < N0), inverse y (keep a1 < N1)        X1 -> X1 (in place)
+//            (fused in one kernel when the column fits in shared memory, else three
+//             kernels y / z-multiply / y-inverse through X2[c][a0<N0][kx][L1])
+//   inv x    X1 -> H[c][a0][a1][a2<N2] * Ms0  (A/m; B = mu0 * H)
+// Zero padding is never materialised: the transforms skip the known-zero inputs and
+// outputs outside the data block are never stored.
+//
+// Kernel (FP64): Kernel_Arne (kernel_magnetostatic.go:25-241) evaluated on the GPU, one
+// thread per (wrapped target cell in the folded octant, source axis), images summed in
+// the reference's loop order; each component is transformed with the same FFT code in
+// FP64, the real part of the folded octant kept and scaled by 1/(L0 L1 L2)
+// (maxwell_convolution.go:135-223, 350-388), stored FP32 as kern[kx][k1f][k0f][6].
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+
+#include "hsb_common.cuh"
+#include "hsb_demag.h"
+#include "hsb_fft.cuh"
+
+
+static bool is_pow2(int n) { return n >= 1 && (n & (n - 1)) == 0; }
+
+// ------------------------------------------------------------------------------ x pass
+// Forward R2C along a2 for rows of `planes` x N1 rows.  Row (p, y) of the input starts at
+// in + p * in_pstride + y * N2 (in_pstride = N1 * N2 for plain layouts).  For FP32 input the
+// optional mask multiplies every value.  Output X[(p * C2 + kx) * ldo + y], ldo >= N1.
+template <typename Real>
+__global__ void k_fft_x_fwd(const Real* __restrict__ in0, const Real* __restrict__ in1, const int* __restrict__ isel,
+                            int iinv, const float* __restrict__ mask,
+                            long in_cstride, int ncomp_planes_per_comp,
+                            int N1, int N2, int L2, int ldo,
+                            typename cplx_t<Real>::T* __restrict__ out,
+                            const typename cplx_t<Real>::T* __restrict__ tw, int twL, int TY, const int* __restrict__ active) {
+    if (active && !*active) return;
+    typedef typename cplx_t<Real>::T C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    const int M = L2 / 2;
+    const int bs = fpad_len(M);
+    C* scr = buf + TY * bs;
+    const Real* in = (isel && ((*isel) ^ iinv)) ? in1 : in0;
+    const int C2 = M + 1;
+    const int p = blockIdx.y;                 // plane = comp * N0 + a0
+    const int y0 = blockIdx.x * TY;
+    const int ny = min(TY, N1 - y0);
+    const int comp = p / ncomp_planes_per_comp;
+    const int a0 = p - comp * ncomp_planes_per_comp;
+    const Real* src = in + comp * in_cstride + ((long)a0 * N1 + y0) * N2;
+    const float* msk = mask ? mask + ((long)a0 * N1 + y0) * N2 : nullptr;
+    const int tid = threadIdx.x;
+    const int nthr = blockDim.x;
+    // load packed z[n] = x[2n] + i x[2n+1], zero beyond N2
+    for (int e = tid; e < TY * M; e += nthr) {
+        const int r = e / M;
+        const int n = e - r * M;
+        Real a = 0, b = 0;
+        if (r < ny) {
+            const int i0 = 2 * n, i1 = 2 * n + 1;
+            if (i0 < N2) { a = src[(long)r * N2 + i0]; if (msk) a *= (Real)msk[(long)r * N2 + i0]; }
+            if (i1 < N2) { b = src[(long)r * N2 + i1]; if (msk) b *= (Real)msk[(long)r * N2 + i1]; }
+        }
+        buf[r * bs + fpad(n)] = mkc(a, b);
+    }
+    buf = block_fft<-1>(buf, scr, M, TY, bs, tw, twL);
+    // post-process: X[k] = E[k] + W^k O[k]; write transposed, y fastest
+    const int tstep = twL / L2;
+    for (int e = tid; e < C2 * TY; e += nthr) {
+        const int k = e / TY;
+        const int r = e - k * TY;
+        if (r >= ny) continue;
+        const C* z = buf + r * bs;
+        const C zk = z[fpad(k == M ? 0 : k)];
+        const C zc = cconj(z[fpad(k == 0 ? 0 : M - k)]);
+        const C ev = mkc((Real)0.5 * (zk.x + zc.x), (Real)0.5 * (zk.y + zc.y));
+        // O = (zk - zc) / (2i) = (-i/2)(zk - zc)
+        const C df = csub(zk, zc);
+        const C od = mkc((Real)0.5 * df.y, (Real)-0.5 * df.x);
+        const C w = tw[k * tstep];
+        const C xk = cadd(ev, cmul(w, od));
+        out[((long)p * C2 + k) * ldo + y0 + r] = xk;
+    }
+}
+
+// Inverse C2R along a2 with transposed input X[(p * C2 + kx) * ldi + y]; writes the first
+// N2 reals of each row, times `scale`, to out + comp * out_cstride + (a0 * N1 + y) * N2.
+__global__ void k_fft_x_inv(const float2* __restrict__ in, int ldi, int planes_per_comp, int N1,
+                            int N2, int L2, float* __restrict__ out0, float* __restrict__ out1,
+                            const int* __restrict__ osel, int oinv, long out_cstride, float scale,
+                            const float2* __restrict__ tw, int twL, int TY, const int* __restrict__ active) {
+    if (active && !*active) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* buf = reinterpret_cast<float2*>(smem_raw);
+    const int M = L2 / 2;
+    const int bs = fpad_len(M);
+    float2* scr = buf + TY * bs;
+    const int C2 = M + 1;
+    const int p = blockIdx.y;
+    const int y0 = blockIdx.x * TY;
+    const int ny = min(TY, N1 - y0);
+    const int comp = p / planes_per_comp;
+    const int a0 = p - comp * planes_per_comp;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int tstep = twL / L2;
+    // stage X[k] for k < M into smem rows as Z[k] = (X[k] + conj(X[M-k])) + i W^-k (X[k] - conj(X[M-k]))
+    for (int e = tid; e < M * TY; e += nthr) {
+        const int k = e / TY;
+        const int r = e - k * TY;
+        float2 zk = make_float2(0.f, 0.f);
+        if (r < ny) {
+            const float2 xk = in[((long)p * C2 + k) * ldi + y0 + r];
+            const float2 xc = cconj(in[((long)p * C2 + (M - k)) * ldi + y0 + r]);
+            const float2 s = cadd(xk, xc);
+            const float2 d = csub(xk, xc);
+            const float2 w = cconj(tw[k * tstep]);
+            const float2 wd = cmul(w, d);
+            zk = make_float2(s.x - wd.y, s.y + wd.x);  // s + i * wd
+        }
+        buf[r * bs + fpad(k)] = zk;
+    }
+    buf = block_fft<+1>(buf, scr, M, TY, bs, tw, twL);
+    float* out = (osel && ((*osel) ^ oinv)) ? out1 : out0;
+    float* dst = out + comp * out_cstride + ((long)a0 * N1 + y0) * N2;
+    for (int e = tid; e < TY * N2; e += nthr) {
+        const int r = e / N2;
+        const int x = e - r * N2;
+        if (r >= ny) continue;
+        const float2 z = buf[r * bs + fpad(x >> 1)];
+        dst[(long)r * N2 + x] = scale * ((x & 1) ? z.y : z.x);
+    }
+}
+
+// ------------------------------------------------------------------------------ y pass
+// Columns col = 0..ncol-1, column c holds `nin` values at in + c * ldi (zero-padded to L)
+// and `nout` values are stored at out + c * ldo.  May run in place when ldi == ldo.
+template <typename Real, int DIR>
+__global__ void k_fft_cols(const typename cplx_t<Real>::T* in, int ldi, int nin,
+                           typename cplx_t<Real>::T* out, int ldo, int nout, int L, long ncol,
+                           const typename cplx_t<Real>::T* __restrict__ tw, int twL, int TB, const int* __restrict__ active) {
+    if (active && !*active) return;
+    typedef typename cplx_t<Real>::T C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    const int bs = fpad_len(L);
+    C* scr = buf + TB * bs;
+    const long c0 = (long)blockIdx.x * TB;
+    const int nb = (int)min((long)TB, ncol - c0);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    for (int e = tid; e < TB * L; e += nthr) {
+        const int b = e / L;
+        const int n = e - b * L;
+        C v = mkc((Real)0, (Real)0);
+        if (b < nb && n < nin) v = in[(c0 + b) * (long)ldi + n];
+        buf[b * bs + fpad(n)] = v;
+    }
+    buf = block_fft<DIR>(buf, scr, L, TB, bs, tw, twL);
+    for (int e = tid; e < TB * nout; e += nthr) {
+        const int b = e / nout;
+        const int n = e - b * nout;
+        if (b < nb) out[(c0 + b) * (long)ldo + n] = buf[b * bs + fpad(n)];
+    }
+}
+
+// ------------------------------------------------------------------------------ z pass
+// Data X[((c * Nz + a0) * C2 + kx) * L1 + k1] for c < ncomp, a0 < Nz.  Block = (kx, tile of
+// TK consecutive k1).  Forward z transform of the Nz stored rows (zero-padded to L0);
+// with `conv`, the symmetric tensor multiply and the inverse transform follow and the
+// first Nz rows are stored back.  Without `conv` (kernel setup) all L0 rows are stored
+// (then Nz must equal L0).
+template <typename Real>
+__global__ void k_fft_z(typename cplx_t<Real>::T* X, int ncomp, int Nz, int L0, int C2, int L1,
+                        const float* __restrict__ kern, int conv,
+                        const typename cplx_t<Real>::T* __restrict__ tw, int twL, int TK, const int* __restrict__ active) {
+    if (active && !*active) return;
+    typedef typename cplx_t<Real>::T C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    const int bs = fpad_len(L0);
+    C* scr = buf + ncomp * TK * bs;
+    const int kx = blockIdx.y;
+    const int k10 = blockIdx.x * TK;
+    const int nk = min(TK, L1 - k10);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int nbatch = ncomp * TK;  // batch index = c * TK + t
+    for (int e = tid; e < ncomp * L0 * TK; e += nthr) {
+        const int t = e % TK;
+        const int rest = e / TK;
+        const int a0 = rest % L0;
+        const int c = rest / L0;
+        C v = mkc((Real)0, (Real)0);
+        if (t < nk && a0 < Nz) v = X[(((long)c * Nz + a0) * C2 + kx) * L1 + k10 + t];
+        buf[(c * TK + t) * bs + fpad(a0)] = v;
+    }
+    buf = block_fft<-1>(buf, scr, L0, nbatch, bs, tw, twL);
+    scr = (buf == reinterpret_cast<C*>(smem_raw)) ? buf + ncomp * TK * bs : reinterpret_cast<C*>(smem_raw);
+    if (conv) {
+        const int h0 = L0 / 2, h1 = L1 / 2;
+        for (int e = tid; e < L0 * TK; e += nthr) {
+            const int t = e % TK;
+            const int k0 = e / TK;
+            if (t >= nk) continue;
+            const int k1 = k10 + t;
+            const int f0 = k0 > h0 ? L0 - k0 : k0;
+            const int f1 = k1 > h1 ? L1 - k1 : k1;
+            const Real s0 = k0 > h0 ? (Real)-1 : (Real)1;
+            const Real s1 = k1 > h1 ? (Real)-1 : (Real)1;
+            const float* K = kern + (((long)kx * (h1 + 1) + f1) * (h0 + 1) + f0) * 6;
+            const Real kxx = K[KXX], kyy = K[KYY], kzz = K[KZZ];
+            const Real kyz = s1 * K[KYZ], kxz = s0 * K[KXZ], kxy = s0 * s1 * K[KXY];
+            C* p0 = &buf[(0 * TK + t) * bs + fpad(k0)];
+            C* p1 = &buf[(1 * TK + t) * bs + fpad(k0)];
+            C* p2 = &buf[(2 * TK + t) * bs + fpad(k0)];
+            const C m0 = *p0, m1 = *p1, m2 = *p2;
+            *p0 = mkc(kxx * m0.x + kxy * m1.x + kxz * m2.x, kxx * m0.y + kxy * m1.y + kxz * m2.y);
+            *p1 = mkc(kxy * m0.x + kyy * m1.x + kyz * m2.x, kxy * m0.y + kyy * m1.y + kyz * m2.y);
+            *p2 = mkc(kxz * m0.x + kyz * m1.x + kzz * m2.x, kxz * m0.y + kyz * m1.y + kzz * m2.y);
+        }
+        buf = block_fft<+1>(buf, scr, L0, nbatch, bs, tw, twL);
+    }
+    const int nstore = conv ? Nz : L0;
+    for (int e = tid; e < ncomp * nstore * TK; e += nthr) {
+        const int t = e % TK;
+        const int rest = e / TK;
+        const int a0 = rest % nstore;
+        const int c = rest / nstore;
+        if (t < nk) X[(((long)c * Nz + a0) * C2 + kx) * L1 + k10 + t] = buf[(c * TK + t) * bs + fpad(a0)];
+    }
+}
+
+// ------------------------------------------------------------------------------ fused y/z
+// One block per kx column.  X1[((c * N0 + a0) * C2 + kx) * N1 + a1].  Shared memory holds
+// the 3*N0 y-columns of length L1; the z transform (length L0 = LZ <= 16) runs in
+// registers, one thread per k1.
+// Threads per block of the fused kernel: the per-thread z transform holds 3 x LZ complex
+// values, so long z axes trade threads for registers.
+template <int LZ> struct yz_threads { static const int value = LZ >= 16 ? 256 : (LZ >= 8 ? 512 : 1024); };
+
+template <int LZ>
+__global__ void __launch_bounds__(yz_threads<LZ>::value) k_fft_yz_conv(float2* __restrict__ X1, int N0, int N1, int L1, int C2,
+                                                     const float* __restrict__ kern,
+                                                     const float2* __restrict__ tw, int twL, const int* __restrict__ active) {
+    if (active && !*active) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* buf = reinterpret_cast<float2*>(smem_raw);
+    const int bs = fpad_len(L1);
+    const int kx = blockIdx.x;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int ncol = 3 * N0;
+    float2* scr = buf + ncol * bs;
+    // load columns (N1 values each, zero-padded to L1)
+    for (int e = tid; e < ncol * L1; e += nthr) {
+        const int col = e / L1;
+        const int n = e - col * L1;
+        float2 v = make_float2(0.f, 0.f);
+        if (n < N1) v = X1[((long)col * C2 + kx) * N1 + n];
+        buf[col * bs + fpad(n)] = v;
+    }
+    buf = block_fft<-1>(buf, scr, L1, ncol, bs, tw, twL);
+    scr = (buf == reinterpret_cast<float2*>(smem_raw)) ? buf + ncol * bs : reinterpret_cast<float2*>(smem_raw);
+    const int h0 = LZ / 2, h1 = L1 / 2;
+    const int ztstep = twL / LZ;
+    (void)ztstep;
+    for (int k1 = tid; k1 < L1; k1 += nthr) {
+        float2 v[3][LZ];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int z = 0; z < LZ; z++)
+                v[c][z] = (z < N0) ? buf[(c * N0 + z) * bs + fpad(k1)] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int c = 0; c < 3; c++) fft_regp<LZ, -1>(v[c]);
+        const int f1 = k1 > h1 ? L1 - k1 : k1;
+        const float s1 = k1 > h1 ? -1.f : 1.f;
+        const float* Kb = kern + ((long)kx * (h1 + 1) + f1) * (h0 + 1) * 6;
+#pragma unroll
+        for (int k0 = 0; k0 < LZ; k0++) {
+            const int f0 = k0 > h0 ? LZ - k0 : k0;
+            const float s0 = k0 > h0 ? -1.f : 1.f;
+            const float* K = Kb + f0 * 6;
+            const float kxx = K[KXX], kyy = K[KYY], kzz = K[KZZ];
+            const float kyz = s1 * K[KYZ], kxz = s0 * K[KXZ], kxy = s0 * s1 * K[KXY];
+            const float2 m0 = v[0][k0], m1 = v[1][k0], m2 = v[2][k0];
+            v[0][k0] = make_float2(kxx * m0.x + kxy * m1.x + kxz * m2.x, kxx * m0.y + kxy * m1.y + kxz * m2.y);
+            v[1][k0] = make_float2(kxy * m0.x + kyy * m1.x + kyz * m2.x, kxy * m0.y + kyy * m1.y + kyz * m2.y);
+            v[2][k0] = make_float2(kxz * m0.x + kyz * m1.x + kzz * m2.x, kxz * m0.y + kyz * m1.y + kzz * m2.y);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) fft_regp<LZ, +1>(v[c]);
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int z = 0; z < LZ; z++)
+                if (z < N0) buf[(c * N0 + z) * bs + fpad(k1)] = v[c][z];
+    }
+    buf = block_fft<+1>(buf, scr, L1, ncol, bs, tw, twL);
+    for (int e = tid; e < ncol * N1; e += nthr) {
+        const int col = e / N1;
+        const int n = e - col * N1;
+        X1[((long)col * C2 + kx) * N1 + n] = buf[col * bs + fpad(n)];
+    }
+}
+
+// ------------------------------------------------------------------------------ extract
+// Real part of the folded octant of one transformed component, scaled, into kern.
+__global__ void k_extract(const double2* __restrict__ X, int L0, int C2, int L1, int comp,
+                          double scale, float* __restrict__ kern, double* __restrict__ maximag) {
+    const int h0 = L0 / 2, h1 = L1 / 2;
+    const long tot = (long)C2 * (h1 + 1) * (h0 + 1);
+    double mi = 0;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < tot; q += (long)gridDim.x * blockDim.x) {
+        const int f0 = (int)(q % (h0 + 1));
+        const int f1 = (int)((q / (h0 + 1)) % (h1 + 1));
+        const int kx = (int)(q / ((long)(h0 + 1) * (h1 + 1)));
+        const double2 v = X[((long)f0 * C2 + kx) * L1 + f1];
+        kern[q * 6 + comp] = (float)(v.x * scale);
+        mi = fmax(mi, fabs(v.y * scale));
+    }
+    mi = warp_max_d(mi);
+    if ((threadIdx.x & 31) == 0 && mi > 0) {
+        unsigned long long* a = (unsigned long long*)maximag;
+        atomicMax(a, __double_as_longlong(mi));  // positive doubles order like integers
+    }
+}
+
+// ------------------------------------------------------------------------------ host plan
+struct hsb_demag_plan_s {
+    int N[3], L[3], pbc[3];
+    double cs[3];
+    int C2, twL;
+    int fused;          // 1 = single yz kernel
+    int lz;             // compile-time z length for the fused kernel
+    float* kern;        // [C2][L1/2+1][L0/2+1][6]
+    float2* X1;         // [3][N0][C2][N1]
+    float2* X2;         // multipass: [3][N0][C2][L1]
+    float2* tw;
+    double kern_max_imag;
+    double kern_max_real;
+    int smem_x, smem_xi, smem_yz, smem_y, smem_z;
+    int TYx, TYxi, TBy, TKz;
+};
+
+// Largest power-of-two tile (<= cap) whose ping-pong buffers of `per_item` padded complex
+// elements of `esize` bytes fit in `budget` bytes of shared memory.
+static int pick_tile(int per_item, int esize, int budget, int cap) {
+    long per = 2L * fpad_len(per_item) * esize;
+    long t = budget / (per > 0 ? per : 1);
+    if (t > cap) t = cap;
+    if (t < 1) t = 1;
+    int p = 1;
+    while (p * 2 <= t) p *= 2;
+    return p;
+}
+
+template <typename C>
+static int make_twiddles(int twL, C** out) {
+    std::vector<C> h(twL);
+    for (int i = 0; i < twL; i++) {
+        double a = -2.0 * M_PI * (double)i / (double)twL;
+        h[i].x = cos(a);
+        h[i].y = sin(a);
+    }
+    HSB_CUDA_TRY(cudaMalloc((void**)out, sizeof(C) * twL));
+    HSB_CUDA_TRY(cudaMemcpy(*out, h.data(), sizeof(C) * twL, cudaMemcpyHostToDevice));
+    return HSB_OK;
+}
+
+static const int XTHREADS = 256;
+static const int SMEM_TILE_BUDGET = 72 * 1024;
+
+// FP64 transform of the kernel and extraction (setup only).
+static int build_kernel_spectrum(hsb_demag_plan_s* P, int accuracy, cudaStream_t st) {
+    const int L0 = P->L[0], L1 = P->L[1], L2 = P->L[2];
+    const int h0 = L0 / 2, h1 = L1 / 2, h2 = L2 / 2;
+    const int C2 = P->C2;
+    ArneGeom g;
+    for (int a = 0; a < 3; a++) {
+        g.size[a] = P->L[a];
+        g.cs[a] = P->cs[a];
+        g.h[a] = P->L[a] / 2;
+        if (P->pbc[a] == 0) {
+            g.r1[a] = -(long)((P->L[a] - 1) / 2);
+            g.r2[a] = (long)((P->L[a] - 1) / 2);
+        } else {
+            g.r1[a] = -((long)P->L[a] * P->pbc[a] - 1);
+            g.r2[a] = (long)P->L[a] * P->pbc[a] - 1;
+        }
+    }
+    if (P->L[2] == 1 && P->pbc[2] == 0) g.r2[2] = 0;
+    g.Lmin = fmin(P->cs[0], fmin(P->cs[1], P->cs[2]));
+    g.accuracy = (double)accuracy;
+    const long nfold = (long)(h0 + 1) * (h1 + 1) * (h2 + 1);
+    double* Kc = nullptr;
+    double* full = nullptr;
+    double2* X = nullptr;
+    double2* tw64 = nullptr;
+    double* dmax = nullptr;
+    int rc = HSB_OK;
+    const long vol = (long)L0 * L1 * L2;
+#define TRY(x)                                  \
+    do {                                        \
+        cudaError_t e_ = (x);                   \
+        if (e_ != cudaSuccess) {                \
+            hsb_set_error("demag setup: %s: %s", #x, cudaGetErrorString(e_)); \
+            rc = HSB_ERR_CUDA;                  \
+            goto done;                          \
+        }                                       \
+    } while (0)
+    TRY(cudaMalloc(&Kc, sizeof(double) * 6 * nfold));
+    TRY(cudaMalloc(&full, sizeof(double) * vol));
+    TRY(cudaMalloc(&X, sizeof(double2) * (long)L0 * C2 * L1));
+    TRY(cudaMalloc(&dmax, sizeof(double)));
+    TRY(cudaMemsetAsync(dmax, 0, sizeof(double), st));
+    if (make_twiddles<double2>(P->twL, &tw64) != HSB_OK) { rc = HSB_ERR_CUDA; goto done; }
+    TRY(hsb_arne_launch(&g, Kc, st));
+    {
+        const int M = L2 / 2;
+        const int TY = pick_tile(M, sizeof(double2), SMEM_TILE_BUDGET, 16);
+        const int smx = 2 * TY * fpad_len(M) * (int)sizeof(double2);
+        TRY(cudaFuncSetAttribute(k_fft_x_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
+        const int TB = pick_tile(L1, sizeof(double2), SMEM_TILE_BUDGET, 16);
+        const int smy = 2 * TB * fpad_len(L1) * (int)sizeof(double2);
+        TRY(cudaFuncSetAttribute(k_fft_cols<double, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smy));
+        const int TK = pick_tile(L0, sizeof(double2), SMEM_TILE_BUDGET, 16);
+        const int smz = 2 * TK * fpad_len(L0) * (int)sizeof(double2);
+        TRY(cudaFuncSetAttribute(k_fft_z<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz));
+        const double scale = 1.0 / ((double)L0 * L1 * L2);
+        for (int comp = 0; comp < 6; comp++) {
+            TRY(hsb_arne_expand_launch(Kc, comp, L0, L1, L2, full, st));
+            dim3 gx(hsb_div_up(L1, TY), L0);
+            k_fft_x_fwd<double><<<gx, XTHREADS, smx, st>>>(full, full, nullptr, 0, nullptr, 0, L0, L1, L2, L2, L1, X,
+                                                               tw64, P->twL, TY, nullptr);
+            const long ncol = (long)L0 * C2;
+            k_fft_cols<double, -1><<<hsb_div_up(ncol, TB), XTHREADS, smy, st>>>(X, L1, L1, X, L1, L1, L1,
+                                                                                  ncol, tw64, P->twL, TB, nullptr);
+            dim3 gz(hsb_div_up(L1, TK), C2);
+            k_fft_z<double><<<gz, XTHREADS, smz, st>>>(X, 1, L0, L0, C2, L1, nullptr, 0, tw64, P->twL, TK, nullptr);
+            k_extract<<<hsb_grid_1d((long)C2 * (h1 + 1) * (h0 + 1), 256), 256, 0, st>>>(X, L0, C2, L1, comp, scale,
+                                                                                         P->kern, dmax);
+            TRY(cudaGetLastError());
+        }
+        TRY(cudaMemcpyAsync(&P->kern_max_imag, dmax, sizeof(double), cudaMemcpyDeviceToHost, st));
+        TRY(cudaStreamSynchronize(st));
+    }
+done:
+#undef TRY
+    cudaFree(Kc);
+    cudaFree(full);
+    cudaFree(X);
+    cudaFree(tw64);
+    cudaFree(dmax);
+    return rc;
+}
+
+HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, const int* pbc,
+                                     int accuracy, void* stream, hsb_demag_plan* out) {
+    if (!size || !cellsize || !pbc || !out) {
+        hsb_set_error("hsb_demag_plan_create: null argument");
+        return HSB_ERR_INVALID;
+    }
+    *out = nullptr;
+    hsb_demag_plan_s* P = (hsb_demag_plan_s*)calloc(1, sizeof(hsb_demag_plan_s));
+    if (!P) return HSB_ERR_NOMEM;
+    for (int a = 0; a < 3; a++) {
+        P->N[a] = size[a];
+        P->pbc[a] = pbc[a];
+        P->cs[a] = cellsize[a];
+        if (size[a] < 1 || cellsize[a] <= 0 || pbc[a] < 0) {
+            free(P);
+            hsb_set_error("hsb_demag_plan_create: bad size/cellsize/pbc on axis %d", a);
+            return HSB_ERR_INVALID;
+        }
+        P->L[a] = (size[a] > 1 && pbc[a] == 0) ? 2 * size[a] : size[a];
+        if (!is_pow2(P->L[a])) {
+            free(P);
+            hsb_set_error("hsb_demag_plan_create: padded size %d on axis %d is not a power of two", P->L[a], a);
+            return HSB_ERR_UNSUPPORTED;
+        }
+    }
+    if (P->L[2] < 2 || P->L[0] > 4096 || P->L[1] > 4096 || P->L[2] > 8192) {
+        free(P);
+        hsb_set_error("hsb_demag_plan_create: padded size (%d,%d,%d) outside 2..4096 (a2 >= 2)", P->L[0], P->L[1], P->L[2]);
+        return HSB_ERR_UNSUPPORTED;
+    }
+    const int N0 = P->N[0], N1 = P->N[1], L0 = P->L[0], L1 = P->L[1], L2 = P->L[2];
+    P->C2 = L2 / 2 + 1;
+    P->twL = L0 > L1 ? L0 : L1;
+    if (L2 > P->twL) P->twL = L2;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+#define PTRY(x)                                                                   \
+    do {                                                                          \
+        cudaError_t e_ = (x);                                                     \
+        if (e_ != cudaSuccess) {                                                  \
+            hsb_set_error("hsb_demag_plan_create: %s: %s", #x, cudaGetErrorString(e_)); \
+            hsb_demag_plan_destroy(P);                                            \
+            return HSB_ERR_CUDA;                                                  \
+        }                                                                         \
+    } while (0)
+    const long kcount = (long)P->C2 * (L1 / 2 + 1) * (L0 / 2 + 1) * 6;
+    PTRY(cudaMalloc(&P->kern, sizeof(float) * kcount));
+    PTRY(cudaMalloc(&P->X1, sizeof(float2) * 3L * N0 * P->C2 * N1));
+    rc = make_twiddles<float2>(P->twL, &P->tw);
+    if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }
+    // launch geometry
+    const int M = L2 / 2;
+    P->TYx = pick_tile(M, sizeof(float2), SMEM_TILE_BUDGET, 16);
+    P->smem_x = 2 * P->TYx * fpad_len(M) * (int)sizeof(float2);
+    P->TYxi = P->TYx;
+    P->smem_xi = P->smem_x;
+    PTRY(cudaFuncSetAttribute(k_fft_x_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_x));
+    PTRY(cudaFuncSetAttribute(k_fft_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_xi));
+    const int yz_smem = 2 * 3 * N0 * fpad_len(L1) * (int)sizeof(float2);
+    P->fused = (L0 <= 16 && yz_smem <= 220 * 1024);
+    if (P->fused) {
+        P->lz = L0;
+        P->smem_yz = yz_smem;
+        switch (L0) {
+#define SETYZ(LZ) case LZ: PTRY(cudaFuncSetAttribute(k_fft_yz_conv<LZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz_smem)); break;
+            SETYZ(1) SETYZ(2) SETYZ(4) SETYZ(8) SETYZ(16)
+#undef SETYZ
+        }
+    } else {
+        PTRY(cudaMalloc(&P->X2, sizeof(float2) * 3L * N0 * P->C2 * L1));
+        P->TBy = pick_tile(L1, sizeof(float2), SMEM_TILE_BUDGET, 16);
+        P->smem_y = 2 * P->TBy * fpad_len(L1) * (int)sizeof(float2);
+        PTRY(cudaFuncSetAttribute(k_fft_cols<float, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_y));
+        PTRY(cudaFuncSetAttribute(k_fft_cols<float, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_y));
+        P->TKz = pick_tile(L0, 3 * sizeof(float2), SMEM_TILE_BUDGET, 32);
+        P->smem_z = 2 * 3 * P->TKz * fpad_len(L0) * (int)sizeof(float2);
+        PTRY(cudaFuncSetAttribute(k_fft_z<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_z));
+    }
+#undef PTRY
+    rc = build_kernel_spectrum(P, accuracy, st);
+    if (rc != HSB_OK) {
+        hsb_demag_plan_destroy(P);
+        return rc;
+    }
+    *out = P;
+    return HSB_OK;
+}
+
+HSB_EXPORT int hsb_demag_plan_destroy(hsb_demag_plan P) {
+    if (!P) return HSB_OK;
+    cudaFree(P->kern);
+    cudaFree(P->X1);
+    cudaFree(P->X2);
+    cudaFree(P->tw);
+    free(P);
+    return HSB_OK;
+}
+
+int hsb_demag_nlaunch(hsb_demag_plan P) { return P ? (P->fused ? 3 : 5) : 0; }
+
+HSB_EXPORT int hsb_demag_plan_info(hsb_demag_plan P, int* logic, int* fused, double* max_imag) {
+    if (!P) return HSB_ERR_INVALID;
+    if (logic) for (int a = 0; a < 3; a++) logic[a] = P->L[a];
+    if (fused) *fused = P->fused;
+    if (max_imag) *max_imag = P->kern_max_imag;
+    return HSB_OK;
+}
+
+// Launch the convolution: H (A/m, FP32 SoA [3][N0][N1][N2]) = Ms0 * K (*) (m * mask).
+int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, float ms0,
+                     cudaStream_t st, const int* active) {
+    const int N0 = P->N[0], N1 = P->N[1], N2 = P->N[2];
+    const int L0 = P->L[0], L1 = P->L[1], L2 = P->L[2];
+    const int C2 = P->C2;
+    const long ncell = (long)N0 * N1 * N2;
+    if (io.ev) cudaEventRecord(io.ev[0], st);
+    dim3 gx(hsb_div_up(N1, P->TYx), 3 * N0);
+    k_fft_x_fwd<float><<<gx, XTHREADS, P->smem_x, st>>>(io.m[0], io.m[1], io.msel, io.minv, mask, ncell, N0, N1, N2, L2, N1, P->X1, P->tw,
+                                                                P->twL, P->TYx, active);
+    if (io.ev) cudaEventRecord(io.ev[1], st);
+    if (P->fused) {
+        switch (P->lz) {
+#define RUNYZ(LZ) case LZ: k_fft_yz_conv<LZ><<<C2, yz_threads<LZ>::value, P->smem_yz, st>>>(P->X1, N0, N1, L1, C2, P->kern, P->tw, P->twL, active); break;
+            RUNYZ(1) RUNYZ(2) RUNYZ(4) RUNYZ(8) RUNYZ(16)
+#undef RUNYZ
+        }
+    } else {
+        const long ncol = 3L * N0 * C2;
+        k_fft_cols<float, -1><<<hsb_div_up(ncol, P->TBy), XTHREADS, P->smem_y, st>>>(
+            P->X1, N1, N1, P->X2, L1, L1, L1, ncol, P->tw, P->twL, P->TBy, active);
+        dim3 gz(hsb_div_up(L1, P->TKz), C2);
+        k_fft_z<float><<<gz, XTHREADS, P->smem_z, st>>>(P->X2, 3, N0, L0, C2, L1, P->kern, 1, P->tw, P->twL,
+                                                               P->TKz, active);
+        k_fft_cols<float, +1><<<hsb_div_up(ncol, P->TBy), XTHREADS, P->smem_y, st>>>(
+            P->X2, L1, L1, P->X1, N1, N1, L1, ncol, P->tw, P->twL, P->TBy, active);
+    }
+    if (io.ev) cudaEventRecord(io.ev[2], st);
+    dim3 gi(hsb_div_up(N1, P->TYxi), 3 * N0);
+    k_fft_x_inv<<<gi, XTHREADS, P->smem_xi, st>>>(P->X1, N1, N0, N1, N2, L2, io.h[0], io.h[1], io.hsel, io.hinv,
+                                                  ncell, ms0, P->tw, P->twL,
+                                                         P->TYxi, active);
+    if (io.ev) cudaEventRecord(io.ev[3], st);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        hsb_set_error("hsb_demag_launch: %s", cudaGetErrorString(e));
+        return HSB_ERR_CUDA;
+    }
+    return HSB_OK;
+}
+
+HSB_EXPORT int hsb_demag_field(hsb_demag_plan P, const float* m, const float* mask, double msat0T0,
+                               float* H, void* stream) {
+    if (!P || !m || !H) {
+        hsb_set_error("hsb_demag_field: null argument");
+        return HSB_ERR_INVALID;
+    }
+    HsbDemagIO io = {{m, m}, nullptr, 0, {H, H}, nullptr, 0, nullptr};
+    return hsb_demag_launch(P, io, mask, (float)msat0T0, (cudaStream_t)stream, nullptr);
+}
+
+// Per-kernel device time of one convolution: ms[0] x-pass, ms[1] y/z pass(es), ms[2] inverse
+// x-pass (CUDA events on `stream`, averaged over `reps` launches after one warm-up).
+HSB_EXPORT int hsb_demag_profile(hsb_demag_plan P, const float* m, const float* mask, double msat0T0, float* H,
+                                 void* stream, int reps, double* ms) {
+    if (!P || !m || !H || !ms || reps < 1) return HSB_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t ev[4];
+    for (int i = 0; i < 4; i++) HSB_CUDA_TRY(cudaEventCreate(&ev[i]));
+    double acc[3] = {0, 0, 0};
+    int rc = HSB_OK;
+    for (int r = 0; r <= reps && rc == HSB_OK; r++) {
+        HsbDemagIO io = {{m, m}, nullptr, 0, {H, H}, nullptr, 0, ev};
+        rc = hsb_demag_launch(P, io, mask, (float)msat0T0, st, nullptr);
+        if (rc != HSB_OK) break;
+        if (cudaEventSynchronize(ev[3]) != cudaSuccess) { rc = HSB_ERR_CUDA; break; }
+        if (r == 0) continue;
+        for (int i = 0; i < 3; i++) {
+            float t = 0;
+            cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+            acc[i] += t;
+        }
+    }
+    for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
+    for (int i = 0; i < 3; i++) ms[i] = acc[i] / reps;
+    return rc;
+}
+
+HSB_EXPORT int hsb_demag_kernel_copy(hsb_demag_plan P, float* host_out, long count) {
+    if (!P || !host_out) return HSB_ERR_INVALID;
+    const long kcount = (long)P->C2 * (P->L[1] / 2 + 1) * (P->L[0] / 2 + 1) * 6;
+    if (count < kcount) {
+        hsb_set_error("hsb_demag_kernel_copy: need %ld floats", kcount);
+        return HSB_ERR_INVALID;
+    }
+    HSB_CUDA_TRY(cudaMemcpy(host_out, P->kern, sizeof(float) * kcount, cudaMemcpyDeviceToHost));
+    return HSB_OK;
+}

@@ -1,0 +1,399 @@
+// Fused LLBar / LLB / two-temperature right-hand side and Runge-Kutta stage update.
+//
+// One thread per cell evaluates, in registers, everything hotspin computes with a chain of
+// separate kernels and host syncs per right-hand side (SURVEY call stack CS2):
+//   H_eff = H_ex (exchange6.cu:11-127) + H_anis (uniaxialanisotropy.cu:12-52)
+//         + B_ext/mu0 (mod_zeeman.go) + H_demag (input) + H_lf (long_field.cu:13-72)
+//         + H_therm (temperature.cu:14-70 on Philox normals)
+//   dm/dt = gamma (H x m) + gamma diag(lambda) H   (llbar-torque.cu, llbar-local00nc.cu)
+//   dTe/dt = (ke lap Te + G (Tl - Te) + Q_laser) / (gamma_e Te),
+//   dTl/dt = (kl lap Tl + G (Te - Tl)) / Cl       (Qspat.cu, Qinter.cu, div.cu, mod_ce.go)
+// and then performs the stage arithmetic of the integrator (store k_s, form the next stage
+// point / the new state, renormalise m, accumulate the error norm).  Storage is FP32 SoA
+// [channel][a0][a1][a2]; the error norm is a max-norm (exact in any precision).
+#include <math.h>
+
+#include "hsb_common.cuh"
+#include "hsb_llg.cuh"
+#include "hsb_philox.cuh"
+
+__device__ __forceinline__ float* resolve(const PtrSel& s, const HsbSolverDev* sd) {
+    switch (s.sel) {
+        case SEL_CUR: return s.p[sd->cur];
+        case SEL_NEXT: return s.p[1 - sd->cur];
+        case SEL_K1: return s.p[sd->kslot];
+        case SEL_K7: return s.p[1 - sd->kslot];
+        default: return s.p[0];
+    }
+}
+
+// B_J(x) and B_J'(x) with the reference's 4-term series below the linear range
+// (common_func.h:72-120); Langevin L(x), L'(x) for classical spins (common_func.h:122-138).
+__device__ __forceinline__ void mfa_w(const HsbPhys& P, float x, float& W, float& dW) {
+    if (P.lf_langevin) {
+        if (fabsf(x) < 0.2f) {
+            const float x2 = x * x;
+            W = x / 3.0f - x * x2 / 45.0f + x * x2 * x2 * 2.0f / 945.0f - x * x2 * x2 * x2 / 4725.0f;
+            dW = 1.0f / 3.0f - x2 / 15.0f + x2 * x2 * 2.0f / 189.0f - x2 * x2 * x2 / 675.0f;
+        } else {
+            const float c = 1.0f / tanhf(x);
+            W = c - 1.0f / x;
+            dW = 1.0f - c * c + 1.0f / (x * x);
+        }
+        return;
+    }
+    const float g = P.lf_gpre, l = P.lf_lpre;
+    if (fabsf(x) < P.lf_lim) {
+        const float g2 = g * g, l2 = l * l, g4 = g2 * g2, l4 = l2 * l2, g6 = g4 * g2, l6 = l4 * l2,
+                    g8 = g4 * g4, l8 = l4 * l4, x2 = x * x;
+        W = (g2 - l2) * x / 3.0f - (g4 - l4) * x * x2 / 45.0f + (g6 - l6) * x * x2 * x2 * 2.0f / 945.0f -
+            (g8 - l8) * x * x2 * x2 * x2 / 4725.0f;
+        dW = (g2 - l2) / 3.0f - (g4 - l4) * x2 / 15.0f + (g6 - l6) * x2 * x2 * 2.0f / 189.0f -
+             (g8 - l8) * x2 * x2 * x2 / 675.0f;
+    } else {
+        const float cg = 1.0f / tanhf(g * x), cl = 1.0f / tanhf(l * x);
+        W = g * cg - l * cl;
+        dW = (g * g - l * l) + l * l * cl * cl - g * g * cg * cg;
+    }
+}
+
+template <int CH>
+__device__ __forceinline__ void load_ch(const float* __restrict__ y, long n, long i, float* v) {
+#pragma unroll
+    for (int c = 0; c < CH; c++) v[c] = __ldg(y + c * n + i);
+}
+
+// Right-hand side at cell (a0, a1, a2) = index i.  k[0..2] = dm/dt, k[3], k[4] = dTe/dt, dTl/dt.
+template <int CH>
+__device__ __forceinline__ void rhs_cell(const HsbPhys& P, const float* __restrict__ ys,
+                                         const float* __restrict__ hd, const float* __restrict__ yth,
+                                         double t, double dt, long long step, int a0, int a1, int a2,
+                                         long i, float* y, float* k) {
+    const long n = P.ncell;
+    const long s1 = P.N2, s0 = (long)P.N1 * P.N2;
+    load_ch<CH>(ys, n, i, y);
+    const float ms = P.msat_mask ? __ldg(P.msat_mask + i) : 1.0f;
+    float H[3] = {0.f, 0.f, 0.f};
+    // ---- exchange (6 neighbours, clamp / wrap)
+    {
+        const float l0 = P.lex_mask ? __ldg(P.lex_mask + i) : 1.0f;
+        const float l02 = l0 * l0;
+        const int lo[3] = {nb_lo(a0, P.N0, P.pbc0), nb_lo(a1, P.N1, P.pbc1), nb_lo(a2, P.N2, P.pbc2)};
+        const int hi[3] = {nb_hi(a0, P.N0, P.pbc0), nb_hi(a1, P.N1, P.pbc1), nb_hi(a2, P.N2, P.pbc2)};
+        const int me[3] = {a0, a1, a2};
+        const long st[3] = {s0, s1, 1};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if (P.ex_c[d] == 0.f) continue;
+            const long im = i + (long)(lo[d] - me[d]) * st[d];
+            const long ip = i + (long)(hi[d] - me[d]) * st[d];
+            float w1 = 1.f, w2 = 1.f;
+            if (P.lex_mask) {
+                const float lm = __ldg(P.lex_mask + im), lp = __ldg(P.lex_mask + ip);
+                w1 = harm0(l02, lm * lm);
+                w2 = harm0(l02, lp * lp);
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float fm = __ldg(ys + c * n + im), fp = __ldg(ys + c * n + ip);
+                H[c] += P.ex_c[d] * ((w1 * fm + w2 * fp) - (w1 * y[c] + w2 * y[c]));
+            }
+        }
+    }
+    // ---- uniaxial anisotropy
+    if (P.ku_pre != 0.f && ms != 0.f) {
+        const float pre = P.ku_pre / ms;
+        const float mu = y[0] * P.uhat[0] + y[1] * P.uhat[1] + y[2] * P.uhat[2];
+#pragma unroll
+        for (int c = 0; c < 3; c++) H[c] += pre * mu * P.u[c];
+    }
+    // ---- demag + Zeeman
+    if (hd) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) H[c] += __ldg(hd + c * n + i);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) H[c] += P.bext[c];
+    // ---- spin temperature
+    float Ts = P.T_uniform;
+    if (CH >= 5) Ts = y[3];
+    // ---- MFA longitudinal field
+    if (P.llb && ms != 0.f) {
+        const float am = sqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+        if (am > 1e-30f && Ts > 0.f) {
+            const float b = P.lf_b / Ts;
+            float W, dW;
+            mfa_w(P, am * b, W, dW);
+            const float mult = P.lf_pre * Ts * (W - am) / (ms * dW);
+            const float inv = 1.0f / am;
+#pragma unroll
+            for (int c = 0; c < 3; c++) H[c] += mult * y[c] * inv;
+        }
+    }
+    // ---- thermal field: Philox normals of this cell and step, amplitude from the step start
+    if (P.thermal && ms != 0.f) {
+        float Tth = P.T_uniform;
+        if (CH >= 5) Tth = __ldg(yth + 3 * n + i);
+        if (Tth > 0.f) {
+            const double dte = dt > P.cutoff_dt ? dt : P.cutoff_dt;
+            const float amp = sqrtf((float)(P.th_pre / dte) * Tth / ms);
+            float g[3];
+            philox_normals3((uint32_t)i, (uint64_t)step, P.seed_lo, P.seed_hi, g);
+#pragma unroll
+            for (int c = 0; c < 3; c++) H[c] += amp * sqrtf(P.lam[c]) * g[c];
+        }
+    }
+    // ---- LLBar torque + zero-order local relaxation (zero in vacuum)
+    if (ms == 0.f) {
+        k[0] = k[1] = k[2] = 0.f;
+    } else {
+        const float g = P.gamma;
+        k[0] = g * (-H[1] * y[2] + H[2] * y[1]) + g * P.lam[0] * H[0];
+        k[1] = g * (-H[2] * y[0] + H[0] * y[2]) + g * P.lam[1] * H[1];
+        k[2] = g * (-H[0] * y[1] + H[1] * y[0]) + g * P.lam[2] * H[2];
+    }
+    // ---- two-temperature model
+    if (CH >= 5) {
+        const float Te = y[3], Tl = y[4];
+        float lapE = 0.f, lapL = 0.f;
+        const int lo[3] = {nb_lo(a0, P.N0, P.pbc0), nb_lo(a1, P.N1, P.pbc1), nb_lo(a2, P.N2, P.pbc2)};
+        const int hi[3] = {nb_hi(a0, P.N0, P.pbc0), nb_hi(a1, P.N1, P.pbc1), nb_hi(a2, P.N2, P.pbc2)};
+        const int me[3] = {a0, a1, a2};
+        const long st[3] = {s0, s1, 1};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const long im = i + (long)(lo[d] - me[d]) * st[d];
+            const long ip = i + (long)(hi[d] - me[d]) * st[d];
+            if (P.ke_c[d] != 0.f) lapE += P.ke_c[d] * ((__ldg(ys + 3 * n + im) + __ldg(ys + 3 * n + ip)) - (Te + Te));
+            if (P.kl_c[d] != 0.f) lapL += P.kl_c[d] * ((__ldg(ys + 4 * n + im) + __ldg(ys + 4 * n + ip)) - (Tl + Tl));
+        }
+        float Qe = lapE + P.g_ep * (Tl - Te);
+        if (P.laser_p0 != 0.f) {
+            const float ts = (float)(t - (double)P.laser_t0);
+            float q = P.laser_p0 * expf(-P.laser_c * ts * ts);
+            if (P.laser_inv2s2 != 0.f) {
+                const float yy = ((float)a1 + 0.5f - 0.5f * (float)P.N1) * P.cs1;
+                const float xx = ((float)a2 + 0.5f - 0.5f * (float)P.N2) * P.cs2;
+                q *= expf(-(xx * xx + yy * yy) * P.laser_inv2s2);
+            }
+            Qe += q;
+        }
+        const float Ce = P.gamma_e * Te;
+        k[3] = (Ce == 0.f) ? 0.f : Qe / Ce;
+        const float Ql = lapL + P.g_ep * (Te - Tl);
+        k[4] = (P.c_l == 0.f) ? 0.f : Ql / P.c_l;
+    }
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned int* a, float v) {
+    atomicMax(a, __float_as_uint(v));
+}
+
+template <int CH>
+__global__ void __launch_bounds__(256) k_stage(const HsbPhys P, const StageArgs A, HsbSolverDev* sd) {
+    if (!A.ungated && !sd->active) return;
+    const double t = sd->t;
+    const double dt = sd->dt;
+    const long long step = sd->step;
+    const float* ys = resolve(A.ys, sd);
+    const float* hd = resolve(A.hd, sd);
+    const float* yth = resolve(A.ytherm, sd);
+    float* kout = resolve(A.kout, sd);
+    const float* kacc = resolve(A.kacc, sd);
+    float* ynext = resolve(A.ynext, sd);
+    const float* ybase = resolve(A.ybase, sd);
+    const float* yerr0 = resolve(A.yerr0, sd);
+    const float* kin[HSB_MAXK];
+#pragma unroll
+    for (int j = 0; j < HSB_MAXK; j++) kin[j] = (j < A.nk || A.err) ? resolve(A.kin[j], sd) : nullptr;
+    const double ts = t + (double)A.tfrac * dt;
+    const float fdt = (float)dt;
+    const long n = P.ncell;
+    float emax = 0.f;
+    bool bad = false;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int a2 = (int)(i % P.N2);
+        const long r = i / P.N2;
+        const int a1 = (int)(r % P.N1);
+        const int a0 = (int)(r / P.N1);
+        float y[CH], k[CH];
+        rhs_cell<CH>(P, ys, hd, yth, ts, dt, step, a0, a1, a2, i, y, k);
+        if (kout) {
+#pragma unroll
+            for (int c = 0; c < CH; c++) {
+                float v = A.kself_w * k[c];
+                if (kacc) v += A.kacc_w * __ldg(kacc + c * n + i);
+                kout[c * n + i] = v;
+            }
+        }
+        if (ynext) {
+            float acc[CH];
+#pragma unroll
+            for (int c = 0; c < CH; c++) acc[c] = A.cself * k[c];
+#pragma unroll
+            for (int j = 0; j < HSB_MAXK; j++) {
+                if (j < A.nk && A.ck[j] != 0.f) {
+#pragma unroll
+                    for (int c = 0; c < CH; c++) acc[c] += A.ck[j] * __ldg(kin[j] + c * n + i);
+                }
+            }
+            float out[CH];
+#pragma unroll
+            for (int c = 0; c < CH; c++) out[c] = __ldg(ybase + c * n + i) + fdt * acc[c];
+            if (A.normalize) {
+                const float l2 = out[0] * out[0] + out[1] * out[1] + out[2] * out[2];
+                const float inv = (l2 == 0.f) ? 0.f : rsqrtf(l2);
+                out[0] *= inv;
+                out[1] *= inv;
+                out[2] *= inv;
+            }
+#pragma unroll
+            for (int c = 0; c < CH; c++) {
+                ynext[c * n + i] = out[c];
+                bad |= !isfinite(out[c]);
+            }
+        }
+        if (A.err) {
+            float e[CH];
+#pragma unroll
+            for (int c = 0; c < CH; c++) e[c] = A.ceself * k[c];
+#pragma unroll
+            for (int j = 0; j < HSB_MAXK; j++) {
+                if (A.ce[j] != 0.f) {
+#pragma unroll
+                    for (int c = 0; c < CH; c++) e[c] += A.ce[j] * __ldg(kin[j] + c * n + i);
+                }
+            }
+            float em = fmaxf(fabsf(e[0]), fmaxf(fabsf(e[1]), fabsf(e[2]))) * fdt / A.rtol;
+#pragma unroll
+            for (int c = 3; c < CH; c++) {
+                const float sc = A.rtol * fmaxf(fabsf(__ldg(yerr0 + c * n + i)), fabsf(y[c]));
+                const float ec = fabsf(e[c]) * fdt;
+                em = fmaxf(em, sc > 0.f ? ec / sc : (ec > 0.f ? INFINITY : 0.f));
+            }
+            if (!(em == em)) bad = true;   // NaN
+            emax = fmaxf(emax, em);
+        }
+    }
+    if (A.err) {
+        emax = warp_max_f(emax);
+        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&sd->err_acc, emax);
+    }
+    if (bad) atomicOr(&sd->nonfinite, 1u);
+}
+
+// Next stage point / new state without a right-hand-side evaluation:
+// ynext = ybase + dt * sum_j ck[j] kin[j] (renormalised in LLG mode).
+template <int CH>
+__global__ void __launch_bounds__(256) k_combine(const HsbPhys P, const StageArgs A, HsbSolverDev* sd) {
+    if (!sd->active) return;
+    const float fdt = (float)sd->dt;
+    const long n = P.ncell;
+    float* ynext = resolve(A.ynext, sd);
+    const float* ybase = resolve(A.ybase, sd);
+    const float* kin[HSB_MAXK];
+#pragma unroll
+    for (int j = 0; j < HSB_MAXK; j++) kin[j] = (j < A.nk) ? resolve(A.kin[j], sd) : nullptr;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        float out[CH];
+#pragma unroll
+        for (int c = 0; c < CH; c++) {
+            float acc = 0.f;
+#pragma unroll
+            for (int j = 0; j < HSB_MAXK; j++)
+                if (j < A.nk && A.ck[j] != 0.f) acc += A.ck[j] * __ldg(kin[j] + c * n + i);
+            out[c] = __ldg(ybase + c * n + i) + fdt * acc;
+        }
+        if (A.normalize) {
+            const float l2 = out[0] * out[0] + out[1] * out[1] + out[2] * out[2];
+            const float inv = (l2 == 0.f) ? 0.f : rsqrtf(l2);
+            out[0] *= inv;
+            out[1] *= inv;
+            out[2] *= inv;
+        }
+#pragma unroll
+        for (int c = 0; c < CH; c++) ynext[c * n + i] = out[c];
+    }
+}
+
+// Dormand-Prince step-size control, one thread (see the controller rule in the header of
+// include/hotspin_b200.h).  Consumes the attempt's error maximum.
+__global__ void k_dp45_control(HsbSolverDev* sd) {
+    if (!sd->active) return;
+    const float ef = __uint_as_float(sd->err_acc);
+    const unsigned int nf = sd->nonfinite;
+    sd->err_acc = 0u;
+    sd->nonfinite = 0u;
+    const double h = sd->dt;
+    double err = (double)ef;
+    bool finite = (nf == 0u) && isfinite(err);
+    bool accept = finite && (err <= 1.0 || h <= sd->mindt);
+    double fac;
+    if (!finite) fac = 0.2;
+    else if (err == 0.0) fac = 5.0;
+    else fac = 0.9 * pow(err, -0.2);
+    fac = fmin(fmax(fac, 0.2), accept ? 5.0 : 1.0);
+    double nd = fmin(fmax(h * fac, sd->mindt), sd->maxdt);
+    sd->err = finite ? err : INFINITY;
+    sd->attempts += 1;
+    if (!finite && h <= sd->mindt) sd->status |= 1;
+    if (accept) {
+        sd->t += h;
+        sd->step += 1;
+        sd->cur = 1 - sd->cur;
+        sd->kslot = 1 - sd->kslot;
+    } else {
+        sd->rejects += 1;
+        if (h <= sd->mindt) sd->status |= 2;
+    }
+    if (sd->t_stop > 0.0) {
+        const double rem = sd->t_stop - sd->t;
+        if (rem <= 1e-6 * nd || rem <= 0.0) sd->active = 0;
+        else if (nd > rem) nd = rem;
+    }
+    if (sd->step_stop >= 0 && sd->step >= sd->step_stop) sd->active = 0;
+    if (sd->status & 1) sd->active = 0;
+    sd->dt = nd;
+}
+
+// Fixed-step bookkeeping: t += dt, step++, swap state buffers, stop at the target.
+__global__ void k_fixed_advance(HsbSolverDev* sd) {
+    if (!sd->active) return;
+    sd->t += sd->dt;
+    sd->step += 1;
+    sd->cur = 1 - sd->cur;
+    sd->attempts += 1;
+    if (sd->nonfinite) {
+        sd->status |= 1;
+        sd->active = 0;
+    }
+    if (sd->step_stop >= 0 && sd->step >= sd->step_stop) sd->active = 0;
+    if (sd->t_stop > 0.0 && sd->t_stop - sd->t <= 1e-6 * sd->dt) sd->active = 0;
+}
+
+// ------------------------------------------------------------------------------ launchers
+int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st) {
+    const int threads = 256;
+    const int grid = hsb_grid_1d(P.ncell, threads, 8);
+    if (P.nch == 5) k_stage<5><<<grid, threads, 0, st>>>(P, A, sd);
+    else k_stage<3><<<grid, threads, 0, st>>>(P, A, sd);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}
+
+int hsb_launch_combine(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st) {
+    const int threads = 256;
+    const int grid = hsb_grid_1d(P.ncell, threads, 8);
+    if (P.nch == 5) k_combine<5><<<grid, threads, 0, st>>>(P, A, sd);
+    else k_combine<3><<<grid, threads, 0, st>>>(P, A, sd);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}
+
+int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st) {
+    k_dp45_control<<<1, 1, 0, st>>>(sd);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}
+
+int hsb_launch_fixed_advance(HsbSolverDev* sd, cudaStream_t st) {
+    k_fixed_advance<<<1, 1, 0, st>>>(sd);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}

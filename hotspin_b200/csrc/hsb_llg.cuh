@@ -1,0 +1,96 @@
+// Fused right-hand side + Runge-Kutta stage kernel: shared declarations.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+// Maximum number of stored stages any integrator reads (Dormand-Prince: 7).
+#define HSB_MAXK 7
+
+// Uniform physics parameters of one simulation, FP32 where used in the bulk arithmetic.
+struct HsbPhys {
+    int N0, N1, N2;      // program order, N2 fastest (user x)
+    int pbc0, pbc1, pbc2;
+    int nch;             // state channels: 3 (m) or 5 (m, Te, Tl)
+    long ncell;
+    float ex_c[3];       // Ms0 * lex^2 / cs_d^2 (A/m)
+    const float* lex_mask;   // optional per-cell lex mask (harmonic lex^2 weights)
+    const float* msat_mask;  // optional per-cell Ms0 mask (0 = vacuum)
+    float gamma;         // gamma_LL (m/As)
+    float lam[3];        // relativistic damping diagonal (program components)
+    float bext[3];       // B_ext / mu0 (A/m)
+    float ku_pre;        // 2 Ku / (mu0 Ms0) (A/m)
+    float u[3];          // anisotropy axis as given
+    float uhat[3];       // normalised axis
+    int demag;
+    // MFA longitudinal field
+    int llb;
+    float lf_pre;        // n kB / (mu0 Ms0)  (A/m per K)
+    float lf_b;          // 3 S/(S+1) Tc   (K)   (S = J; 3 Tc for the Langevin case)
+    float lf_gpre, lf_lpre, lf_lim;  // Brillouin constants (2J+1)/2J, 1/2J, series limit
+    int lf_langevin;
+    float T_uniform;     // bath temperature when there is no two-temperature model
+    // thermal field
+    int thermal;
+    uint32_t seed_lo, seed_hi;
+    double th_pre;       // 2 kB / (mu0 V gamma Ms0) (multiplied by T / dt_eff)
+    double cutoff_dt;
+    // two-temperature model
+    int ttm;
+    float ke_c[3], kl_c[3];  // k / cs_d^2 (W/m^3/K)
+    float g_ep, gamma_e, c_l;
+    float laser_p0, laser_t0, laser_c;  // c = 4 ln2 / fwhm^2
+    float laser_inv2s2;                 // 1/(2 sigma^2), 0 = uniform spot
+    float cs1, cs2;
+};
+
+// Device-resident solver state (read by every kernel of an attempt, written by the
+// controller).  Lives in device memory so whole steps can be captured in a CUDA graph.
+struct HsbSolverDev {
+    double t, dt;
+    long long step;        // accepted steps
+    long long attempts, rejects;
+    int cur;               // state buffer holding y0 (0/1)
+    int kslot;             // which of the two first/last stage slots holds k1 (DP45)
+    int active;            // 0 once the target is reached: kernels of later attempts return
+    int status;            // bit 0: non-finite state seen; bit 1: dt hit mindt
+    double err;            // last error norm
+    double mindt, maxdt;
+    double t_stop;         // > 0: do not step past this time
+    long long step_stop;   // >= 0: stop after this many accepted steps
+    unsigned int err_acc;  // float bits of the running max error of the attempt
+    unsigned int nonfinite;
+};
+
+// Pointer selectors resolved on the device against HsbSolverDev.
+enum { SEL_FIXED = 0, SEL_CUR = 1, SEL_NEXT = 2, SEL_K1 = 3, SEL_K7 = 4 };
+
+struct PtrSel {
+    float* p[2];
+    int sel;
+};
+
+struct StageArgs {
+    PtrSel ys;               // right-hand-side input state [nch][ncell]
+    PtrSel hd;               // demag field of ys (3 x ncell) or null
+    PtrSel ytherm;           // state whose Te sets the thermal amplitude (step start)
+    float tfrac;             // stage time = t + tfrac * dt
+    // k_s storage: kout = kacc_w * kacc + kself_w * k_s
+    PtrSel kout;
+    PtrSel kacc;
+    float kacc_w, kself_w;
+    // next state: ynext = ybase + dt * (sum_j ck[j] kin[j] + cself k_s)
+    PtrSel ynext;
+    PtrSel ybase;
+    int nk;
+    PtrSel kin[HSB_MAXK];
+    float ck[HSB_MAXK];
+    float cself;
+    int normalize;           // renormalise m of ynext
+    // error estimate: e = dt * (sum_j ce[j] kin[j] + ceself k_s), max-norm per equation
+    int err;
+    float ce[HSB_MAXK];
+    float ceself;
+    PtrSel yerr0;            // y0 (for the relative temperature norm)
+    float rtol;
+    int ungated;             // run even when the solver is inactive (state queries)
+};

@@ -1,0 +1,132 @@
+"""Python view of the simulation handle (hsb_sim_* in include/hotspin_b200.h).
+
+Arrays are numpy float64 in hotspin's program order: scalar fields (N0, N1, N2), vector
+fields (3, N0, N1, N2) with component 0 the program X axis (user z).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+SOLVERS = {"euler": 0, "heun": 1, "rk4": 2, "dp45": 3, "rk45": 3}
+
+_FIELDS = {f[0] for f in _lib.SimDesc._fields_}
+
+
+def make_desc(**kw):
+    """Build an hsb_sim_desc from keyword arguments (names as in the C struct)."""
+    d = _lib.SimDesc()
+    d.gamma_ll = 2.211e5
+    d.spin_j = 0.5
+    d.rtol = 1e-5
+    d.mindt = 1e-22
+    d.maxdt = 1e-12
+    d.laser_fwhm = 1e-13
+    for k, v in kw.items():
+        if k not in _FIELDS:
+            raise KeyError("unknown simulation parameter %r" % k)
+        if k == "solver" and isinstance(v, str):
+            v = SOLVERS[v.lower()]
+        cur = getattr(d, k)
+        if isinstance(cur, ctypes.Array):
+            for i, x in enumerate(v):
+                cur[i] = x
+        elif isinstance(v, bool):
+            setattr(d, k, int(v))
+        else:
+            setattr(d, k, v)
+    return d
+
+
+class Simulation:
+    def __init__(self, **kw):
+        self._lib = _lib.load()
+        self.desc = make_desc(**kw)
+        self.size = tuple(self.desc.size)
+        self.ncell = int(np.prod(self.size))
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.hsb_sim_create(ctypes.byref(self.desc), ctypes.byref(h)), "hsb_sim_create")
+        self._h = h
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hsb_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- state
+    def set(self, name, arr):
+        if arr is None:
+            _lib.check(self._lib.hsb_sim_set(self._h, name.encode(), None, 0), "hsb_sim_set(%s)" % name)
+            return
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        _lib.check(self._lib.hsb_sim_set(self._h, name.encode(), a.ctypes.data_as(_lib.c_dp), a.size),
+                   "hsb_sim_set(%s)" % name)
+
+    def get(self, name):
+        ncomp = {"m": 3, "H_demag": 3, "Te": 1, "Tl": 1}.get(name)
+        if name == "k":
+            ncomp = 5 if self.desc.ttm else 3
+        if ncomp is None:
+            raise KeyError(name)
+        out = np.empty((ncomp,) + self.size if ncomp > 1 else self.size, dtype=np.float64)
+        _lib.check(self._lib.hsb_sim_get(self._h, name.encode(), out.ctypes.data_as(_lib.c_dp), out.size),
+                   "hsb_sim_get(%s)" % name)
+        return out
+
+    # -- time stepping
+    def step(self, n=1):
+        _lib.check(self._lib.hsb_sim_step(self._h, int(n)), "hsb_sim_step")
+
+    def run_until(self, t):
+        _lib.check(self._lib.hsb_sim_run_until(self._h, float(t)), "hsb_sim_run_until")
+
+    def sync(self):
+        _lib.check(self._lib.hsb_sim_sync(self._h), "hsb_sim_sync")
+
+    def status(self):
+        t, dt, err = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        st, at, rj = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        s = ctypes.c_int32()
+        _lib.check(self._lib.hsb_sim_status(self._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st),
+                                            ctypes.byref(at), ctypes.byref(rj), ctypes.byref(err),
+                                            ctypes.byref(s)), "hsb_sim_status")
+        return dict(t=t.value, dt=dt.value, steps=st.value, attempts=at.value, rejects=rj.value,
+                    err=err.value, status=s.value)
+
+    def set_time(self, t, dt=0.0):
+        _lib.check(self._lib.hsb_sim_set_time(self._h, float(t), float(dt)), "hsb_sim_set_time")
+
+    def energy(self):
+        e = ctypes.c_double()
+        _lib.check(self._lib.hsb_sim_energy(self._h, ctypes.byref(e)), "hsb_sim_energy")
+        return e.value
+
+    def average_m(self):
+        a = (ctypes.c_double * 3)()
+        _lib.check(self._lib.hsb_sim_average_m(self._h, a), "hsb_sim_average_m")
+        return np.array(list(a))
+
+
+def demag_plan(size, cellsize, pbc=(0, 0, 0), accuracy=6, stream=None):
+    """Create a demag plan; returns an opaque handle (ctypes.c_void_p)."""
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    s = (ctypes.c_int * 3)(*size)
+    c = (ctypes.c_double * 3)(*cellsize)
+    p = (ctypes.c_int * 3)(*pbc)
+    _lib.check(lib.hsb_demag_plan_create(s, c, p, accuracy, stream, ctypes.byref(h)), "hsb_demag_plan_create")
+    return h

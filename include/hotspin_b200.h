@@ -1,0 +1,164 @@
+/*
+ * hotspin_b200 -- B200 (sm_100a) implementation of the hotspin solver hot path.
+ *
+ * Two C-ABI surfaces, both exported by libhsb200.so:
+ *
+ *  1. Drop-in FP64 kernels with the names, argument order and meaning of hotspin's
+ *     libhotspin.h (generated from src/libhotspin/*.h by src/libhotspin/Makefile:35-38).
+ *     The Go layer (src/hotspin-core/gpu/libhotspin.go, wrap_*.go) binds them unchanged
+ *     through cgo; they are declared in include/libhotspin_dropin.h.
+ *
+ *  2. The simulation handle API below: one call advances the whole per-step right-hand
+ *     side and integrator (exchange, anisotropy, Zeeman, demag, MFA longitudinal field,
+ *     Philox thermal field, two-temperature model; Euler / Heun / RK4 / Dormand-Prince 4(5))
+ *     with FP32 state resident on the GPU.  It replaces the sequence that hotspin's
+ *     engine drives per step (engine/engine.go:473-508 Engine.Step -> Solver.Step ->
+ *     Quant.Update graph walk -> libhotspin kernels + cuFFT + host syncs).
+ *
+ * Conventions (reference engine/api.go:41-62, common/index.go:68-113): arrays are
+ * structure-of-arrays in *program order* -- shape (N0, N1, N2), N2 fastest = the user's x --
+ * and vector fields are component-major with component 0 = program X (user z).  All
+ * host-facing values are double.  Every function returns an int status (HSB_OK = 0);
+ * hsb_last_error() describes the last failure of the calling thread.  Nothing aborts.
+ *
+ * Dormand-Prince step control (device side, no host round trip):
+ *   err = max( max_i |e_m,i| / rtol , max_i |e_T,i| / (rtol max(|T0_i|, |T1_i|)) )
+ *   accept when err <= 1 (or dt == mindt); dt *= clamp(0.9 err^-1/5, 0.2, 5 | 1 on reject),
+ *   clamped to [mindt, maxdt] and to the requested stop time.
+ */
+#ifndef HOTSPIN_B200_H
+#define HOTSPIN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    HSB_OK = 0,
+    HSB_ERR_INVALID = 1,
+    HSB_ERR_CUDA = 2,
+    HSB_ERR_NOMEM = 3,
+    HSB_ERR_UNSUPPORTED = 4,
+    HSB_ERR_NONFINITE = 5,
+    HSB_ERR_SOLVER = 6
+};
+
+enum { HSB_SOLVER_EULER = 0, HSB_SOLVER_HEUN = 1, HSB_SOLVER_RK4 = 2, HSB_SOLVER_DP45 = 3 };
+
+/* Simulation description.  Replaces the module graph a hotspin script builds with
+ * load(...)/setv(...): exchange6, anisotropy/uniaxial, zeeman, demag, llbar +
+ * llbar/torque + llbar/damping/nonconservative/00/local, normalizer, mfa/longfield,
+ * temperature/brown, temperature/ETM + PTM + E-P + Drude + ETM/diffusion, solver/<x>. */
+typedef struct hsb_sim_desc {
+    int32_t size[3];        /* N0, N1, N2 (program order)                          */
+    int32_t pbc[3];         /* periodic images per axis, 0 = open                  */
+    double cellsize[3];     /* m, program order                                    */
+    double msat0T0;         /* Ms(T=0), A/m   (msat0T0 multiplier)                 */
+    double lex;             /* exchange length multiplier, m (lex)                 */
+    double gamma_ll;        /* m/As  (gamma_LL)                                    */
+    double alpha[3];        /* lambda diagonal, program components (alpha)         */
+    double ku;              /* J/m^3 (Ku)                                          */
+    double anis_u[3];       /* program components (anisU)                          */
+    double b_ext[3];        /* tesla, program components (B_ext)                   */
+    int32_t demag;          /* 1: demag module loaded                               */
+    int32_t normalize;      /* 1: normalizer module on m (LLG mode)                 */
+    int32_t llb;            /* 1: mfa/longfield added to H_eff                      */
+    double tc;              /* K                                                   */
+    double spin_j;          /* J                                                   */
+    double n_spins;         /* 1/m^3                                               */
+    double temperature;     /* K, bath temperature when ttm == 0                   */
+    int32_t thermal;        /* 1: temperature/brown thermal field (mu = alpha)      */
+    uint64_t seed;          /* Philox key                                          */
+    double cutoff_dt;       /* s                                                   */
+    int32_t ttm;            /* 1: two-temperature model (Te, Tl state channels)     */
+    double gamma_e;         /* J/(m^3 K^2): Ce = gamma_e Te                        */
+    double c_l;             /* J/(m^3 K)                                           */
+    double g_ep;            /* W/(m^3 K)                                           */
+    double k_e, k_l;        /* W/(m K)                                             */
+    double laser_p0;        /* W/m^3 peak absorbed power                           */
+    double laser_t0;        /* s, pulse centre                                     */
+    double laser_fwhm;      /* s                                                   */
+    double laser_sigma;     /* m, lateral Gaussian spot; 0 = uniform               */
+    int32_t solver;         /* HSB_SOLVER_*                                        */
+    double dt;              /* initial / fixed time step, s                        */
+    double rtol;            /* DP45 tolerance                                      */
+    double mindt, maxdt;    /* DP45 step bounds                                    */
+} hsb_sim_desc;
+
+typedef struct hsb_sim_s* hsb_sim;
+
+const char* hsb_last_error(void);
+void hsb_clear_error(void);
+int hsb_version(void);
+
+/* Allocate device state, build the demag kernel (FP64 Kernel_Arne on the GPU), set the
+ * initial state m = (0,0,1), Te = Tl = temperature.  Runs on the current CUDA device. */
+int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim* out);
+int hsb_sim_destroy(hsb_sim sim);
+
+/* Host <-> device state transfer in double.  name: "m" (3 N values), "Te", "Tl" (N),
+ * "msat_mask", "lex_mask" (N; set before stepping, NULL host pointer clears the mask),
+ * read-only "H_demag" (3 N, A/m, of the current state), "k" (3 N or 5 N, the right-hand
+ * side of the current state). */
+int hsb_sim_set(hsb_sim sim, const char* name, const double* host, int64_t count);
+int hsb_sim_get(hsb_sim sim, const char* name, double* host, int64_t count);
+
+/* Advance `nsteps` accepted steps / up to time t.  Asynchronous on the handle's stream
+ * except for the periodic completion checks of the adaptive solver. */
+int hsb_sim_step(hsb_sim sim, int64_t nsteps);
+int hsb_sim_run_until(hsb_sim sim, double t);
+int hsb_sim_sync(hsb_sim sim);
+
+/* Solver bookkeeping: time, current dt, accepted steps, attempts, rejected attempts,
+ * last error norm, status bits (1: non-finite state, 2: dt at mindt). */
+int hsb_sim_status(hsb_sim sim, double* t, double* dt, int64_t* steps, int64_t* attempts,
+                   int64_t* rejects, double* err, int32_t* status);
+int hsb_sim_set_time(hsb_sim sim, double t, double dt);
+
+/* Total energy (J) as hotspin's micromag/energy module sums it (mod_energy.go:20-66),
+ * FP64 compensated reduction on the device; and the average of m (3 values). */
+int hsb_sim_energy(hsb_sim sim, double* energy);
+int hsb_sim_average_m(hsb_sim sim, double* avg3);
+
+/* Device time of one attempt by kernel family (eager launches between CUDA events on the
+ * handle's stream; each profiled attempt is a real step): out[0] fused RHS+stage kernels,
+ * out[1] demag x-pass, out[2] demag y/z pass(es), out[3] demag inverse x-pass,
+ * out[4] combine / step control, out[5] launches per attempt, out[6] accepted steps. */
+int hsb_sim_profile(hsb_sim sim, int reps, double* out7);
+int hsb_sim_launches_per_attempt(hsb_sim sim, int* n);
+
+/* Mean-field tables in FP64 on the GPU: T_i = Tc i/(npts-1), m_e(T_i) by the Ridders
+ * iteration of brillouinKern (src/libhotspin/brillouin.cu:88-138) and the reduced
+ * longitudinal susceptibility chi(T_i) of kappaKern (kappa.cu:15-61) with unit masks
+ * (times Ms0^2 mu0 / (n kB) for the physical value, mod_kappa.go:76-89).
+ * hsb_mfa_equilibrium interpolates a 1024-point table. */
+int hsb_mfa_table(double Tc, double J, int npts, double* T, double* me, double* chi);
+int hsb_mfa_equilibrium(double T, double Tc, double J, double* me);
+
+/* The handle's CUDA stream (cudaStream_t) for callers that interleave their own work. */
+void* hsb_sim_stream(hsb_sim sim);
+
+/* Demag convolution on caller-owned FP32 device arrays (SoA [3][N0][N1][N2]):
+ * H (A/m) = Ms0 * K (*) (m * mask); mask may be NULL.  The plan builds the Kernel_Arne
+ * tensor (kernel_magnetostatic.go:25-241) on the GPU in FP64 (accuracy as the reference,
+ * normally 6).  Padded sizes must be powers of two, a2 padded >= 2. */
+typedef struct hsb_demag_plan_s* hsb_demag_plan;
+int hsb_demag_plan_create(const int* size, const double* cellsize, const int* pbc, int accuracy,
+                          void* stream, hsb_demag_plan* out);
+int hsb_demag_plan_destroy(hsb_demag_plan plan);
+int hsb_demag_plan_info(hsb_demag_plan plan, int* logic3, int* fused, double* kern_max_imag);
+int hsb_demag_field(hsb_demag_plan plan, const float* m, const float* mask, double msat0T0,
+                    float* H, void* stream);
+/* Device time of the three phases of one convolution (ms[0] x-pass, ms[1] y/z, ms[2]
+ * inverse x), CUDA events on `stream`, averaged over reps after a warm-up. */
+int hsb_demag_profile(hsb_demag_plan plan, const float* m, const float* mask, double msat0T0, float* H,
+                      void* stream, int reps, double* ms3);
+/* Folded FP32 kernel spectrum, layout [kx][k1][k0][6] (XX YY ZZ YZ XZ XY). */
+int hsb_demag_kernel_copy(hsb_demag_plan plan, float* host_out, long count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,208 @@
+"""FP64 time integrators (test infrastructure).
+
+* ``euler``, ``heun``, ``rk12`` restate the reference solvers (engine/solve_euler.go:22-50,
+  solve_heun.go:27-79, solve_rk12.go:91-214), including the in-place renormalisation that
+  the ``normalizer`` module applies each time m is updated (engine/quant.go:417-445).
+* ``rk4`` and ``dp45`` are integrators the reference does not have; they use the same
+  right-hand side and the same renormalisation rule: every stage point and every accepted
+  state is renormalised before it is used (LLG mode only).
+
+DP45 (Dormand-Prince 5(4), first-same-as-last) error norm, per equation:
+  m:  max_i |e_i| / rtol                       (m is reduced by Ms0, |m| <= 1)
+  T:  max_i |e_i| / (rtol * max(|T0_i|, |T1_i|))
+err = max over equations; accept when err <= 1;
+dt_new = dt * clamp(0.9 err^-1/5, 0.2, 5) after an accepted step, clamp(., 0.2, 1) after a
+rejected one, then clamped to [mindt, maxdt]; a step at mindt is always accepted.
+"""
+import math
+
+import numpy as np
+
+from . import fields as F
+
+DP_C = [0.0, 1 / 5, 3 / 10, 4 / 5, 8 / 9, 1.0, 1.0]
+DP_A = [
+    [],
+    [1 / 5],
+    [3 / 40, 9 / 40],
+    [44 / 45, -56 / 15, 32 / 9],
+    [19372 / 6561, -25360 / 2187, 64448 / 6561, -212 / 729],
+    [9017 / 3168, -355 / 33, 46732 / 5247, 49 / 176, -5103 / 18656],
+    [35 / 384, 0.0, 500 / 1113, 125 / 192, -2187 / 6784, 11 / 84],
+]
+DP_B = DP_A[6] + [0.0]
+DP_BS = [5179 / 57600, 0.0, 7571 / 16695, 393 / 640, -92097 / 339200, 187 / 2100, 1 / 40]
+DP_E = [b - bs for b, bs in zip(DP_B, DP_BS)]
+
+
+def _comb(y0, ks, coefs, h):
+    out = {}
+    for key in y0:
+        acc = np.zeros_like(y0[key])
+        for c, k in zip(coefs, ks):
+            if c != 0.0:
+                acc = acc + c * k[key]
+        out[key] = y0[key] + h * acc
+    return out
+
+
+class Integrator:
+    """Drives a ``Model``.  ``y`` is a dict of arrays; ``t``, ``dt``, ``step`` as in the
+    reference engine (engine/engine.go:473-508)."""
+
+    def __init__(self, model, y, method, dt, rtol=1e-5, mindt=1e-20, maxdt=1e-10,
+                 maxerr=1e-4, t=0.0):
+        self.model = model
+        self.norm = model.s.normalize
+        self.y = {k: np.array(v, dtype=np.float64) for k, v in y.items()}
+        if self.norm:
+            self.y["m"] = F.normalize(self.y["m"])
+        self.method = method
+        self.t = t
+        self.dt = dt
+        self.step_count = 0
+        self.rtol = rtol
+        self.mindt = mindt
+        self.maxdt = maxdt
+        self.maxerr = maxerr
+        self.bad_steps = 0
+        self.k_fsal = None
+        self.last_err = 0.0
+
+    def _fix(self, y):
+        if self.norm:
+            y = dict(y)
+            y["m"] = F.normalize(y["m"])
+        return y
+
+    def _thermal(self, dt):
+        T = self.model.spin_temperature(self.y)
+        self.model.set_thermal(self.step_count, dt, T)
+
+    def step(self):
+        getattr(self, "_" + self.method)()
+
+    def run_steps(self, n):
+        for _ in range(n):
+            self.step()
+
+    def run_until(self, t_end):
+        """Step until t_end; adaptive steps are clamped to land on it (as the device does)."""
+        while t_end - self.t > 1e-6 * self.dt:
+            if self.method == "dp45":
+                self.dt = min(self.dt, t_end - self.t)
+            self.step()
+
+    # -- reference solvers --------------------------------------------------------
+    def _euler(self):
+        f = self.model.rhs
+        self._thermal(self.dt)
+        k = f(self.t, self.y)
+        self.y = self._fix(_comb(self.y, [k], [1.0], self.dt))
+        self.t += self.dt
+        self.step_count += 1
+
+    def _heun(self):
+        f, h = self.model.rhs, self.dt
+        self._thermal(h)
+        k0 = f(self.t, self.y)
+        y1 = self._fix(_comb(self.y, [k0], [1.0], h))
+        self.t += h
+        k1 = f(self.t, y1)
+        self.y = self._fix(_comb(y1, [k1, k0], [0.5, -0.5], h))
+        self.step_count += 1
+
+    def _rk12(self):
+        """solve_rk12.go:91-214 with a single maxError for all equations."""
+        f = self.model.rhs
+        t0 = self.t
+        self._thermal(self.dt)
+        k0 = f(t0, self.y)
+        y0 = self.y
+        for tr in range(11):
+            dt = self.dt
+            y1 = self._fix(_comb(y0, [k0], [1.0], dt))
+            k1 = f(t0 + dt, y1)
+            ynew = self._fix(_comb(y1, [k1, k0], [0.5, -0.5], dt))
+            err = max(float(np.abs(k1[key] - k0[key]).max()) for key in k0) * dt
+            bad = err > self.maxerr
+            if bad:
+                self.bad_steps += 1
+                factor = (self.maxerr / err) ** (1.0 / 3.0)
+            else:
+                factor = math.sqrt(self.maxerr / err) if err > 0 else 1.5 / 0.8
+            factor = min(max(factor * 0.8, 0.1), 1.5)
+            newdt = min(max(dt * factor, self.mindt), self.maxdt)
+            self.dt = newdt
+            self.last_err = err
+            if not bad or newdt == self.mindt:
+                self.y = ynew
+                self.t = t0 + dt
+                break
+            if tr > 10:
+                raise RuntimeError("The solver cannot converge after 10 badsteps")
+        self.step_count += 1
+
+    # -- new integrators ----------------------------------------------------------
+    def _rk4(self):
+        f, h, t = self.model.rhs, self.dt, self.t
+        self._thermal(h)
+        y0 = self.y
+        k1 = f(t, y0)
+        y2 = self._fix(_comb(y0, [k1], [0.5], h))
+        k2 = f(t + 0.5 * h, y2)
+        y3 = self._fix(_comb(y0, [k2], [0.5], h))
+        k3 = f(t + 0.5 * h, y3)
+        y4 = self._fix(_comb(y0, [k3], [1.0], h))
+        k4 = f(t + h, y4)
+        self.y = self._fix(_comb(y0, [k1, k2, k3, k4], [1 / 6, 1 / 3, 1 / 3, 1 / 6], h))
+        self.t = t + h
+        self.step_count += 1
+
+    def _err_norm(self, y0, y1, e):
+        err = 0.0
+        for key in e:
+            d = np.abs(e[key])
+            if key == "m":
+                v = float(d.max()) / self.rtol
+            else:
+                scale = self.rtol * np.maximum(np.abs(y0[key]), np.abs(y1[key]))
+                v = float((d / np.where(scale == 0.0, 1.0, scale)).max())
+            err = max(err, v)
+        return err
+
+    def _dp45(self):
+        f, t0 = self.model.rhs, self.t
+        y0 = self.y
+        if self.k_fsal is None:
+            self._thermal(self.dt)
+            self.k_fsal = f(t0, y0)
+        for tr in range(64):
+            h = self.dt
+            self._thermal(h)
+            if self.model.s.thermal:
+                # the held thermal field changes with the step (and its dt), so the
+                # first stage is re-evaluated instead of reusing the last one
+                self.k_fsal = f(t0, y0)
+            ks = [self.k_fsal]
+            for s in range(1, 7):
+                ys = self._fix(_comb(y0, ks, DP_A[s], h))
+                ks.append(f(t0 + DP_C[s] * h, ys))
+            y5 = ys
+            e = {key: h * sum(DP_E[i] * ks[i][key] for i in range(7)) for key in y0}
+            err = self._err_norm(y0, y5, e)
+            self.last_err = err
+            accept = err <= 1.0 or h <= self.mindt
+            if err == 0.0:
+                fac = 5.0
+            else:
+                fac = 0.9 * err ** -0.2
+            fac = min(max(fac, 0.2), 5.0 if accept else 1.0)
+            self.dt = min(max(h * fac, self.mindt), self.maxdt)
+            if accept:
+                self.y = y5
+                self.t = t0 + h
+                self.k_fsal = ks[6]
+                break
+            self.bad_steps += 1
+        self.step_count += 1

@@ -1,0 +1,175 @@
+"""Fused FP32 right-hand side and integrators (simulation handle) against the FP64 oracle."""
+import numpy as np
+import pytest
+
+from hotspin_b200.sim import Simulation
+from oracle import fields as F
+from oracle.model import Model, Spec
+from oracle.solvers import Integrator
+from tests.gpu_util import rel_err
+
+pytestmark = pytest.mark.gpu
+
+MS, AEX = 8e5, 1.3e-11
+LEX = float(np.sqrt(2 * AEX / (F.MU0 * MS * MS)))
+
+
+def unit(seed, size):
+    m = np.random.default_rng(seed).normal(size=(3,) + size)
+    return m / np.sqrt((m * m).sum(0))
+
+
+def pair(**kw):
+    """The same problem as an oracle Spec and a device Simulation."""
+    spec = Spec(**kw)
+    desc = dict(kw)
+    desc.pop("msat_mask", None)
+    desc.pop("lex_mask", None)
+    return spec, desc
+
+
+LLG = dict(size=(2, 16, 32), cellsize=(3e-9, 3.9e-9, 3.9e-9), msat0T0=MS, lex=LEX,
+           gamma_ll=F.GAMMA0 / (1 + 0.02 ** 2), alpha=(0.02, 0.02, 0.02), b_ext=(0.0, 0.012, 0.016),
+           demag=True, normalize=True, ku=2e4, anis_u=(0.3, 0.0, 1.0))
+LLB = dict(size=(4, 16, 16), cellsize=(2e-9, 2e-9, 2e-9), msat0T0=1.1e6, lex=float(np.sqrt(2 * 1e-11 / (F.MU0 * 1.1e6 ** 2))),
+           gamma_ll=F.GAMMA0, alpha=(0.1, 0.1, 0.1), ku=7e6, anis_u=(1.0, 0.0, 0.0), demag=True, llb=True,
+           tc=700.0, spin_j=0.5, n_spins=1.1e6 / (2 * F.MUB * 0.5), temperature=300.0)
+TTM = dict(LLB, size=(2, 16, 32), cellsize=(4e-9, 4e-9, 4e-9), msat0T0=MS, lex=LEX, tc=630.0,
+           n_spins=MS / (2 * F.MUB * 0.5), alpha=(0.02, 0.02, 0.02), ku=0.0, ttm=True, gamma_e=700.0, c_l=3e6,
+           g_ep=6e17, k_e=90.0, k_l=0.0, laser_p0=5e20, laser_t0=0.0, laser_fwhm=1e-13, laser_sigma=40e-9)
+
+
+def state(kw, seed=5):
+    size = kw["size"]
+    m = unit(seed, size)
+    y = {}
+    if kw.get("llb"):
+        m = m * np.random.default_rng(seed + 1).uniform(0.6, 0.95, size=size)
+    y["m"] = m
+    if kw.get("ttm"):
+        rng = np.random.default_rng(seed + 2)
+        y["Te"] = rng.uniform(300.0, 900.0, size=size)
+        y["Tl"] = rng.uniform(300.0, 400.0, size=size)
+    return y
+
+
+@pytest.mark.parametrize("kw", [LLG, LLB, TTM], ids=["llg", "llb", "ttm"])
+@pytest.mark.parametrize("thermal", [False, True])
+def test_rhs_matches_oracle(cuda, kw, thermal):
+    kw = dict(kw, thermal=thermal, seed=77, dt=1e-14, solver="rk4")
+    if thermal and not kw.get("llb"):
+        kw["temperature"] = 200.0
+    spec, desc = pair(**{k: v for k, v in kw.items() if k not in ("solver", "dt")})
+    y = state(kw)
+    model = Model(spec)
+    model.set_thermal(0, kw["dt"], model.spin_temperature(y))
+    want = model.rhs(0.0, y)
+    with Simulation(**desc, solver="rk4", dt=kw["dt"]) as sim:
+        for name, v in y.items():
+            sim.set(name, v)
+        k = sim.get("k")
+    assert rel_err(k[:3], want["m"]) < 3e-5
+    if kw.get("ttm"):
+        assert rel_err(k[3], want["Te"]) < 3e-5
+        assert rel_err(k[4], want["Tl"]) < 3e-5
+
+
+def test_masks_rhs(cuda):
+    size = (2, 12, 20)
+    rng = np.random.default_rng(4)
+    ms = rng.uniform(0.3, 1.0, size=size)
+    ms[0, 3:5, 3:6] = 0.0
+    lex = 1.0 / np.maximum(ms, 0.3)
+    kw = dict(LLG, size=size)
+    spec = Spec(**kw, msat_mask=ms, lex_mask=lex)
+    y = state(kw)
+    want = Model(spec).rhs(0.0, y)
+    with Simulation(**kw, solver="rk4", dt=1e-14) as sim:
+        sim.set("msat_mask", ms)
+        sim.set("lex_mask", lex)
+        sim.set("m", y["m"])
+        k = sim.get("k")
+        assert rel_err(k, want["m"]) < 3e-5
+        assert np.all(k[:, 0, 3:5, 3:6] == 0.0)
+        E = sim.energy()
+    assert abs(E - Model(spec).energy(y)) < 1e-4 * abs(Model(spec).energy(y))
+
+
+@pytest.mark.parametrize("method", ["euler", "heun", "rk4"])
+def test_fixed_step_trajectory(cuda, method):
+    kw = dict(LLG)
+    spec, desc = pair(**kw)
+    y = state(kw, seed=9)
+    it = Integrator(Model(spec), y, method, 2e-14)
+    it.run_steps(25)
+    with Simulation(**desc, solver=method, dt=2e-14) as sim:
+        sim.set("m", y["m"])
+        sim.step(25)
+        st = sim.status()
+        m = sim.get("m")
+    assert st["steps"] == 25 and st["t"] == pytest.approx(25 * 2e-14, rel=1e-12)
+    assert np.abs(m - it.y["m"]).max() < 2e-5
+
+
+def test_rk4_smooth_4000_steps_parity(cuda):
+    """Well-conditioned thin film (uniform start, the reference's stdproblem4 geometry):
+    4000 RK4 steps of 50 fs stay within 1e-5 max|dm| of the FP64 oracle."""
+    size = (1, 32, 128)
+    kw = dict(size=size, cellsize=(3e-9, 500e-9 / 128, 125e-9 / 32), msat0T0=MS, lex=LEX,
+              gamma_ll=F.GAMMA0 / (1 + 0.02 ** 2), alpha=(0.02,) * 3, b_ext=(0.0, 4.3e-3, -24.6e-3),
+              demag=True, normalize=True)
+    spec, desc = pair(**kw)
+    m0 = np.zeros((3,) + size)
+    m0[1] = m0[2] = 1 / np.sqrt(2)
+    it = Integrator(Model(spec), {"m": m0}, "rk4", 50e-15)
+    it.run_steps(4000)
+    with Simulation(**desc, solver="rk4", dt=50e-15) as sim:
+        sim.set("m", m0)
+        sim.step(4000)
+        m = sim.get("m")
+        E = sim.energy()
+    assert np.abs(m - it.y["m"]).max() < 1e-5
+    Eo = Model(spec).energy(it.y)
+    assert abs(E - Eo) < 1e-5 * abs(Eo)
+
+
+@pytest.mark.parametrize("kw", [LLG, TTM], ids=["llg", "ttm"])
+def test_dp45_matches_oracle(cuda, kw):
+    kw = dict(kw, thermal=False)
+    spec, desc = pair(**kw)
+    y = state(kw, seed=11)
+    it = Integrator(Model(spec), y, "dp45", 1e-15, rtol=1e-4, mindt=1e-20, maxdt=1e-12)
+    t_end = 2e-13
+    it.run_until(t_end)
+    with Simulation(**desc, solver="dp45", dt=1e-15, rtol=1e-4, mindt=1e-20, maxdt=1e-12) as sim:
+        for name, v in y.items():
+            sim.set(name, v)
+        sim.run_until(t_end)
+        st = sim.status()
+        m = sim.get("m")
+        T = sim.get("Te") if kw.get("ttm") else None
+    assert st["t"] == pytest.approx(t_end, rel=1e-9)
+    assert abs(st["steps"] - it.step_count) <= max(2, it.step_count // 10)
+    assert np.abs(m - it.y["m"]).max() < 2e-4
+    if T is not None:
+        assert rel_err(T, it.y["Te"]) < 1e-4
+
+
+def test_thermal_field_statistics(cuda):
+    """Single uncoupled spins at finite T: the thermal field has zero mean and the variance
+    2 kB T lambda / (mu0 Ms V gamma dt) per component (mod_brown.go:125-145)."""
+    size = (4, 64, 64)
+    kw = dict(size=size, cellsize=(2e-9,) * 3, msat0T0=MS, gamma_ll=F.GAMMA0, alpha=(0.1, 0.1, 0.1),
+              thermal=True, seed=2, temperature=300.0, solver="rk4", dt=1e-14)
+    with Simulation(**kw) as sim:
+        m = np.zeros((3,) + size)
+        m[2] = 1.0
+        sim.set("m", m)
+        k = sim.get("k")
+    # k = gamma (H x m) + gamma lambda H with m = z: k_x = gamma (H_y + lambda H_x) ...
+    g = F.GAMMA0
+    Hz = k[2] / (g * 0.1)
+    var = F.thermal_prefactor(300.0, (2e-9,) * 3, g, 1e-14, 0.0, MS) * 0.1
+    n = Hz.size
+    assert abs(Hz.mean()) < 4 * np.sqrt(var / n)
+    assert abs(Hz.var() / var - 1) < 4 * np.sqrt(2.0 / n)
