@@ -31,6 +31,7 @@
 #include "hsb_common.cuh"
 #include "hsb_demag.h"
 #include "hsb_fft.cuh"
+#include "hsb_fft4.cuh"
 
 
 static bool is_pow2(int n) { return n >= 1 && (n & (n - 1)) == 0; }
@@ -65,17 +66,23 @@ __global__ void k_fft_x_fwd(const Real* __restrict__ in0, const Real* __restrict
     const int tid = threadIdx.x;
     const int nthr = blockDim.x;
     // load packed z[n] = x[2n] + i x[2n+1], zero beyond N2
-    for (int e = tid; e < TY * M; e += nthr) {
-        const int r = e / M;
-        const int n = e - r * M;
-        Real a = 0, b = 0;
-        if (r < ny) {
-            const int i0 = 2 * n, i1 = 2 * n + 1;
-            if (i0 < N2) { a = src[(long)r * N2 + i0]; if (msk) a *= (Real)msk[(long)r * N2 + i0]; }
-            if (i1 < N2) { b = src[(long)r * N2 + i1]; if (msk) b *= (Real)msk[(long)r * N2 + i1]; }
-        }
-        buf[r * bs + fpad(n)] = mkc(a, b);
-    }
+    batched_fill<8, C>(
+        TY * M, tid, nthr,
+        [&](int e) {
+            const int r = e / M;
+            const int n = e - r * M;
+            Real a = 0, b = 0;
+            if (r < ny) {
+                const int i0 = 2 * n, i1 = 2 * n + 1;
+                if (i0 < N2) { a = src[(long)r * N2 + i0]; if (msk) a *= (Real)msk[(long)r * N2 + i0]; }
+                if (i1 < N2) { b = src[(long)r * N2 + i1]; if (msk) b *= (Real)msk[(long)r * N2 + i1]; }
+            }
+            return mkc(a, b);
+        },
+        [&](int e, C v) {
+            const int r = e / M;
+            buf[r * bs + fpad(e - r * M)] = v;
+        });
     buf = block_fft<-1>(buf, scr, M, TY, bs, tw, twL);
     // post-process: X[k] = E[k] + W^k O[k]; write transposed, y fastest
     const int tstep = twL / L2;
@@ -117,21 +124,27 @@ __global__ void k_fft_x_inv(const float2* __restrict__ in, int ldi, int planes_p
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int tstep = twL / L2;
     // stage X[k] for k < M into smem rows as Z[k] = (X[k] + conj(X[M-k])) + i W^-k (X[k] - conj(X[M-k]))
-    for (int e = tid; e < M * TY; e += nthr) {
-        const int k = e / TY;
-        const int r = e - k * TY;
-        float2 zk = make_float2(0.f, 0.f);
-        if (r < ny) {
-            const float2 xk = in[((long)p * C2 + k) * ldi + y0 + r];
-            const float2 xc = cconj(in[((long)p * C2 + (M - k)) * ldi + y0 + r]);
-            const float2 s = cadd(xk, xc);
-            const float2 d = csub(xk, xc);
-            const float2 w = cconj(tw[k * tstep]);
-            const float2 wd = cmul(w, d);
-            zk = make_float2(s.x - wd.y, s.y + wd.x);  // s + i * wd
-        }
-        buf[r * bs + fpad(k)] = zk;
-    }
+    batched_fill<8, float2>(
+        M * TY, tid, nthr,
+        [&](int e) {
+            const int k = e / TY;
+            const int r = e - k * TY;
+            float2 zk = make_float2(0.f, 0.f);
+            if (r < ny) {
+                const float2 xk = in[((long)p * C2 + k) * ldi + y0 + r];
+                const float2 xc = cconj(in[((long)p * C2 + (M - k)) * ldi + y0 + r]);
+                const float2 s = cadd(xk, xc);
+                const float2 d = csub(xk, xc);
+                const float2 w = cconj(tw[k * tstep]);
+                const float2 wd = cmul(w, d);
+                zk = make_float2(s.x - wd.y, s.y + wd.x);  // s + i * wd
+            }
+            return zk;
+        },
+        [&](int e, float2 v) {
+            const int k = e / TY;
+            buf[(e - k * TY) * bs + fpad(k)] = v;
+        });
     buf = block_fft<+1>(buf, scr, M, TY, bs, tw, twL);
     float* out = (osel && ((*osel) ^ oinv)) ? out1 : out0;
     float* dst = out + comp * out_cstride + ((long)a0 * N1 + y0) * N2;
@@ -160,13 +173,19 @@ __global__ void k_fft_cols(const typename cplx_t<Real>::T* in, int ldi, int nin,
     const long c0 = (long)blockIdx.x * TB;
     const int nb = (int)min((long)TB, ncol - c0);
     const int tid = threadIdx.x, nthr = blockDim.x;
-    for (int e = tid; e < TB * L; e += nthr) {
-        const int b = e / L;
-        const int n = e - b * L;
-        C v = mkc((Real)0, (Real)0);
-        if (b < nb && n < nin) v = in[(c0 + b) * (long)ldi + n];
-        buf[b * bs + fpad(n)] = v;
-    }
+    batched_fill<8, C>(
+        TB * L, tid, nthr,
+        [&](int e) {
+            const int b = e / L;
+            const int n = e - b * L;
+            C v = mkc((Real)0, (Real)0);
+            if (b < nb && n < nin) v = in[(c0 + b) * (long)ldi + n];
+            return v;
+        },
+        [&](int e, C v) {
+            const int b = e / L;
+            buf[b * bs + fpad(e - b * L)] = v;
+        });
     buf = block_fft<DIR>(buf, scr, L, TB, bs, tw, twL);
     for (int e = tid; e < TB * nout; e += nthr) {
         const int b = e / nout;
@@ -196,15 +215,22 @@ __global__ void k_fft_z(typename cplx_t<Real>::T* X, int ncomp, int Nz, int L0, 
     const int nk = min(TK, L1 - k10);
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int nbatch = ncomp * TK;  // batch index = c * TK + t
-    for (int e = tid; e < ncomp * L0 * TK; e += nthr) {
-        const int t = e % TK;
-        const int rest = e / TK;
-        const int a0 = rest % L0;
-        const int c = rest / L0;
-        C v = mkc((Real)0, (Real)0);
-        if (t < nk && a0 < Nz) v = X[(((long)c * Nz + a0) * C2 + kx) * L1 + k10 + t];
-        buf[(c * TK + t) * bs + fpad(a0)] = v;
-    }
+    batched_fill<8, C>(
+        ncomp * L0 * TK, tid, nthr,
+        [&](int e) {
+            const int t = e % TK;
+            const int rest = e / TK;
+            const int a0 = rest % L0;
+            const int c = rest / L0;
+            C v = mkc((Real)0, (Real)0);
+            if (t < nk && a0 < Nz) v = X[(((long)c * Nz + a0) * C2 + kx) * L1 + k10 + t];
+            return v;
+        },
+        [&](int e, C v) {
+            const int t = e % TK;
+            const int rest = e / TK;
+            buf[((rest / L0) * TK + t) * bs + fpad(rest % L0)] = v;
+        });
     buf = block_fft<-1>(buf, scr, L0, nbatch, bs, tw, twL);
     scr = (buf == reinterpret_cast<C*>(smem_raw)) ? buf + ncomp * TK * bs : reinterpret_cast<C*>(smem_raw);
     if (conv) {
@@ -262,13 +288,19 @@ __global__ void __launch_bounds__(yz_threads<LZ>::value) k_fft_yz_conv(float2* _
     const int ncol = 3 * N0;
     float2* scr = buf + ncol * bs;
     // load columns (N1 values each, zero-padded to L1)
-    for (int e = tid; e < ncol * L1; e += nthr) {
-        const int col = e / L1;
-        const int n = e - col * L1;
-        float2 v = make_float2(0.f, 0.f);
-        if (n < N1) v = X1[((long)col * C2 + kx) * N1 + n];
-        buf[col * bs + fpad(n)] = v;
-    }
+    batched_fill<8, float2>(
+        ncol * L1, tid, nthr,
+        [&](int e) {
+            const int col = e / L1;
+            const int n = e - col * L1;
+            float2 v = make_float2(0.f, 0.f);
+            if (n < N1) v = X1[((long)col * C2 + kx) * N1 + n];
+            return v;
+        },
+        [&](int e, float2 v) {
+            const int col = e / L1;
+            buf[col * bs + fpad(e - col * L1)] = v;
+        });
     buf = block_fft<-1>(buf, scr, L1, ncol, bs, tw, twL);
     scr = (buf == reinterpret_cast<float2*>(smem_raw)) ? buf + ncol * bs : reinterpret_cast<float2*>(smem_raw);
     const int h0 = LZ / 2, h1 = L1 / 2;
@@ -314,6 +346,279 @@ __global__ void __launch_bounds__(yz_threads<LZ>::value) k_fft_yz_conv(float2* _
     }
 }
 
+// ------------------------------------------------------------------------------ fast path
+// Compile-time-sized kernels on the four-step register FFT (hsb_fft4.cuh).  Same data
+// layouts and results as the generic kernels above; selected when the lengths fit.
+
+// R2C along a2 for TY rows per block, B lanes per row; M = L2/2 packed complex points.
+template <int M>
+__global__ void __launch_bounds__(256) k_xfwd4(const float* __restrict__ in0, const float* __restrict__ in1,
+                                               const int* __restrict__ isel, int iinv,
+                                               const float* __restrict__ mask, long in_cstride,
+                                               int planes_per_comp, int N1, int N2, int ldo,
+                                               float2* __restrict__ out, const float2* __restrict__ tw, int twL,
+                                               int TY, const int* __restrict__ active) {
+    if (active && !*active) return;
+    constexpr int A = Split<M>::A, B = Split<M>::B, SS = Slot<M>::S, L2 = 2 * M, C2 = M + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int r = tid / B, lane = tid - r * B;
+    const int p = blockIdx.y;
+    const int y0 = blockIdx.x * TY;
+    const int ny = min(TY, N1 - y0);
+    const int comp = p / planes_per_comp;
+    const int a0 = p - comp * planes_per_comp;
+    const float* in = (isel && ((*isel) ^ iinv)) ? in1 : in0;
+    float2* slot = sm + r * SS;
+    float2 v[A];
+    {
+        const long row = ((long)a0 * N1 + y0 + r) * N2;
+        const float* src = in + comp * in_cstride + row;
+        const float* msk = mask ? mask + row : nullptr;
+        const bool even = (N2 & 1) == 0;
+#pragma unroll
+        for (int n1 = 0; n1 < A; n1++) {
+            const int n = B * n1 + lane;
+            float a = 0.f, b = 0.f;
+            if (r < ny && 2 * n < N2) {
+                if (even) {
+                    const float2 t = __ldg(reinterpret_cast<const float2*>(src) + n);
+                    a = t.x;
+                    b = t.y;
+                    if (msk) {
+                        const float2 q = __ldg(reinterpret_cast<const float2*>(msk) + n);
+                        a *= q.x;
+                        b *= q.y;
+                    }
+                } else {
+                    a = __ldg(src + 2 * n);
+                    if (msk) a *= __ldg(msk + 2 * n);
+                    if (2 * n + 1 < N2) {
+                        b = __ldg(src + 2 * n + 1);
+                        if (msk) b *= __ldg(msk + 2 * n + 1);
+                    }
+                }
+            }
+            v[n1] = make_float2(a, b);
+        }
+    }
+    fft4<M, -1>(v, slot, lane, tw, twL);
+    // natural order Z[k] into the slot
+#pragma unroll
+    for (int j = 0; j < A; j++) slot[fft4_out_index<M>(lane, j)] = v[j];
+    __syncwarp();
+    // X[k] = E[k] + W^k O[k], k = lane + B j (and k = M on lane 0)
+    const int ts = twL / L2;
+#pragma unroll
+    for (int j = 0; j < A; j++) {
+        const int k = lane + B * j;
+        const float2 zk = slot[k];
+        const float2 zc0 = slot[(M - k) & (M - 1)];
+        const float2 zc = make_float2(zc0.x, -zc0.y);
+        const float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+        const float2 od = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
+        const float2 w = __ldg(&tw[k * ts]);
+        v[j] = make_float2(ev.x + w.x * od.x - w.y * od.y, ev.y + w.x * od.y + w.y * od.x);
+    }
+    float2 xm = make_float2(0.f, 0.f);
+    if (lane == 0) {
+        const float2 z0 = slot[0];  // X[M] = E[0] - O[0]
+        xm = make_float2(z0.x - z0.y, 0.f);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < A; j++) slot[lane + B * j] = v[j];
+    if (lane == 0) slot[M] = xm;
+    __syncthreads();
+    for (int e = tid; e < C2 * TY; e += nthr) {
+        const int rr = e % TY, kx = e / TY;
+        if (rr < ny) out[((long)p * C2 + kx) * ldo + y0 + rr] = sm[rr * SS + kx];
+    }
+}
+
+// C2R along a2 with transposed input; writes the first N2 reals times `scale`.
+template <int M>
+__global__ void __launch_bounds__(256) k_xinv4(const float2* __restrict__ in, int ldi, int planes_per_comp, int N1,
+                                               int N2, float* __restrict__ out0, float* __restrict__ out1,
+                                               const int* __restrict__ osel, int oinv, long out_cstride,
+                                               float scale, const float2* __restrict__ tw, int twL, int TY,
+                                               const int* __restrict__ active) {
+    if (active && !*active) return;
+    constexpr int A = Split<M>::A, B = Split<M>::B, SS = Slot<M>::S, L2 = 2 * M, C2 = M + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int r = tid / B, lane = tid - r * B;
+    const int p = blockIdx.y;
+    const int y0 = blockIdx.x * TY;
+    const int ny = min(TY, N1 - y0);
+    const int comp = p / planes_per_comp;
+    const int a0 = p - comp * planes_per_comp;
+    batched_fill<8, float2>(
+        C2 * TY, tid, nthr,
+        [&](int e) {
+            const int rr = e % TY, kx = e / TY;
+            return rr < ny ? in[((long)p * C2 + kx) * ldi + y0 + rr] : make_float2(0.f, 0.f);
+        },
+        [&](int e, float2 v) { sm[(e % TY) * SS + e / TY] = v; });
+    __syncthreads();
+    float2* slot = sm + r * SS;
+    const int ts = twL / L2;
+    float2 v[A];
+#pragma unroll
+    for (int n1 = 0; n1 < A; n1++) {
+        // Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k]),  k = lane + B n1
+        const int k = lane + B * n1;
+        const float2 xk = slot[k];
+        const float2 xc0 = slot[M - k];
+        const float2 xc = make_float2(xc0.x, -xc0.y);
+        const float2 sA = make_float2(xk.x + xc.x, xk.y + xc.y);
+        const float2 d = make_float2(xk.x - xc.x, xk.y - xc.y);
+        const float2 w0 = __ldg(&tw[k * ts]);
+        const float2 w = make_float2(w0.x, -w0.y);
+        const float2 wd = make_float2(w.x * d.x - w.y * d.y, w.x * d.y + w.y * d.x);
+        v[n1] = make_float2(sA.x - wd.y, sA.y + wd.x);
+    }
+    __syncwarp();
+    fft4<M, +1>(v, slot, lane, tw, twL);
+    float* out = (osel && ((*osel) ^ oinv)) ? out1 : out0;
+    if (r < ny) {
+        float* dst = out + comp * out_cstride + ((long)a0 * N1 + y0 + r) * N2;
+        const bool even = (N2 & 1) == 0;
+#pragma unroll
+        for (int j = 0; j < A; j++) {
+            const int n = fft4_out_index<M>(lane, j);
+            if (2 * n < N2) {
+                if (even) {
+                    reinterpret_cast<float2*>(dst)[n] = make_float2(scale * v[j].x, scale * v[j].y);
+                } else {
+                    dst[2 * n] = scale * v[j].x;
+                    if (2 * n + 1 < N2) dst[2 * n + 1] = scale * v[j].y;
+                }
+            }
+        }
+    }
+}
+
+// Fused y FFT + z FFT + symmetric tensor multiply + inverse z + inverse y for one kx column;
+// 3*N0 sequences of length L1 (B lanes each), z in registers (LZ = L0 <= 16).
+template <int L1, int LZ>
+__global__ void __launch_bounds__(384) k_yz4(float2* __restrict__ X1, int N0, int N1, int C2,
+                                             const float* __restrict__ kern, const float2* __restrict__ tw,
+                                             int twL, const int* __restrict__ active) {
+    if (active && !*active) return;
+    constexpr int A = Split<L1>::A, B = Split<L1>::B, SS = Slot<L1>::S;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int col = tid / B, lane = tid - col * B;
+    const int ncol = 3 * N0;
+    const int kx = blockIdx.x;
+    float2* slot = sm + col * SS;
+    // lanes that exist in this thread's warp (the block may end with a partial warp)
+    const int wbase = tid & ~31;
+    const unsigned wmask = (nthr - wbase >= 32) ? 0xffffffffu : ((1u << (nthr - wbase)) - 1u);
+    (void)ncol;
+    float2 v[A];
+    const float2* src = X1 + ((long)col * C2 + kx) * N1;
+#pragma unroll
+    for (int n1 = 0; n1 < A; n1++) {
+        const int n = B * n1 + lane;
+        v[n1] = (n < N1) ? src[n] : make_float2(0.f, 0.f);
+    }
+    fft4<L1, -1>(v, slot, lane, tw, twL, wmask);
+#pragma unroll
+    for (int j = 0; j < A; j++) slot[fft4_out_index<L1>(lane, j)] = v[j];
+    __syncthreads();
+    const int h0 = LZ / 2, h1 = L1 / 2;
+    for (int k1 = tid; k1 < L1; k1 += nthr) {
+        float2 w[3][LZ];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int z = 0; z < LZ; z++) w[c][z] = (z < N0) ? sm[(c * N0 + z) * SS + k1] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int c = 0; c < 3; c++) fft_reg64<LZ, -1>(w[c]);
+        const int f1 = k1 > h1 ? L1 - k1 : k1;
+        const float s1 = k1 > h1 ? -1.f : 1.f;
+        const float* Kb = kern + ((long)kx * (h1 + 1) + f1) * (h0 + 1) * 6;
+#pragma unroll
+        for (int k0 = 0; k0 < LZ; k0++) {
+            const int f0 = k0 > h0 ? LZ - k0 : k0;
+            const float s0 = k0 > h0 ? -1.f : 1.f;
+            const float* K = Kb + f0 * 6;
+            const float kxx = __ldg(K + KXX), kyy = __ldg(K + KYY), kzz = __ldg(K + KZZ);
+            const float kyz = s1 * __ldg(K + KYZ), kxz = s0 * __ldg(K + KXZ), kxy = s0 * s1 * __ldg(K + KXY);
+            const float2 m0 = w[0][k0], m1 = w[1][k0], m2 = w[2][k0];
+            w[0][k0] = make_float2(kxx * m0.x + kxy * m1.x + kxz * m2.x, kxx * m0.y + kxy * m1.y + kxz * m2.y);
+            w[1][k0] = make_float2(kxy * m0.x + kyy * m1.x + kyz * m2.x, kxy * m0.y + kyy * m1.y + kyz * m2.y);
+            w[2][k0] = make_float2(kxz * m0.x + kyz * m1.x + kzz * m2.x, kxz * m0.y + kyz * m1.y + kzz * m2.y);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) fft_reg64<LZ, +1>(w[c]);
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int z = 0; z < LZ; z++)
+                if (z < N0) sm[(c * N0 + z) * SS + k1] = w[c][z];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int n1 = 0; n1 < A; n1++) v[n1] = slot[B * n1 + lane];
+    __syncwarp(wmask);
+    fft4<L1, +1>(v, slot, lane, tw, twL, wmask);
+    float2* dst = X1 + ((long)col * C2 + kx) * N1;
+#pragma unroll
+    for (int j = 0; j < A; j++) {
+        const int n = fft4_out_index<L1>(lane, j);
+        if (n < N1) dst[n] = v[j];
+    }
+}
+
+// Dispatch tables for the fast kernels.
+typedef void (*xfwd4_fn)(const float*, const float*, const int*, int, const float*, long, int, int, int, int,
+                         float2*, const float2*, int, int, const int*);
+typedef void (*xinv4_fn)(const float2*, int, int, int, int, float*, float*, const int*, int, long, float,
+                         const float2*, int, int, const int*);
+typedef void (*yz4_fn)(float2*, int, int, int, const float*, const float2*, int, const int*);
+
+static xfwd4_fn xfwd4_for(int M, int* B, int* S) {
+    switch (M) {
+#define XF(m) case m: *B = Split<m>::B; *S = Slot<m>::S; return k_xfwd4<m>;
+        XF(8) XF(16) XF(32) XF(64) XF(128) XF(256) XF(512) XF(1024)
+#undef XF
+    }
+    return nullptr;
+}
+static xinv4_fn xinv4_for(int M) {
+    switch (M) {
+#define XI(m) case m: return k_xinv4<m>;
+        XI(8) XI(16) XI(32) XI(64) XI(128) XI(256) XI(512) XI(1024)
+#undef XI
+    }
+    return nullptr;
+}
+template <int L1>
+static yz4_fn yz4_for_z(int LZ) {
+    switch (LZ) {
+        case 1: return k_yz4<L1, 1>;
+        case 2: return k_yz4<L1, 2>;
+        case 4: return k_yz4<L1, 4>;
+        case 8: return k_yz4<L1, 8>;
+        case 16: return k_yz4<L1, 16>;
+    }
+    return nullptr;
+}
+static yz4_fn yz4_for(int L1, int LZ, int* B, int* S) {
+    switch (L1) {
+#define YZ(l) case l: *B = Split<l>::B; *S = Slot<l>::S; return yz4_for_z<l>(LZ);
+        YZ(16) YZ(32) YZ(64) YZ(128) YZ(256) YZ(512) YZ(1024)
+#undef YZ
+    }
+    return nullptr;
+}
+
 // ------------------------------------------------------------------------------ extract
 // Real part of the folded octant of one transformed component, scaled, into kern.
 __global__ void k_extract(const double2* __restrict__ X, int L0, int C2, int L1, int comp,
@@ -351,6 +656,11 @@ struct hsb_demag_plan_s {
     double kern_max_real;
     int smem_x, smem_xi, smem_yz, smem_y, smem_z;
     int TYx, TYxi, TBy, TKz;
+    // four-step fast path (null when the lengths are outside its instantiations)
+    xfwd4_fn xfwd4;
+    xinv4_fn xinv4;
+    yz4_fn yz4;
+    int x4_rows, x4_threads, x4_smem, yz4_threads, yz4_smem;
 };
 
 // Largest power-of-two tile (<= cap) whose ping-pong buffers of `per_item` padded complex
@@ -479,20 +789,20 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
         P->pbc[a] = pbc[a];
         P->cs[a] = cellsize[a];
         if (size[a] < 1 || cellsize[a] <= 0 || pbc[a] < 0) {
-            free(P);
             hsb_set_error("hsb_demag_plan_create: bad size/cellsize/pbc on axis %d", a);
+            free(P);
             return HSB_ERR_INVALID;
         }
         P->L[a] = (size[a] > 1 && pbc[a] == 0) ? 2 * size[a] : size[a];
         if (!is_pow2(P->L[a])) {
-            free(P);
             hsb_set_error("hsb_demag_plan_create: padded size %d on axis %d is not a power of two", P->L[a], a);
+            free(P);
             return HSB_ERR_UNSUPPORTED;
         }
     }
     if (P->L[2] < 2 || P->L[0] > 4096 || P->L[1] > 4096 || P->L[2] > 8192) {
-        free(P);
         hsb_set_error("hsb_demag_plan_create: padded size (%d,%d,%d) outside 2..4096 (a2 >= 2)", P->L[0], P->L[1], P->L[2]);
+        free(P);
         return HSB_ERR_UNSUPPORTED;
     }
     const int N0 = P->N[0], N1 = P->N[1], L0 = P->L[0], L1 = P->L[1], L2 = P->L[2];
@@ -543,6 +853,28 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
         P->smem_z = 2 * 3 * P->TKz * fpad_len(L0) * (int)sizeof(float2);
         PTRY(cudaFuncSetAttribute(k_fft_z<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_z));
     }
+    {
+        // four-step kernels for the FP32 convolution when the lengths fit
+        int B = 0, S = 0;
+        xfwd4_fn xf = xfwd4_for(M, &B, &S);
+        if (xf && B > 0) {
+            P->xfwd4 = xf;
+            P->xinv4 = xinv4_for(M);
+            P->x4_rows = 256 / B;
+            P->x4_threads = 256;
+            P->x4_smem = P->x4_rows * S * (int)sizeof(float2);
+            PTRY(cudaFuncSetAttribute(P->xfwd4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->x4_smem));
+            PTRY(cudaFuncSetAttribute(P->xinv4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->x4_smem));
+        }
+        int By = 0, Sy = 0;
+        yz4_fn yf = (L0 <= 16) ? yz4_for(L1, L0, &By, &Sy) : nullptr;
+        if (yf && 3 * N0 * By <= 384 && 3 * N0 * Sy * (int)sizeof(float2) <= 110 * 1024) {
+            P->yz4 = yf;
+            P->yz4_threads = 3 * N0 * By;
+            P->yz4_smem = 3 * N0 * Sy * (int)sizeof(float2);
+            PTRY(cudaFuncSetAttribute(P->yz4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->yz4_smem));
+        }
+    }
 #undef PTRY
     rc = build_kernel_spectrum(P, accuracy, st);
     if (rc != HSB_OK) {
@@ -563,7 +895,7 @@ HSB_EXPORT int hsb_demag_plan_destroy(hsb_demag_plan P) {
     return HSB_OK;
 }
 
-int hsb_demag_nlaunch(hsb_demag_plan P) { return P ? (P->fused ? 3 : 5) : 0; }
+int hsb_demag_nlaunch(hsb_demag_plan P) { return P ? ((P->yz4 || P->fused) ? 3 : 5) : 0; }
 
 HSB_EXPORT int hsb_demag_plan_info(hsb_demag_plan P, int* logic, int* fused, double* max_imag) {
     if (!P) return HSB_ERR_INVALID;
@@ -581,11 +913,19 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     const int C2 = P->C2;
     const long ncell = (long)N0 * N1 * N2;
     if (io.ev) cudaEventRecord(io.ev[0], st);
-    dim3 gx(hsb_div_up(N1, P->TYx), 3 * N0);
-    k_fft_x_fwd<float><<<gx, XTHREADS, P->smem_x, st>>>(io.m[0], io.m[1], io.msel, io.minv, mask, ncell, N0, N1, N2, L2, N1, P->X1, P->tw,
-                                                                P->twL, P->TYx, active);
+    if (P->xfwd4) {
+        dim3 gx(hsb_div_up(N1, P->x4_rows), 3 * N0);
+        P->xfwd4<<<gx, P->x4_threads, P->x4_smem, st>>>(io.m[0], io.m[1], io.msel, io.minv, mask, ncell, N0, N1, N2,
+                                                        N1, P->X1, P->tw, P->twL, P->x4_rows, active);
+    } else {
+        dim3 gx(hsb_div_up(N1, P->TYx), 3 * N0);
+        k_fft_x_fwd<float><<<gx, XTHREADS, P->smem_x, st>>>(io.m[0], io.m[1], io.msel, io.minv, mask, ncell, N0, N1,
+                                                            N2, L2, N1, P->X1, P->tw, P->twL, P->TYx, active);
+    }
     if (io.ev) cudaEventRecord(io.ev[1], st);
-    if (P->fused) {
+    if (P->yz4) {
+        P->yz4<<<C2, P->yz4_threads, P->yz4_smem, st>>>(P->X1, N0, N1, C2, P->kern, P->tw, P->twL, active);
+    } else if (P->fused) {
         switch (P->lz) {
 #define RUNYZ(LZ) case LZ: k_fft_yz_conv<LZ><<<C2, yz_threads<LZ>::value, P->smem_yz, st>>>(P->X1, N0, N1, L1, C2, P->kern, P->tw, P->twL, active); break;
             RUNYZ(1) RUNYZ(2) RUNYZ(4) RUNYZ(8) RUNYZ(16)
@@ -602,10 +942,15 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
             P->X2, L1, L1, P->X1, N1, N1, L1, ncol, P->tw, P->twL, P->TBy, active);
     }
     if (io.ev) cudaEventRecord(io.ev[2], st);
-    dim3 gi(hsb_div_up(N1, P->TYxi), 3 * N0);
-    k_fft_x_inv<<<gi, XTHREADS, P->smem_xi, st>>>(P->X1, N1, N0, N1, N2, L2, io.h[0], io.h[1], io.hsel, io.hinv,
-                                                  ncell, ms0, P->tw, P->twL,
-                                                         P->TYxi, active);
+    if (P->xinv4) {
+        dim3 gi(hsb_div_up(N1, P->x4_rows), 3 * N0);
+        P->xinv4<<<gi, P->x4_threads, P->x4_smem, st>>>(P->X1, N1, N0, N1, N2, io.h[0], io.h[1], io.hsel, io.hinv,
+                                                        ncell, ms0, P->tw, P->twL, P->x4_rows, active);
+    } else {
+        dim3 gi(hsb_div_up(N1, P->TYxi), 3 * N0);
+        k_fft_x_inv<<<gi, XTHREADS, P->smem_xi, st>>>(P->X1, N1, N0, N1, N2, L2, io.h[0], io.h[1], io.hsel, io.hinv,
+                                                      ncell, ms0, P->tw, P->twL, P->TYxi, active);
+    }
     if (io.ev) cudaEventRecord(io.ev[3], st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

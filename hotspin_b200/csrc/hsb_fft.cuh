@@ -26,6 +26,26 @@ template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
 template <typename C> __device__ __forceinline__ C cconj(C a) { return mkc(a.x, -a.y); }
 template <typename C, typename R> __device__ __forceinline__ C cscale(C a, R s) { return mkc(a.x * s, a.y * s); }
 
+// Global -> shared fill with UB independent loads in flight per thread: load UB elements
+// into registers, then store them (a load followed directly by its dependent store would
+// expose the full memory latency once per element).
+template <int UB, typename T, typename LD, typename ST>
+__device__ __forceinline__ void batched_fill(int total, int tid, int nthr, LD ld, ST st) {
+    for (int base = tid; base < total; base += nthr * UB) {
+        T v[UB];
+#pragma unroll
+        for (int u = 0; u < UB; u++) {
+            const int e = base + u * nthr;
+            if (e < total) v[u] = ld(e);
+        }
+#pragma unroll
+        for (int u = 0; u < UB; u++) {
+            const int e = base + u * nthr;
+            if (e < total) st(e, v[u]);
+        }
+    }
+}
+
 // shared-memory index padding: one spare slot every 16 complex elements
 __host__ __device__ __forceinline__ int fpad(int i) { return i + (i >> 4); }
 __host__ __device__ __forceinline__ int fpad_len(int n) { return n + (n >> 4) + 1; }

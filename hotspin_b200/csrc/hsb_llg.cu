@@ -5,7 +5,8 @@
 //   H_eff = H_ex (exchange6.cu:11-127) + H_anis (uniaxialanisotropy.cu:12-52)
 //         + B_ext/mu0 (mod_zeeman.go) + H_demag (input) + H_lf (long_field.cu:13-72)
 //         + H_therm (temperature.cu:14-70 on Philox normals)
-//   dm/dt = gamma (H x m) + gamma diag(lambda) H   (llbar-torque.cu, llbar-local00nc.cu)
+//   dm/dt = gamma (m x H) + gamma diag(lambda) H   (llbar-torque.cu computes cross(H, M)
+//           with the reference's cross helper, which evaluates m x H; llbar-local00nc.cu)
 //   dTe/dt = (ke lap Te + G (Tl - Te) + Q_laser) / (gamma_e Te),
 //   dTl/dt = (kl lap Tl + G (Te - Tl)) / Cl       (Qspat.cu, Qinter.cu, div.cu, mod_ce.go)
 // and then performs the stage arithmetic of the integrator (store k_s, form the next stage
@@ -27,8 +28,11 @@ __device__ __forceinline__ float* resolve(const PtrSel& s, const HsbSolverDev* s
     }
 }
 
-// B_J(x) and B_J'(x) with the reference's 4-term series below the linear range
-// (common_func.h:72-120); Langevin L(x), L'(x) for classical spins (common_func.h:122-138).
+// B_J(x) and B_J'(x) (common_func.h:72-138): the reference's 4-term series below the linear
+// range; above it the same functions in forms that stay accurate in FP32:
+// B_1/2 = tanh x, B_1/2' = 1/cosh^2 x; B_J' = l^2/sinh^2(l x) - g^2/sinh^2(g x), which equals
+// the reference's (g^2 - l^2) + l^2 coth^2(l x) - g^2 coth^2(g x) without its cancellation;
+// Langevin L = coth x - 1/x, L' = 1/x^2 - 1/sinh^2 x.
 __device__ __forceinline__ void mfa_w(const HsbPhys& P, float x, float& W, float& dW) {
     if (P.lf_langevin) {
         if (fabsf(x) < 0.2f) {
@@ -36,9 +40,9 @@ __device__ __forceinline__ void mfa_w(const HsbPhys& P, float x, float& W, float
             W = x / 3.0f - x * x2 / 45.0f + x * x2 * x2 * 2.0f / 945.0f - x * x2 * x2 * x2 / 4725.0f;
             dW = 1.0f / 3.0f - x2 / 15.0f + x2 * x2 * 2.0f / 189.0f - x2 * x2 * x2 / 675.0f;
         } else {
-            const float c = 1.0f / tanhf(x);
-            W = c - 1.0f / x;
-            dW = 1.0f - c * c + 1.0f / (x * x);
+            const float sh = sinhf(x);
+            W = 1.0f / tanhf(x) - 1.0f / x;
+            dW = 1.0f / (x * x) - 1.0f / (sh * sh);
         }
         return;
     }
@@ -50,10 +54,14 @@ __device__ __forceinline__ void mfa_w(const HsbPhys& P, float x, float& W, float
             (g8 - l8) * x * x2 * x2 * x2 / 4725.0f;
         dW = (g2 - l2) / 3.0f - (g4 - l4) * x2 / 15.0f + (g6 - l6) * x2 * x2 * 2.0f / 189.0f -
              (g8 - l8) * x2 * x2 * x2 / 675.0f;
+    } else if (l == 1.0f && g == 2.0f) {
+        const float c = coshf(x);
+        W = tanhf(x);
+        dW = 1.0f / (c * c);
     } else {
-        const float cg = 1.0f / tanhf(g * x), cl = 1.0f / tanhf(l * x);
-        W = g * cg - l * cl;
-        dW = (g * g - l * l) + l * l * cl * cl - g * g * cg * cg;
+        const float sg = sinhf(g * x), sl = sinhf(l * x);
+        W = g / tanhf(g * x) - l / tanhf(l * x);
+        dW = (l * l) / (sl * sl) - (g * g) / (sg * sg);
     }
 }
 
@@ -143,7 +151,7 @@ __device__ __forceinline__ void rhs_cell(const HsbPhys& P, const float* __restri
             for (int c = 0; c < 3; c++) H[c] += amp * sqrtf(P.lam[c]) * g[c];
         }
     }
-    // ---- LLBar torque + zero-order local relaxation (zero in vacuum)
+    // ---- LLBar torque cross(H, m) = m x H + zero-order local relaxation (zero in vacuum)
     if (ms == 0.f) {
         k[0] = k[1] = k[2] = 0.f;
     } else {
@@ -282,6 +290,298 @@ __global__ void __launch_bounds__(256) k_stage(const HsbPhys P, const StageArgs 
     if (bad) atomicOr(&sd->nonfinite, 1u);
 }
 
+// ------------------------------------------------------------------ 4-cell vector variant
+// Same arithmetic as k_stage, four consecutive cells along a2 per thread with 16-byte loads
+// and stores (N2 % 4 == 0, no per-cell masks).  Neighbours along a0/a1 are float4 loads of
+// the adjacent rows; along a2 the two outer neighbours are scalar loads (L1 hits).
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ void st4(float* p, const float v[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void un4(float4 a, float v[4]) {
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = a.z;
+    v[3] = a.w;
+}
+
+template <int CH>
+__global__ void __launch_bounds__(256, 2) k_stage4(const HsbPhys P, const StageArgs A, HsbSolverDev* sd) {
+    if (!A.ungated && !sd->active) return;
+    const double t = sd->t;
+    const double dt = sd->dt;
+    const long long step = sd->step;
+    const float* ys = resolve(A.ys, sd);
+    const float* hd = resolve(A.hd, sd);
+    const float* yth = resolve(A.ytherm, sd);
+    float* kout = resolve(A.kout, sd);
+    const float* kacc = resolve(A.kacc, sd);
+    float* ynext = resolve(A.ynext, sd);
+    const float* ybase = resolve(A.ybase, sd);
+    const float* yerr0 = resolve(A.yerr0, sd);
+    const double ts = t + (double)A.tfrac * dt;
+    const float fdt = (float)dt;
+    const long n = P.ncell;
+    const long s1 = P.N2, s0 = (long)P.N1 * P.N2;
+    const long ngroups = n >> 2;
+    // per-launch constants
+    const double dte = dt > P.cutoff_dt ? dt : P.cutoff_dt;
+    const float th_amp = (float)(P.th_pre / dte);
+    float laser_t = 0.f;
+    if (CH >= 5 && P.laser_p0 != 0.f) {
+        const float tt = (float)(ts - (double)P.laser_t0);
+        laser_t = P.laser_p0 * expf(-P.laser_c * tt * tt);
+    }
+    float emax = 0.f;
+    bool bad = false;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < ngroups; g += (long)gridDim.x * blockDim.x) {
+        const long i = g << 2;
+        const int a2 = (int)(i % P.N2);
+        const long r = i / P.N2;
+        const int a1 = (int)(r % P.N1);
+        const int a0 = (int)(r / P.N1);
+        float y[CH][4];
+#pragma unroll
+        for (int c = 0; c < CH; c++) un4(ld4(ys + c * n + i), y[c]);
+        float H[3][4];
+        if (hd) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float h[4];
+                un4(ld4(hd + c * n + i), h);
+#pragma unroll
+                for (int q = 0; q < 4; q++) H[c][q] = h[q] + P.bext[c];
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) H[c][q] = P.bext[c];
+        }
+        float lapE[4] = {0.f, 0.f, 0.f, 0.f}, lapL[4] = {0.f, 0.f, 0.f, 0.f};
+        // ---- a0 / a1 neighbours: whole float4 rows
+#pragma unroll
+        for (int d = 0; d < 2; d++) {
+            const int me = d == 0 ? a0 : a1;
+            const int nn = d == 0 ? P.N0 : P.N1;
+            const int wr = d == 0 ? P.pbc0 : P.pbc1;
+            const long st = d == 0 ? s0 : s1;
+            const long im = i + (long)(nb_lo(me, nn, wr) - me) * st;
+            const long ip = i + (long)(nb_hi(me, nn, wr) - me) * st;
+            const float cx = P.ex_c[d];
+            if (cx != 0.f) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    float lo[4], hi[4];
+                    un4(ld4(ys + c * n + im), lo);
+                    un4(ld4(ys + c * n + ip), hi);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) H[c][q] += cx * ((lo[q] + hi[q]) - (y[c][q] + y[c][q]));
+                }
+            }
+            if (CH >= 5) {
+                if (P.ke_c[d] != 0.f) {
+                    float lo[4], hi[4];
+                    un4(ld4(ys + 3 * n + im), lo);
+                    un4(ld4(ys + 3 * n + ip), hi);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) lapE[q] += P.ke_c[d] * ((lo[q] + hi[q]) - (y[3][q] + y[3][q]));
+                }
+                if (P.kl_c[d] != 0.f) {
+                    float lo[4], hi[4];
+                    un4(ld4(ys + 4 * n + im), lo);
+                    un4(ld4(ys + 4 * n + ip), hi);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) lapL[q] += P.kl_c[d] * ((lo[q] + hi[q]) - (y[4][q] + y[4][q]));
+                }
+            }
+        }
+        // ---- a2 neighbours: inside the vector plus one scalar on each side
+        {
+            const long il = i + (long)(nb_lo(a2, P.N2, P.pbc2) - a2);
+            const long ir = (i + 3) + (long)(nb_hi(a2 + 3, P.N2, P.pbc2) - (a2 + 3));
+            const int nst = CH >= 5 ? 5 : 3;
+#pragma unroll
+            for (int c = 0; c < nst; c++) {
+                const float cx = c < 3 ? P.ex_c[2] : (c == 3 ? P.ke_c[2] : P.kl_c[2]);
+                if (cx == 0.f) continue;
+                const float l = __ldg(ys + c * n + il), rr = __ldg(ys + c * n + ir);
+                float v[4];
+                v[0] = cx * ((l + y[c][1]) - (y[c][0] + y[c][0]));
+                v[1] = cx * ((y[c][0] + y[c][2]) - (y[c][1] + y[c][1]));
+                v[2] = cx * ((y[c][1] + y[c][3]) - (y[c][2] + y[c][2]));
+                v[3] = cx * ((y[c][2] + rr) - (y[c][3] + y[c][3]));
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    if (c < 3) H[c][q] += v[q];
+                    else if (c == 3) lapE[q] += v[q];
+                    else lapL[q] += v[q];
+                }
+            }
+        }
+        float thT[4] = {P.T_uniform, P.T_uniform, P.T_uniform, P.T_uniform};
+        if (CH >= 5 && P.thermal) un4(ld4(yth + 3 * n + i), thT);
+        float k[CH][4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float mx = y[0][q], my = y[1][q], mz = y[2][q];
+            float hx = H[0][q], hy = H[1][q], hz = H[2][q];
+            if (P.ku_pre != 0.f) {
+                const float mu = mx * P.uhat[0] + my * P.uhat[1] + mz * P.uhat[2];
+                hx += P.ku_pre * mu * P.u[0];
+                hy += P.ku_pre * mu * P.u[1];
+                hz += P.ku_pre * mu * P.u[2];
+            }
+            const float Ts = (CH >= 5) ? y[3][q] : P.T_uniform;
+            if (P.llb) {
+                const float am = sqrtf(mx * mx + my * my + mz * mz);
+                if (am > 1e-30f && Ts > 0.f) {
+                    const float b = P.lf_b / Ts;
+                    float W, dW;
+                    mfa_w(P, am * b, W, dW);
+                    const float mult = P.lf_pre * Ts * (W - am) / dW / am;
+                    hx += mult * mx;
+                    hy += mult * my;
+                    hz += mult * mz;
+                }
+            }
+            if (P.thermal && thT[q] > 0.f) {
+                const float amp = sqrtf(th_amp * thT[q]);
+                float gg[3];
+                philox_normals3((uint32_t)(i + q), (uint64_t)step, P.seed_lo, P.seed_hi, gg);
+                hx += amp * sqrtf(P.lam[0]) * gg[0];
+                hy += amp * sqrtf(P.lam[1]) * gg[1];
+                hz += amp * sqrtf(P.lam[2]) * gg[2];
+            }
+            const float gm = P.gamma;
+            k[0][q] = gm * (-hy * mz + hz * my) + gm * P.lam[0] * hx;
+            k[1][q] = gm * (-hz * mx + hx * mz) + gm * P.lam[1] * hy;
+            k[2][q] = gm * (-hx * my + hy * mx) + gm * P.lam[2] * hz;
+            if (CH >= 5) {
+                const float Te = y[3][q], Tl = y[4][q];
+                float Qe = lapE[q] + P.g_ep * (Tl - Te);
+                if (laser_t != 0.f) {
+                    float q2 = laser_t;
+                    if (P.laser_inv2s2 != 0.f) {
+                        const float yy = ((float)a1 + 0.5f - 0.5f * (float)P.N1) * P.cs1;
+                        const float xx = ((float)(a2 + q) + 0.5f - 0.5f * (float)P.N2) * P.cs2;
+                        q2 *= expf(-(xx * xx + yy * yy) * P.laser_inv2s2);
+                    }
+                    Qe += q2;
+                }
+                const float Ce = P.gamma_e * Te;
+                k[3][q] = (Ce == 0.f) ? 0.f : Qe / Ce;
+                const float Ql = lapL[q] + P.g_ep * (Te - Tl);
+                k[4][q] = (P.c_l == 0.f) ? 0.f : Ql / P.c_l;
+            }
+        }
+        if (kout) {
+#pragma unroll
+            for (int c = 0; c < CH; c++) {
+                float v[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) v[q] = A.kself_w * k[c][q];
+                if (kacc) {
+                    float a[4];
+                    un4(ld4(kacc + c * n + i), a);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) v[q] += A.kacc_w * a[q];
+                }
+                st4(kout + c * n + i, v);
+            }
+        }
+        if (ynext) {
+            float out[CH][4];
+#pragma unroll
+            for (int c = 0; c < CH; c++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) out[c][q] = A.cself * k[c][q];
+#pragma unroll
+            for (int j = 0; j < HSB_MAXK; j++) {
+                if (j < A.nk && A.ck[j] != 0.f) {
+                    const float* kj = resolve(A.kin[j], sd);
+#pragma unroll
+                    for (int c = 0; c < CH; c++) {
+                        float a[4];
+                        un4(ld4(kj + c * n + i), a);
+#pragma unroll
+                        for (int q = 0; q < 4; q++) out[c][q] += A.ck[j] * a[q];
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CH; c++) {
+                float b[4];
+                un4(ld4(ybase + c * n + i), b);
+#pragma unroll
+                for (int q = 0; q < 4; q++) out[c][q] = b[q] + fdt * out[c][q];
+            }
+            if (A.normalize) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const float l2 = out[0][q] * out[0][q] + out[1][q] * out[1][q] + out[2][q] * out[2][q];
+                    const float inv = (l2 == 0.f) ? 0.f : rsqrtf(l2);
+                    out[0][q] *= inv;
+                    out[1][q] *= inv;
+                    out[2][q] *= inv;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CH; c++) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) bad |= !isfinite(out[c][q]);
+                st4(ynext + c * n + i, out[c]);
+            }
+        }
+        if (A.err) {
+            float e[CH][4];
+#pragma unroll
+            for (int c = 0; c < CH; c++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) e[c][q] = A.ceself * k[c][q];
+#pragma unroll
+            for (int j = 0; j < HSB_MAXK; j++) {
+                if (A.ce[j] != 0.f) {
+                    const float* kj = resolve(A.kin[j], sd);
+#pragma unroll
+                    for (int c = 0; c < CH; c++) {
+                        float a[4];
+                        un4(ld4(kj + c * n + i), a);
+#pragma unroll
+                        for (int q = 0; q < 4; q++) e[c][q] += A.ce[j] * a[q];
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                float em = fmaxf(fabsf(e[0][q]), fmaxf(fabsf(e[1][q]), fabsf(e[2][q]))) * fdt / A.rtol;
+                if (!(em == em)) bad = true;
+                emax = fmaxf(emax, em);
+            }
+            if (CH >= 5) {
+#pragma unroll
+                for (int c = 3; c < CH; c++) {
+                    float y0v[4];
+                    un4(ld4(yerr0 + c * n + i), y0v);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float sc = A.rtol * fmaxf(fabsf(y0v[q]), fabsf(y[c][q]));
+                        const float ec = fabsf(e[c][q]) * fdt;
+                        const float em = sc > 0.f ? ec / sc : (ec > 0.f ? INFINITY : 0.f);
+                        if (!(em == em)) bad = true;
+                        emax = fmaxf(emax, em);
+                    }
+                }
+            }
+        }
+    }
+    if (A.err) {
+        emax = warp_max_f(emax);
+        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&sd->err_acc, emax);
+    }
+    if (bad) atomicOr(&sd->nonfinite, 1u);
+}
+
 // Next stage point / new state without a right-hand-side evaluation:
 // ynext = ybase + dt * sum_j ck[j] kin[j] (renormalised in LLG mode).
 template <int CH>
@@ -374,6 +674,12 @@ __global__ void k_fixed_advance(HsbSolverDev* sd) {
 // ------------------------------------------------------------------------------ launchers
 int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st) {
     const int threads = 256;
+    if (P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask) {
+        const int grid = hsb_grid_1d(P.ncell / 4, threads, 2);
+        if (P.nch == 5) k_stage4<5><<<grid, threads, 0, st>>>(P, A, sd);
+        else k_stage4<3><<<grid, threads, 0, st>>>(P, A, sd);
+        return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+    }
     const int grid = hsb_grid_1d(P.ncell, threads, 8);
     if (P.nch == 5) k_stage<5><<<grid, threads, 0, st>>>(P, A, sd);
     else k_stage<3><<<grid, threads, 0, st>>>(P, A, sd);

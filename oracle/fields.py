@@ -106,15 +106,22 @@ def uniaxial_anisotropy(m, ku_mask, msat_mask, ku_mul, msat_mul, u_mask, u_mul):
     return np.where(msat == 0.0, 0.0, h)
 
 
+def ref_cross(a, b):
+    """The reference's ``cross(a, b)`` (common_func.h:52-55), which evaluates b x a:
+    x = -a.y b.z + a.z b.y, and so on."""
+    return np.cross(b, a, axis=0)
+
+
 def llbar_torque(m, h, msat0T0_mask, gamma_ll):
-    """gamma_LL * (H x m) (llbar-torque.cu:11-45, common_func.h:52-55 cross(H, M)).
+    """gamma_LL * cross(H, M) = gamma_LL * (m x H) (llbar-torque.cu:11-45 with the
+    reference's cross helper, common_func.h:52-55).
 
     The reference kernel writes the bare cross product and sets gamma_LL as the quantity's
     multiplier (mod_llbar-torque.go:55-68); the product is applied here.  Zero in vacuum.
     """
     shape = m.shape[1:]
     ms = _mask(msat0T0_mask, shape)
-    t = np.cross(h, m, axis=0)
+    t = ref_cross(h, m)
     return np.where(ms == 0.0, 0.0, gamma_ll * t)
 
 
@@ -138,13 +145,14 @@ def llbar_local02nc(m, h, msat0T0_mask, mu_mask, mu_mul, gamma_ll):
 
 
 def llbar_local02c(m, h, msat0T0_mask, mu_mask, mu_mul, gamma_ll):
-    """gamma_LL * (diag(mu)(m x H)) x m (llbar-local02c.cu:11-69)."""
+    """gamma_LL * cross(diag(mu) cross(m, H), m) with the reference's cross helper
+    (llbar-local02c.cu:11-69, common_func.h:52-55)."""
     shape = h.shape[1:]
     ms = _mask(msat0T0_mask, shape)
     mu = np.stack([mu_mul[c] * _mask(None if mu_mask is None else mu_mask[c], shape)
                    for c in range(3)])
-    a = mu * np.cross(m, h, axis=0)
-    return np.where(ms == 0.0, 0.0, gamma_ll * np.cross(a, m, axis=0))
+    a = mu * ref_cross(m, h)
+    return np.where(ms == 0.0, 0.0, gamma_ll * ref_cross(a, m))
 
 
 def normalize(m):

@@ -6,7 +6,8 @@ describe (tests/stdproblem4-llbr-modular.py, examples/laser-demag.py):
 * H_eff = H_ex + H_anis + B_ext/mu0 + B_demag/mu0 + H_lf + H_therm
   (SumUpdater over the loaded terms: engine/update_sum.go:29-76, modules/hfield.go:19-28,
   mod_zeeman.go:23-31, mod_demag.go:56-62);
-* dm/dt = llbar_torque + llbar_local00nc = gamma_LL (H x m) + gamma_LL diag(lambda) H
+* dm/dt = llbar_torque + llbar_local00nc = gamma_LL (m x H) + gamma_LL diag(lambda) H
+  (the reference's ``cross(H, M)`` helper evaluates m x H, common_func.h:52-55)
   (modules/mod_llbar.go:29-38, llbar-torque.cu:11-45, llbar-local00nc.cu:11-63);
 * with the ``normalizer`` module (LLG mode) m is renormalised whenever it is updated, i.e.
   before every right-hand-side evaluation (mod_normalize.go:45-55, engine/quant.go:417-445);

@@ -69,7 +69,8 @@ def test_rk4_fourth_order_on_precession():
         n = int(round(4e-11 / dt))
         it.run_steps(n)
         w = spec.gamma_ll * 0.1 / fields.MU0
-        want = np.array([np.cos(w * 4e-11), np.sin(w * 4e-11)])
+        # hotspin's torque is +gamma (m x H): m precesses clockwise about +z
+        want = np.array([np.cos(w * 4e-11), -np.sin(w * 4e-11)])
         errs.append(np.abs(it.y["m"][:2, 0, 0, 0] - want).max())
     assert 12 < errs[0] / errs[1] < 20
 

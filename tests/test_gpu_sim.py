@@ -75,7 +75,7 @@ def test_rhs_matches_oracle(cuda, kw, thermal):
 
 
 def test_masks_rhs(cuda):
-    size = (2, 12, 20)
+    size = (2, 8, 16)
     rng = np.random.default_rng(4)
     ms = rng.uniform(0.3, 1.0, size=size)
     ms[0, 3:5, 3:6] = 0.0
@@ -93,6 +93,22 @@ def test_masks_rhs(cuda):
         assert np.all(k[:, 0, 3:5, 3:6] == 0.0)
         E = sim.energy()
     assert abs(E - Model(spec).energy(y)) < 1e-4 * abs(Model(spec).energy(y))
+
+
+@pytest.mark.parametrize("size", [(3, 5, 7), (2, 6, 12)])
+def test_rhs_without_demag_any_size(cuda, size):
+    """Sizes with no power-of-two padding run without demag; N2 % 4 != 0 takes the
+    one-cell-per-thread kernel, N2 % 4 == 0 the four-cell one."""
+    kw = dict(TTM, size=size, demag=False, laser_sigma=10e-9)
+    spec, desc = pair(**kw)
+    y = state(kw)
+    want = Model(spec).rhs(0.0, y)
+    with Simulation(**desc, solver="rk4", dt=1e-15) as sim:
+        for name, v in y.items():
+            sim.set(name, v)
+        k = sim.get("k")
+    assert rel_err(k[:3], want["m"]) < 3e-5
+    assert rel_err(k[3], want["Te"]) < 3e-5
 
 
 @pytest.mark.parametrize("method", ["euler", "heun", "rk4"])
