@@ -61,6 +61,7 @@ _SIGS = {
     "hsb_sim_stream": (c_vp, [c_vp]),
     "hsb_sim_profile": (c_int, [c_vp, c_int, c_dp]),
     "hsb_sim_launches_per_attempt": (c_int, [c_vp, c_ip]),
+    "hsb_average_m_noalloc": (c_int, [c_vp, c_i64, c_vp, c_vp]),
     "hsb_mfa_table": (c_int, [c_dbl, c_dbl, c_int, c_dp, c_dp, c_dp]),
     "hsb_mfa_equilibrium": (c_int, [c_dbl, c_dbl, c_dbl, c_dp]),
     "hsb_demag_profile": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_vp, c_vp, c_int, c_dp]),

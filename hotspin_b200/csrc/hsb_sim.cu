@@ -135,57 +135,7 @@ __global__ void k_f2d(const float* __restrict__ in, double* __restrict__ out, lo
         out[i] = (double)in[i];
 }
 
-// ------------------------------------------------------------------ reductions
-// Kahan-compensated FP64 block sums of up to 8 per-cell quantities, finished by the last
-// block (device-side, no host pass).  q(i) is produced by the functor.
-struct RedState {
-    unsigned int count;
-};
-
-template <int NQ>
-__device__ void block_reduce_store(double (&v)[NQ], double* partial, unsigned int* counter,
-                                   double* out, int nblocks) {
-    __shared__ double sh[NQ][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q < NQ; q++) {
-        double x = warp_sum_d(v[q]);
-        if (lane == 0) sh[q][warp] = x;
-    }
-    __syncthreads();
-    __shared__ bool last;
-    if (threadIdx.x == 0) {
-        const int nw = blockDim.x >> 5;
-        for (int q = 0; q < NQ; q++) {
-            double s = 0, c = 0;
-            for (int w = 0; w < nw; w++) {
-                double yv = sh[q][w] - c;
-                double tv = s + yv;
-                c = (tv - s) - yv;
-                s = tv;
-            }
-            partial[(long)blockIdx.x * NQ + q] = s;
-        }
-        __threadfence();
-        unsigned int done = atomicAdd(counter, 1u);
-        last = (done == (unsigned int)nblocks - 1);
-    }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        for (int q = 0; q < NQ; q++) {
-            double s = 0, c = 0;
-            for (int b = 0; b < nblocks; b++) {
-                double yv = ((volatile double*)partial)[(long)b * NQ + q] - c;
-                double tv = s + yv;
-                c = (tv - s) - yv;
-                s = tv;
-            }
-            out[q] = s;
-        }
-        *counter = 0;
-    }
-}
+#include "hsb_reduce.cuh"
 
 // Energy-density terms (mod_energy.go:20-66): per cell, with ms = msat mask,
 //   zeeman  -(m . Bext/mu0) ms          (times V mu0 Ms0)

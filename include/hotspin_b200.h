@@ -137,6 +137,16 @@ int hsb_sim_launches_per_attempt(hsb_sim sim, int* n);
 int hsb_mfa_table(double Tc, double J, int npts, double* T, double* me, double* chi);
 int hsb_mfa_equilibrium(double T, double Tc, double J, double* me);
 
+/* Average of a caller-owned FP32 SoA magnetization (3 x ncell, device memory) into
+ * caller-owned device memory avg3[3], enqueued on `stream`; the library allocates nothing.
+ * No counterpart in the reference: it is the device-finished FP64 reduction of
+ * hsb_sim_average_m for callers that own all device memory (as hotspin's Go layer does),
+ * with its scratch in a fixed static device array (about 7 KB per GPU, held until exit).
+ * ncell must be in [1, 2^28]; larger sizes are rejected.  The first call on a device
+ * resolves the scratch address (make it before any stream capture).  All calls share the
+ * scratch: calls that overlap on the GPU race and must be serialised. */
+int hsb_average_m_noalloc(const float* m, int64_t ncell, double* avg3, void* stream);
+
 /* The handle's CUDA stream (cudaStream_t) for callers that interleave their own work. */
 void* hsb_sim_stream(hsb_sim sim);
 
