@@ -62,6 +62,17 @@ _SIGS = {
     "hsb_sim_profile": (c_int, [c_vp, c_int, c_dp]),
     "hsb_sim_launches_per_attempt": (c_int, [c_vp, c_ip]),
     "hsb_average_m_noalloc": (c_int, [c_vp, c_i64, c_vp, c_vp]),
+    "hsb_batch_footprint": (c_int, [ctypes.POINTER(SimDesc), c_i32, ctypes.POINTER(c_i64)]),
+    "hsb_batch_create": (c_int, [ctypes.POINTER(SimDesc), c_i32, ctypes.POINTER(c_vp)]),
+    "hsb_batch_destroy": (c_int, [c_vp]),
+    "hsb_batch_info": (c_int, [c_vp, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), ctypes.POINTER(c_i64)]),
+    "hsb_batch_admit": (c_int, [c_vp, c_i32, ctypes.POINTER(SimDesc), c_dp, c_dbl]),
+    "hsb_batch_launch": (c_int, [c_vp, c_i32]),
+    "hsb_batch_poll": (c_int, [c_vp, ctypes.POINTER(c_i32)]),
+    "hsb_batch_slot_status": (c_int, [c_vp, c_i32, c_dp, c_dp, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64),
+                                      ctypes.POINTER(c_i64), ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)]),
+    "hsb_batch_slot_get": (c_int, [c_vp, c_i32, ctypes.c_char_p, c_dp, c_i64]),
+    "hsb_batch_release": (c_int, [c_vp, c_i32]),
     "hsb_mfa_table": (c_int, [c_dbl, c_dbl, c_int, c_dp, c_dp, c_dp]),
     "hsb_mfa_equilibrium": (c_int, [c_dbl, c_dbl, c_dbl, c_dp]),
     "hsb_demag_profile": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_vp, c_vp, c_int, c_dp]),
@@ -113,6 +124,6 @@ def exported_symbols_from_headers():
                 continue
             if re.search(r"(typedef|#define)[^\n;]*$", pre):
                 continue
-            if re.search(r"\b(void|int|double|float|char|hsb_sim|hsb_demag_plan)\s*\**\s*$", pre):
+            if re.search(r"\b(void|int|double|float|char|hsb_sim|hsb_batch|hsb_demag_plan)\s*\**\s*$", pre):
                 names.add(name)
     return names

@@ -350,6 +350,16 @@ __global__ void __launch_bounds__(yz_threads<LZ>::value) k_fft_yz_conv(float2* _
 // Compile-time-sized kernels on the four-step register FFT (hsb_fft4.cuh).  Same data
 // layouts and results as the generic kernels above; selected when the lengths fit.
 
+// Per-slot offsets of a batched launch (slot = blockIdx.z; all zero for a single convolution).
+struct SlotStrides {
+    long in;            // floats between slots' inputs
+    long x1;            // complex elements between slots' spectra
+    long out;           // floats between slots' outputs
+    int sel;            // ints between slots' selector / active words
+    const float* scale; // per-slot output scale (null: the launch's scale)
+    int scale_stride;
+};
+
 // R2C along a2 for TY rows per block, B lanes per row; M = L2/2 packed complex points.
 template <int M>
 __global__ void __launch_bounds__(256) k_xfwd4(const float* __restrict__ in0, const float* __restrict__ in1,
@@ -357,8 +367,13 @@ __global__ void __launch_bounds__(256) k_xfwd4(const float* __restrict__ in0, co
                                                const float* __restrict__ mask, long in_cstride,
                                                int planes_per_comp, int N1, int N2, int ldo,
                                                float2* __restrict__ out, const float2* __restrict__ tw, int twL,
-                                               int TY, const int* __restrict__ active) {
-    if (active && !*active) return;
+                                               int TY, const int* __restrict__ active, const SlotStrides ss) {
+    const int sl = blockIdx.z;
+    if (active && !active[sl * ss.sel]) return;
+    in0 += sl * ss.in;
+    in1 += sl * ss.in;
+    if (isel) isel += sl * ss.sel;
+    out += sl * ss.x1;
     constexpr int A = Split<M>::A, B = Split<M>::B, SS = Slot<M>::S, L2 = 2 * M, C2 = M + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw);
@@ -443,8 +458,14 @@ __global__ void __launch_bounds__(256) k_xinv4(const float2* __restrict__ in, in
                                                int N2, float* __restrict__ out0, float* __restrict__ out1,
                                                const int* __restrict__ osel, int oinv, long out_cstride,
                                                float scale, const float2* __restrict__ tw, int twL, int TY,
-                                               const int* __restrict__ active) {
-    if (active && !*active) return;
+                                               const int* __restrict__ active, const SlotStrides ss) {
+    const int sl = blockIdx.z;
+    if (active && !active[sl * ss.sel]) return;
+    in += sl * ss.x1;
+    out0 += sl * ss.out;
+    out1 += sl * ss.out;
+    if (osel) osel += sl * ss.sel;
+    if (ss.scale) scale = ss.scale[sl * ss.scale_stride];
     constexpr int A = Split<M>::A, B = Split<M>::B, SS = Slot<M>::S, L2 = 2 * M, C2 = M + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw);
@@ -506,8 +527,10 @@ __global__ void __launch_bounds__(256) k_xinv4(const float2* __restrict__ in, in
 template <int L1, int LZ>
 __global__ void __launch_bounds__(384) k_yz4(float2* __restrict__ X1, int N0, int N1, int C2,
                                              const float* __restrict__ kern, const float2* __restrict__ tw,
-                                             int twL, const int* __restrict__ active) {
-    if (active && !*active) return;
+                                             int twL, const int* __restrict__ active, const SlotStrides ss) {
+    const int sl = blockIdx.z;
+    if (active && !active[sl * ss.sel]) return;
+    X1 += sl * ss.x1;
     constexpr int A = Split<L1>::A, B = Split<L1>::B, SS = Slot<L1>::S;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw);
@@ -578,10 +601,10 @@ __global__ void __launch_bounds__(384) k_yz4(float2* __restrict__ X1, int N0, in
 
 // Dispatch tables for the fast kernels.
 typedef void (*xfwd4_fn)(const float*, const float*, const int*, int, const float*, long, int, int, int, int,
-                         float2*, const float2*, int, int, const int*);
+                         float2*, const float2*, int, int, const int*, const SlotStrides);
 typedef void (*xinv4_fn)(const float2*, int, int, int, int, float*, float*, const int*, int, long, float,
-                         const float2*, int, int, const int*);
-typedef void (*yz4_fn)(float2*, int, int, int, const float*, const float2*, int, const int*);
+                         const float2*, int, int, const int*, const SlotStrides);
+typedef void (*yz4_fn)(float2*, int, int, int, const float*, const float2*, int, const int*, const SlotStrides);
 
 static xfwd4_fn xfwd4_for(int M, int* B, int* S) {
     switch (M) {
@@ -906,17 +929,40 @@ HSB_EXPORT int hsb_demag_plan_info(hsb_demag_plan P, int* logic, int* fused, dou
 }
 
 // Launch the convolution: H (A/m, FP32 SoA [3][N0][N1][N2]) = Ms0 * K (*) (m * mask).
+long hsb_demag_x1_bytes(hsb_demag_plan P) {
+    if (!P || !P->xfwd4 || !P->yz4 || !P->xinv4) return 0;
+    return 3L * P->N[0] * P->C2 * P->N[1] * (long)sizeof(float2);
+}
+
 int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, float ms0,
-                     cudaStream_t st, const int* active) {
+                     cudaStream_t st, const int* active, const HsbDemagBatch* batch) {
     const int N0 = P->N[0], N1 = P->N[1], N2 = P->N[2];
     const int L0 = P->L[0], L1 = P->L[1], L2 = P->L[2];
     const int C2 = P->C2;
     const long ncell = (long)N0 * N1 * N2;
+    SlotStrides ss = {0, 0, 0, 0, nullptr, 0};
+    float2* X1 = P->X1;
+    int nz = 1;
+    if (batch) {
+        if (!hsb_demag_x1_bytes(P) || mask || !batch->X1 || batch->nslot < 1) {
+            hsb_set_error("hsb_demag_launch: batched convolutions need the fast kernels, no mask and a spectrum "
+                          "arena");
+            return HSB_ERR_UNSUPPORTED;
+        }
+        ss.in = batch->m_stride;
+        ss.x1 = batch->x1_stride;
+        ss.out = batch->h_stride;
+        ss.sel = batch->sel_stride;
+        ss.scale = batch->scale;
+        ss.scale_stride = batch->scale_stride;
+        X1 = (float2*)batch->X1;
+        nz = batch->nslot;
+    }
     if (io.ev) cudaEventRecord(io.ev[0], st);
     if (P->xfwd4) {
-        dim3 gx(hsb_div_up(N1, P->x4_rows), 3 * N0);
+        dim3 gx(hsb_div_up(N1, P->x4_rows), 3 * N0, nz);
         P->xfwd4<<<gx, P->x4_threads, P->x4_smem, st>>>(io.m[0], io.m[1], io.msel, io.minv, mask, ncell, N0, N1, N2,
-                                                        N1, P->X1, P->tw, P->twL, P->x4_rows, active);
+                                                        N1, X1, P->tw, P->twL, P->x4_rows, active, ss);
     } else {
         dim3 gx(hsb_div_up(N1, P->TYx), 3 * N0);
         k_fft_x_fwd<float><<<gx, XTHREADS, P->smem_x, st>>>(io.m[0], io.m[1], io.msel, io.minv, mask, ncell, N0, N1,
@@ -924,7 +970,8 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     }
     if (io.ev) cudaEventRecord(io.ev[1], st);
     if (P->yz4) {
-        P->yz4<<<C2, P->yz4_threads, P->yz4_smem, st>>>(P->X1, N0, N1, C2, P->kern, P->tw, P->twL, active);
+        dim3 gyz(C2, 1, nz);
+        P->yz4<<<gyz, P->yz4_threads, P->yz4_smem, st>>>(X1, N0, N1, C2, P->kern, P->tw, P->twL, active, ss);
     } else if (P->fused) {
         switch (P->lz) {
 #define RUNYZ(LZ) case LZ: k_fft_yz_conv<LZ><<<C2, yz_threads<LZ>::value, P->smem_yz, st>>>(P->X1, N0, N1, L1, C2, P->kern, P->tw, P->twL, active); break;
@@ -943,9 +990,9 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     }
     if (io.ev) cudaEventRecord(io.ev[2], st);
     if (P->xinv4) {
-        dim3 gi(hsb_div_up(N1, P->x4_rows), 3 * N0);
-        P->xinv4<<<gi, P->x4_threads, P->x4_smem, st>>>(P->X1, N1, N0, N1, N2, io.h[0], io.h[1], io.hsel, io.hinv,
-                                                        ncell, ms0, P->tw, P->twL, P->x4_rows, active);
+        dim3 gi(hsb_div_up(N1, P->x4_rows), 3 * N0, nz);
+        P->xinv4<<<gi, P->x4_threads, P->x4_smem, st>>>(X1, N1, N0, N1, N2, io.h[0], io.h[1], io.hsel, io.hinv,
+                                                        ncell, ms0, P->tw, P->twL, P->x4_rows, active, ss);
     } else {
         dim3 gi(hsb_div_up(N1, P->TYxi), 3 * N0);
         k_fft_x_inv<<<gi, XTHREADS, P->smem_xi, st>>>(P->X1, N1, N0, N1, N2, L2, io.h[0], io.h[1], io.hsel, io.hinv,

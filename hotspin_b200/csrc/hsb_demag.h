@@ -33,10 +33,26 @@ struct HsbDemagIO {
     cudaEvent_t* ev;   // optional: 4 events recorded before x-fwd, after x-fwd, after y/z, after x-inv
 };
 
+// Batched convolutions (one per slot, slot = blockIdx.z) on the fast kernels: slot s reads
+// m + s * m_stride (its selector msel + s * sel_stride), writes h + s * h_stride, uses the
+// spectrum scratch X1 + s * x1_stride (complex elements) and scales by
+// scale[s * scale_stride]; `active` is read at active + s * sel_stride.
+struct HsbDemagBatch {
+    int nslot;
+    long m_stride, h_stride;   // floats
+    int sel_stride;            // ints
+    void* X1;                  // nslot spectra (hsb_demag_x1_bytes each)
+    long x1_stride;            // complex elements between slots' spectra
+    const float* scale;
+    int scale_stride;          // floats
+};
+
 // `active` (device, nullable): when it points to 0 every kernel returns at once, so a
 // captured solver attempt past its target costs only the launches.
 int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, float ms0,
-                     cudaStream_t st, const int* active);
+                     cudaStream_t st, const int* active, const HsbDemagBatch* batch = nullptr);
+// Bytes of one slot's spectrum scratch; 0 when the plan has no batched (fast) kernels.
+long hsb_demag_x1_bytes(hsb_demag_plan P);
 extern "C" int hsb_demag_plan_create(const int* size, const double* cellsize, const int* pbc,
                                      int accuracy, void* stream, hsb_demag_plan* out);
 extern "C" int hsb_demag_plan_destroy(hsb_demag_plan P);

@@ -305,20 +305,31 @@ __device__ __forceinline__ void un4(float4 a, float v[4]) {
     v[3] = a.w;
 }
 
-template <int CH>
-__global__ void __launch_bounds__(256, 2) k_stage4(const HsbPhys P, const StageArgs A, HsbSolverDev* sd) {
-    if (!A.ungated && !sd->active) return;
+__device__ __forceinline__ float* resolve_off(const PtrSel& s, const HsbSolverDev* sd, long off) {
+    float* p = resolve(s, sd);
+    return p ? p + off : nullptr;
+}
+
+template <int CH, bool BATCH>
+__global__ void __launch_bounds__(256, 2) k_stage4(const __grid_constant__ HsbPhys P0, const StageArgs A,
+                                                   HsbSolverDev* sd0, const BatchArgs Bt) {
+    const int slot = BATCH ? (int)blockIdx.z : 0;
+    HsbSolverDev* sd = sd0 + slot;
+    if (!A.ungated && !(A.prep_gated ? sd->prep : sd->active)) return;
+    const HsbPhys& P = BATCH ? Bt.phys[slot] : P0;
+    const long off = BATCH ? (long)slot * Bt.stride : 0;
+    const int normalize = BATCH ? (A.normalize && P.normalize) : A.normalize;
     const double t = sd->t;
     const double dt = sd->dt;
     const long long step = sd->step;
-    const float* ys = resolve(A.ys, sd);
-    const float* hd = resolve(A.hd, sd);
-    const float* yth = resolve(A.ytherm, sd);
-    float* kout = resolve(A.kout, sd);
-    const float* kacc = resolve(A.kacc, sd);
-    float* ynext = resolve(A.ynext, sd);
-    const float* ybase = resolve(A.ybase, sd);
-    const float* yerr0 = resolve(A.yerr0, sd);
+    const float* ys = resolve_off(A.ys, sd, off);
+    const float* hd = resolve_off(A.hd, sd, off);
+    const float* yth = resolve_off(A.ytherm, sd, off);
+    float* kout = resolve_off(A.kout, sd, off);
+    const float* kacc = resolve_off(A.kacc, sd, off);
+    float* ynext = resolve_off(A.ynext, sd, off);
+    const float* ybase = resolve_off(A.ybase, sd, off);
+    const float* yerr0 = resolve_off(A.yerr0, sd, off);
     const double ts = t + (double)A.tfrac * dt;
     const float fdt = (float)dt;
     const long n = P.ncell;
@@ -499,7 +510,7 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const HsbPhys P, const StageA
 #pragma unroll
             for (int j = 0; j < HSB_MAXK; j++) {
                 if (j < A.nk && A.ck[j] != 0.f) {
-                    const float* kj = resolve(A.kin[j], sd);
+                    const float* kj = resolve_off(A.kin[j], sd, off);
 #pragma unroll
                     for (int c = 0; c < CH; c++) {
                         float a[4];
@@ -516,7 +527,7 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const HsbPhys P, const StageA
 #pragma unroll
                 for (int q = 0; q < 4; q++) out[c][q] = b[q] + fdt * out[c][q];
             }
-            if (A.normalize) {
+            if (normalize) {
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     const float l2 = out[0][q] * out[0][q] + out[1][q] * out[1][q] + out[2][q] * out[2][q];
@@ -542,7 +553,7 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const HsbPhys P, const StageA
 #pragma unroll
             for (int j = 0; j < HSB_MAXK; j++) {
                 if (A.ce[j] != 0.f) {
-                    const float* kj = resolve(A.kin[j], sd);
+                    const float* kj = resolve_off(A.kin[j], sd, off);
 #pragma unroll
                     for (int c = 0; c < CH; c++) {
                         float a[4];
@@ -584,16 +595,21 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const HsbPhys P, const StageA
 
 // Next stage point / new state without a right-hand-side evaluation:
 // ynext = ybase + dt * sum_j ck[j] kin[j] (renormalised in LLG mode).
-template <int CH>
-__global__ void __launch_bounds__(256) k_combine(const HsbPhys P, const StageArgs A, HsbSolverDev* sd) {
+template <int CH, bool BATCH>
+__global__ void __launch_bounds__(256) k_combine(const __grid_constant__ HsbPhys P0, const StageArgs A,
+                                                 HsbSolverDev* sd0, const BatchArgs Bt) {
+    const int slot = BATCH ? (int)blockIdx.z : 0;
+    HsbSolverDev* sd = sd0 + slot;
     if (!sd->active) return;
+    const HsbPhys& P = BATCH ? Bt.phys[slot] : P0;
+    const long off = BATCH ? (long)slot * Bt.stride : 0;
     const float fdt = (float)sd->dt;
     const long n = P.ncell;
-    float* ynext = resolve(A.ynext, sd);
-    const float* ybase = resolve(A.ybase, sd);
+    float* ynext = resolve_off(A.ynext, sd, off);
+    const float* ybase = resolve_off(A.ybase, sd, off);
     const float* kin[HSB_MAXK];
 #pragma unroll
-    for (int j = 0; j < HSB_MAXK; j++) kin[j] = (j < A.nk) ? resolve(A.kin[j], sd) : nullptr;
+    for (int j = 0; j < HSB_MAXK; j++) kin[j] = (j < A.nk) ? resolve_off(A.kin[j], sd, off) : nullptr;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         float out[CH];
 #pragma unroll
@@ -604,7 +620,7 @@ __global__ void __launch_bounds__(256) k_combine(const HsbPhys P, const StageArg
                 if (j < A.nk && A.ck[j] != 0.f) acc += A.ck[j] * __ldg(kin[j] + c * n + i);
             out[c] = __ldg(ybase + c * n + i) + fdt * acc;
         }
-        if (A.normalize) {
+        if (BATCH ? (A.normalize && P.normalize) : A.normalize) {
             const float l2 = out[0] * out[0] + out[1] * out[1] + out[2] * out[2];
             const float inv = (l2 == 0.f) ? 0.f : rsqrtf(l2);
             out[0] *= inv;
@@ -618,7 +634,10 @@ __global__ void __launch_bounds__(256) k_combine(const HsbPhys P, const StageArg
 
 // Dormand-Prince step-size control, one thread (see the controller rule in the header of
 // include/hotspin_b200.h).  Consumes the attempt's error maximum.
-__global__ void k_dp45_control(HsbSolverDev* sd) {
+__global__ void k_dp45_control(HsbSolverDev* sd0, int nslot) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslot) return;
+    HsbSolverDev* sd = sd0 + slot;
     if (!sd->active) return;
     const float ef = __uint_as_float(sd->err_acc);
     const unsigned int nf = sd->nonfinite;
@@ -657,7 +676,10 @@ __global__ void k_dp45_control(HsbSolverDev* sd) {
 }
 
 // Fixed-step bookkeeping: t += dt, step++, swap state buffers, stop at the target.
-__global__ void k_fixed_advance(HsbSolverDev* sd) {
+__global__ void k_fixed_advance(HsbSolverDev* sd0, int nslot) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslot) return;
+    HsbSolverDev* sd = sd0 + slot;
     if (!sd->active) return;
     sd->t += sd->dt;
     sd->step += 1;
@@ -676,8 +698,9 @@ int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cud
     const int threads = 256;
     if (P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask) {
         const int grid = hsb_grid_1d(P.ncell / 4, threads, 2);
-        if (P.nch == 5) k_stage4<5><<<grid, threads, 0, st>>>(P, A, sd);
-        else k_stage4<3><<<grid, threads, 0, st>>>(P, A, sd);
+        BatchArgs nb = {0, nullptr, 1};
+        if (P.nch == 5) k_stage4<5, false><<<grid, threads, 0, st>>>(P, A, sd, nb);
+        else k_stage4<3, false><<<grid, threads, 0, st>>>(P, A, sd, nb);
         return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
     }
     const int grid = hsb_grid_1d(P.ncell, threads, 8);
@@ -689,17 +712,69 @@ int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cud
 int hsb_launch_combine(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st) {
     const int threads = 256;
     const int grid = hsb_grid_1d(P.ncell, threads, 8);
-    if (P.nch == 5) k_combine<5><<<grid, threads, 0, st>>>(P, A, sd);
-    else k_combine<3><<<grid, threads, 0, st>>>(P, A, sd);
+    BatchArgs nb = {0, nullptr, 1};
+    if (P.nch == 5) k_combine<5, false><<<grid, threads, 0, st>>>(P, A, sd, nb);
+    else k_combine<3, false><<<grid, threads, 0, st>>>(P, A, sd, nb);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }
 
 int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st) {
-    k_dp45_control<<<1, 1, 0, st>>>(sd);
+    k_dp45_control<<<1, 1, 0, st>>>(sd, 1);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}
+
+// Batched variants: one grid plane per slot (blockIdx.z); Bt.phys / sd are slot arrays.
+// P carries the class-wide geometry (size, channels; masks are not supported in batches).
+int hsb_launch_stage_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
+                             cudaStream_t st) {
+    const int threads = 256;
+    if (P.N2 % 4 != 0 || P.msat_mask || P.lex_mask) return HSB_ERR_UNSUPPORTED;
+    long g = (P.ncell / 4 + threads - 1) / threads;
+    const long cap = (long)hsb_sm_count() * 2;
+    dim3 grid((unsigned)(g < cap ? g : cap), 1, (unsigned)Bt.nslot);
+    if (P.nch == 5) k_stage4<5, true><<<grid, threads, 0, st>>>(P, A, sd, Bt);
+    else k_stage4<3, true><<<grid, threads, 0, st>>>(P, A, sd, Bt);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}
+
+int hsb_launch_combine_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
+                               cudaStream_t st) {
+    const int threads = 256;
+    long g = (P.ncell + threads - 1) / threads;
+    const long cap = (long)hsb_sm_count() * 4;
+    dim3 grid((unsigned)(g < cap ? g : cap), 1, (unsigned)Bt.nslot);
+    if (P.nch == 5) k_combine<5, true><<<grid, threads, 0, st>>>(P, A, sd, Bt);
+    else k_combine<3, true><<<grid, threads, 0, st>>>(P, A, sd, Bt);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}
+
+int hsb_launch_dp45_control_batched(HsbSolverDev* sd, int nslot, cudaStream_t st) {
+    k_dp45_control<<<(nslot + 31) / 32, 32, 0, st>>>(sd, nslot);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}
+
+// Slots whose preparation just ran start stepping.
+__global__ void k_activate_prepped(HsbSolverDev* sd0, int nslot) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslot) return;
+    HsbSolverDev* sd = sd0 + slot;
+    if (sd->prep) {
+        sd->prep = 0;
+        sd->active = 1;
+    }
+}
+
+int hsb_launch_fixed_advance_batched(HsbSolverDev* sd, int nslot, cudaStream_t st) {
+    k_fixed_advance<<<(nslot + 31) / 32, 32, 0, st>>>(sd, nslot);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}
+
+int hsb_launch_activate_prepped(HsbSolverDev* sd, int nslot, cudaStream_t st) {
+    k_activate_prepped<<<(nslot + 31) / 32, 32, 0, st>>>(sd, nslot);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }
 
 int hsb_launch_fixed_advance(HsbSolverDev* sd, cudaStream_t st) {
-    k_fixed_advance<<<1, 1, 0, st>>>(sd);
+    k_fixed_advance<<<1, 1, 0, st>>>(sd, 1);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }

@@ -41,6 +41,16 @@ struct HsbPhys {
     float laser_p0, laser_t0, laser_c;  // c = 4 ln2 / fwhm^2
     float laser_inv2s2;                 // 1/(2 sigma^2), 0 = uniform spot
     float cs1, cs2;
+    int normalize;       // renormalise m at stage formation (LLG mode); used by batched launches
+    float ms0;           // Ms0 (A/m), the demag scale of this simulation
+};
+
+// Batched launches: slot = blockIdx.z; every per-slot buffer of slot s lives at the slot-0
+// address + s * stride (one arena per slot), physics and solver state per slot.
+struct BatchArgs {
+    long stride;               // floats between slots' arenas (0 = not batched)
+    const HsbPhys* phys;       // device array [nslot]
+    int nslot;
 };
 
 // Device-resident solver state (read by every kernel of an attempt, written by the
@@ -59,6 +69,8 @@ struct HsbSolverDev {
     long long step_stop;   // >= 0: stop after this many accepted steps
     unsigned int err_acc;  // float bits of the running max error of the attempt
     unsigned int nonfinite;
+    int prep;              // batched slots: 1 while the slot's first-stage data is being prepared
+    int pad_;
 };
 
 // Pointer selectors resolved on the device against HsbSolverDev.
@@ -93,4 +105,5 @@ struct StageArgs {
     PtrSel yerr0;            // y0 (for the relative temperature norm)
     float rtol;
     int ungated;             // run even when the solver is inactive (state queries)
+    int prep_gated;          // gate on HsbSolverDev.prep instead of .active (batched slot preparation)
 };

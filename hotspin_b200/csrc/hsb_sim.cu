@@ -21,6 +21,13 @@ int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cud
 int hsb_launch_combine(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st);
 int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st);
 int hsb_launch_fixed_advance(HsbSolverDev* sd, cudaStream_t st);
+int hsb_launch_stage_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
+                             cudaStream_t st);
+int hsb_launch_combine_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
+                               cudaStream_t st);
+int hsb_launch_dp45_control_batched(HsbSolverDev* sd, int nslot, cudaStream_t st);
+int hsb_launch_fixed_advance_batched(HsbSolverDev* sd, int nslot, cudaStream_t st);
+int hsb_launch_activate_prepped(HsbSolverDev* sd, int nslot, cudaStream_t st);
 
 // Mirror of the public descriptor (include/hotspin_b200.h).
 struct hsb_sim_desc {
@@ -68,6 +75,21 @@ struct hsb_sim_s {
     long n;
     cudaStream_t st;
     hsb_demag_plan demag;
+    // Buffers of one simulation ("slot") lie in one arena; a batch holds nslot arenas at a
+    // uniform stride, and every pointer below addresses slot 0's.
+    float* arena;
+    long slot_stride;   // floats between slots' arenas
+    int nslot;
+    bool batched;       // launches use the slot-batched kernels (per-slot physics and solver state)
+    HsbPhys* phys_dev;  // batched: per-slot physics [nslot]
+    std::vector<HsbPhys> phys_h;
+    void* X1b;          // batched: per-slot demag spectra
+    long x1_stride;     // complex elements
+    BatchArgs bt;
+    bool prep_mode;     // enqueueing the preparation of newly admitted slots
+    int nprep;          // slots admitted since the last launch
+    cudaEvent_t done_ev;
+    bool launched;
     float* y[2];        // state double buffer
     float* ystage[2];   // stage points (ping-pong: a kernel never reads and writes one)
     float* k[8];        // stage derivatives
@@ -75,12 +97,13 @@ struct hsb_sim_s {
     float* hd01[2];     // demag field of y[0], y[1] (DP45 with a thermal field)
     float* msat_mask;
     float* lex_mask;
-    HsbSolverDev* sd;   // device
-    HsbSolverDev* sd_host;  // pinned mirror
+    HsbSolverDev* sd;   // device [nslot]
+    HsbSolverDev* sd_host;  // pinned mirror [nslot]
     double* red;        // reduction scratch (device)
     double* red_host;   // pinned
     float* stage_f;     // device staging for FP64 <-> FP32 conversion
     double* stage_d;
+    void* stage_pin;    // batched: pinned per-slot staging of admissions
     cudaGraphExec_t graph;
     int graph_steps;    // attempts captured in one graph launch
     bool initialized;   // k1 / hd01 of the current state computed (DP45)
@@ -278,8 +301,22 @@ static int run_demag(hsb_sim_s* S, const float* m, int msel, float* h, int hsel,
         io.ev = ev;
     }
     S->launches += hsb_demag_nlaunch(S->demag);
-    int rc = hsb_demag_launch(S->demag, io, S->msat_mask, (float)S->d.msat0T0, S->st,
-                              gated ? &S->sd->active : nullptr);
+    const int* gate = gated ? (S->prep_mode ? &S->sd->prep : &S->sd->active) : nullptr;
+    int rc;
+    if (S->batched) {
+        HsbDemagBatch b;
+        b.nslot = S->nslot;
+        b.m_stride = S->slot_stride;
+        b.h_stride = S->slot_stride;
+        b.sel_stride = (int)(sizeof(HsbSolverDev) / sizeof(int));
+        b.X1 = S->X1b;
+        b.x1_stride = S->x1_stride;
+        b.scale = &S->phys_dev[0].ms0;
+        b.scale_stride = (int)(sizeof(HsbPhys) / sizeof(float));
+        rc = hsb_demag_launch(S->demag, io, nullptr, 1.0f, S->st, gate, &b);
+    } else {
+        rc = hsb_demag_launch(S->demag, io, S->msat_mask, (float)S->d.msat0T0, S->st, gate);
+    }
     if (S->profiling) {
         S->prof.push_back({PROF_XFWD, {ev[0], ev[1]}});
         S->prof.push_back({PROF_YZ, {ev[1], ev[2]}});
@@ -307,11 +344,30 @@ static int timed(hsb_sim_s* S, int cat, F&& f) {
         if (rc_ != HSB_OK) return rc_; \
     } while (0)
 
+// Launches of one simulation or of a batch of slots.
+static int L_stage(hsb_sim_s* S, StageArgs A) {
+    if (S->prep_mode) A.prep_gated = 1;
+    if (S->batched) return hsb_launch_stage_batched(S->P, A, S->sd, S->bt, S->st);
+    return hsb_launch_stage(S->P, A, S->sd, S->st);
+}
+static int L_combine(hsb_sim_s* S, const StageArgs& A) {
+    if (S->batched) return hsb_launch_combine_batched(S->P, A, S->sd, S->bt, S->st);
+    return hsb_launch_combine(S->P, A, S->sd, S->st);
+}
+static int L_control(hsb_sim_s* S) {
+    if (S->batched) return hsb_launch_dp45_control_batched(S->sd, S->nslot, S->st);
+    return hsb_launch_dp45_control(S->sd, S->st);
+}
+static int L_advance(hsb_sim_s* S) {
+    if (S->batched) return hsb_launch_fixed_advance_batched(S->sd, S->nslot, S->st);
+    return hsb_launch_fixed_advance(S->sd, S->st);
+}
+
 // Enqueue one attempt (one step for the fixed-step methods) of the configured integrator.
 // All buffer choices that depend on accept/reject are made on the device.
 static int enqueue_attempt(hsb_sim_s* S) {
-    HsbSolverDev* sd = S->sd;
-    const int norm = S->d.normalize;
+    // batched: every slot's own HsbPhys.normalize decides
+    const int norm = S->batched ? 1 : S->d.normalize;
     float* hd = S->demag ? S->hd : nullptr;
     float* ya = S->ystage[0];
     float* yb = S->ystage[1];
@@ -330,8 +386,8 @@ static int enqueue_attempt(hsb_sim_s* S) {
             A.ybase = YC;
             A.cself = 1.0f;
             A.normalize = norm;
-            RC(timed(S, PROF_STAGE, [&] { return hsb_launch_stage(S->P, A, sd, S->st); }));
-            RC(timed(S, PROF_OTHER, [&] { return hsb_launch_fixed_advance(sd, S->st); }));
+            RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
+            RC(timed(S, PROF_OTHER, [&] { return L_advance(S); }));
             break;
         }
         case SOLVER_HEUN: {  // solve_heun.go:27-79
@@ -346,7 +402,7 @@ static int enqueue_attempt(hsb_sim_s* S) {
             A.ybase = YC;
             A.cself = 1.0f;
             A.normalize = norm;
-            RC(timed(S, PROF_STAGE, [&] { return hsb_launch_stage(S->P, A, sd, S->st); }));
+            RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
             RC(run_demag(S, ya, -1, hd, -1));
             StageArgs B = empty_args();
             B.ys = fixed(ya);
@@ -360,8 +416,8 @@ static int enqueue_attempt(hsb_sim_s* S) {
             B.ck[0] = -0.5f;
             B.cself = 0.5f;
             B.normalize = norm;
-            RC(timed(S, PROF_STAGE, [&] { return hsb_launch_stage(S->P, B, sd, S->st); }));
-            RC(timed(S, PROF_OTHER, [&] { return hsb_launch_fixed_advance(sd, S->st); }));
+            RC(timed(S, PROF_STAGE, [&] { return L_stage(S, B); }));
+            RC(timed(S, PROF_OTHER, [&] { return L_advance(S); }));
             break;
         }
         case SOLVER_RK4: {
@@ -393,9 +449,9 @@ static int enqueue_attempt(hsb_sim_s* S) {
                     A.ck[0] = 1.0f / 6.0f;
                     A.cself = 1.0f / 6.0f;
                 }
-                RC(timed(S, PROF_STAGE, [&] { return hsb_launch_stage(S->P, A, sd, S->st); }));
+                RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
             }
-            RC(timed(S, PROF_OTHER, [&] { return hsb_launch_fixed_advance(sd, S->st); }));
+            RC(timed(S, PROF_OTHER, [&] { return L_advance(S); }));
             break;
         }
         case SOLVER_DP45: {
@@ -419,7 +475,7 @@ static int enqueue_attempt(hsb_sim_s* S) {
                 A.ybase = YC;
                 A.cself = (float)DPA[1][0];
                 A.normalize = norm;
-                RC(timed(S, PROF_STAGE, [&] { return hsb_launch_stage(S->P, A, sd, S->st); }));
+                RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
             } else {
                 StageArgs A = empty_args();
                 A.ynext = fixed(ya);
@@ -428,7 +484,7 @@ static int enqueue_attempt(hsb_sim_s* S) {
                 A.kin[0] = K1;
                 A.ck[0] = (float)DPA[1][0];
                 A.normalize = norm;
-                RC(timed(S, PROF_OTHER, [&] { return hsb_launch_combine(S->P, A, sd, S->st); }));
+                RC(timed(S, PROF_OTHER, [&] { return L_combine(S, A); }));
             }
             float* cur = ya;
             float* other = yb;
@@ -450,7 +506,7 @@ static int enqueue_attempt(hsb_sim_s* S) {
                 }
                 A.cself = (float)DPA[s + 1][s];
                 A.normalize = norm;
-                RC(timed(S, PROF_STAGE, [&] { return hsb_launch_stage(S->P, A, sd, S->st); }));
+                RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
                 float* t = cur;
                 cur = other;
                 other = t;
@@ -480,8 +536,8 @@ static int enqueue_attempt(hsb_sim_s* S) {
             A.ceself = (float)DPE[6];
             A.yerr0 = YC;
             A.rtol = (float)S->d.rtol;
-            RC(timed(S, PROF_STAGE, [&] { return hsb_launch_stage(S->P, A, sd, S->st); }));
-            RC(timed(S, PROF_OTHER, [&] { return hsb_launch_dp45_control(sd, S->st); }));
+            RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
+            RC(timed(S, PROF_OTHER, [&] { return L_control(S); }));
             break;
         }
         default:
@@ -512,7 +568,7 @@ static int prepare(hsb_sim_s* S) {
         A.ytherm = YC;
         A.kout = pair(S->k[0], S->k[6], SEL_K1);
         A.kself_w = 1.0f;
-        RC(hsb_launch_stage(S->P, A, S->sd, S->st));
+        RC(L_stage(S, A));
     }
     S->initialized = true;
     return HSB_OK;
@@ -541,8 +597,17 @@ static int build_graph(hsb_sim_s* S) {
     return HSB_OK;
 }
 
+static int plain_only(hsb_sim_s* S, const char* who) {
+    if (S && S->batched) {
+        hsb_set_error("%s: a batch handle takes the hsb_batch_* functions", who);
+        return HSB_ERR_INVALID;
+    }
+    return HSB_OK;
+}
+
 // Advance until the device clears `active` (step or time target reached).
 static int advance(hsb_sim_s* S, int64_t nsteps, double t_stop) {
+    RC(plain_only(S, "hsb_sim_step/run_until"));
     RC(get_sd(S));
     HsbSolverDev* h = S->sd_host;
     if (h->status & 1) {
@@ -587,9 +652,7 @@ static int advance(hsb_sim_s* S, int64_t nsteps, double t_stop) {
 }
 
 // ------------------------------------------------------------------ public API
-static void fill_phys(hsb_sim_s* S) {
-    const hsb_sim_desc& d = S->d;
-    HsbPhys& P = S->P;
+static void phys_from_desc(const hsb_sim_desc& d, int nch, long ncell, HsbPhys& P) {
     memset(&P, 0, sizeof(P));
     P.N0 = d.size[0];
     P.N1 = d.size[1];
@@ -597,8 +660,8 @@ static void fill_phys(hsb_sim_s* S) {
     P.pbc0 = d.pbc[0];
     P.pbc1 = d.pbc[1];
     P.pbc2 = d.pbc[2];
-    P.nch = S->nch;
-    P.ncell = S->n;
+    P.nch = nch;
+    P.ncell = ncell;
     for (int a = 0; a < 3; a++) {
         P.ex_c[a] = (float)(d.msat0T0 * d.lex * d.lex / (d.cellsize[a] * d.cellsize[a]));
         P.lam[a] = (float)d.alpha[a];
@@ -641,8 +704,59 @@ static void fill_phys(hsb_sim_s* S) {
     P.laser_inv2s2 = d.laser_sigma > 0 ? (float)(1.0 / (2.0 * d.laser_sigma * d.laser_sigma)) : 0.f;
     P.cs1 = (float)d.cellsize[1];
     P.cs2 = (float)d.cellsize[2];
-    P.msat_mask = S->msat_mask;
-    P.lex_mask = S->lex_mask;
+    P.normalize = d.normalize;
+    P.ms0 = (float)d.msat0T0;
+}
+
+static void fill_phys(hsb_sim_s* S) {
+    phys_from_desc(S->d, S->nch, S->n, S->P);
+    S->P.msat_mask = S->msat_mask;
+    S->P.lex_mask = S->lex_mask;
+}
+
+// Offsets (floats) of one slot's buffers in its arena.
+struct SlotLayout {
+    long y, ystage, k, hd, hd01, total;
+    int nk;
+};
+static SlotLayout slot_layout(const hsb_sim_desc& d, long n) {
+    auto al = [](long x) { return (x + 63) & ~63L; };  // 256-byte boundaries
+    SlotLayout L;
+    const long ny = (long)(d.ttm ? 5 : 3) * n;
+    L.nk = (d.solver == SOLVER_DP45) ? 7 : 1;
+    long o = 0;
+    L.y = o;
+    o += al(2 * ny);
+    L.ystage = o;
+    o += al(2 * ny);
+    L.k = o;
+    o += al(L.nk * ny);
+    L.hd = -1;
+    L.hd01 = -1;
+    if (d.demag) {
+        L.hd = o;
+        o += al(3 * n);
+        if (d.thermal && d.solver == SOLVER_DP45) {
+            L.hd01 = o;
+            o += al(6 * n);
+        }
+    }
+    L.total = o;
+    return L;
+}
+
+static void point_slot0(hsb_sim_s* S, const SlotLayout& L) {
+    const long ny = (long)S->nch * S->n;
+    float* a = S->arena;
+    S->y[0] = a + L.y;
+    S->y[1] = S->y[0] + ny;
+    S->ystage[0] = a + L.ystage;
+    S->ystage[1] = S->ystage[0] + ny;
+    for (int j = 0; j < 8; j++) S->k[j] = (j < L.nk) ? a + L.k + j * ny : nullptr;
+    S->hd = L.hd >= 0 ? a + L.hd : nullptr;
+    S->hd01[0] = L.hd01 >= 0 ? a + L.hd01 : nullptr;
+    S->hd01[1] = L.hd01 >= 0 ? S->hd01[0] + 3 * S->n : nullptr;
+    S->slot_stride = L.total;
 }
 
 static void free_sim(hsb_sim_s* S) {
@@ -650,11 +764,10 @@ static void free_sim(hsb_sim_s* S) {
     if (S->graph) cudaGraphExecDestroy(S->graph);
     for (auto e : S->ev_pool) cudaEventDestroy(e);
     if (S->demag) hsb_demag_plan_destroy(S->demag);
-    cudaFree(S->y[0]);
-    cudaFree(S->ystage[0]);
-    cudaFree(S->k[0]);
-    cudaFree(S->hd);
-    cudaFree(S->hd01[0]);
+    cudaFree(S->arena);
+    cudaFree(S->phys_dev);
+    cudaFree(S->X1b);
+    if (S->done_ev) cudaEventDestroy(S->done_ev);
     cudaFree(S->msat_mask);
     cudaFree(S->lex_mask);
     cudaFree(S->sd);
@@ -662,6 +775,7 @@ static void free_sim(hsb_sim_s* S) {
     cudaFree(S->stage_f);
     cudaFree(S->stage_d);
     if (S->sd_host) cudaFreeHost(S->sd_host);
+    if (S->stage_pin) cudaFreeHost(S->stage_pin);
     if (S->red_host) cudaFreeHost(S->red_host);
     if (S->st) cudaStreamDestroy(S->st);
     delete S;
@@ -683,6 +797,37 @@ __global__ void k_fill(float* p, long n, float v) {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) p[i] = v;
 }
 
+static int check_desc(const hsb_sim_desc& d, const char* who) {
+    for (int a = 0; a < 3; a++) {
+        if (d.size[a] < 1 || d.cellsize[a] <= 0 || d.pbc[a] < 0) {
+            hsb_set_error("%s: bad size/cellsize/pbc on axis %d", who, a);
+            return HSB_ERR_INVALID;
+        }
+    }
+    if (d.solver < SOLVER_EULER || d.solver > SOLVER_DP45) {
+        hsb_set_error("%s: unknown solver %d", who, d.solver);
+        return HSB_ERR_INVALID;
+    }
+    if (!(d.dt > 0) || !(d.msat0T0 > 0) || (d.solver == SOLVER_DP45 && !(d.rtol > 0))) {
+        hsb_set_error("%s: dt, msat0T0 (and rtol for DP45) must be positive", who);
+        return HSB_ERR_INVALID;
+    }
+    if (d.llb && !(d.tc > 0 && d.spin_j > 0 && d.n_spins > 0)) {
+        hsb_set_error("%s: llb needs tc, spin_j and n_spins > 0", who);
+        return HSB_ERR_INVALID;
+    }
+    if (d.ttm && !(d.gamma_e > 0 && d.c_l > 0)) {
+        hsb_set_error("%s: ttm needs gamma_e > 0 and c_l > 0", who);
+        return HSB_ERR_INVALID;
+    }
+    const long n = (long)d.size[0] * d.size[1] * d.size[2];
+    if (n > (1L << 31) / 8) {
+        hsb_set_error("%s: %ld cells exceed the 2^28 limit", who, n);
+        return HSB_ERR_UNSUPPORTED;
+    }
+    return HSB_OK;
+}
+
 HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     if (!desc || !out) {
         hsb_set_error("hsb_sim_create: null argument");
@@ -690,57 +835,23 @@ HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     }
     *out = nullptr;
     const hsb_sim_desc& d = *desc;
-    for (int a = 0; a < 3; a++) {
-        if (d.size[a] < 1 || d.cellsize[a] <= 0 || d.pbc[a] < 0) {
-            hsb_set_error("hsb_sim_create: bad size/cellsize/pbc on axis %d", a);
-            return HSB_ERR_INVALID;
-        }
-    }
-    if (d.solver < SOLVER_EULER || d.solver > SOLVER_DP45) {
-        hsb_set_error("hsb_sim_create: unknown solver %d", d.solver);
-        return HSB_ERR_INVALID;
-    }
-    if (!(d.dt > 0) || !(d.msat0T0 > 0) || (d.solver == SOLVER_DP45 && !(d.rtol > 0))) {
-        hsb_set_error("hsb_sim_create: dt, msat0T0 (and rtol for DP45) must be positive");
-        return HSB_ERR_INVALID;
-    }
-    if (d.llb && !(d.tc > 0 && d.spin_j > 0 && d.n_spins > 0)) {
-        hsb_set_error("hsb_sim_create: llb needs tc, spin_j and n_spins > 0");
-        return HSB_ERR_INVALID;
-    }
-    if (d.ttm && !(d.gamma_e > 0 && d.c_l > 0)) {
-        hsb_set_error("hsb_sim_create: ttm needs gamma_e > 0 and c_l > 0");
-        return HSB_ERR_INVALID;
-    }
+    RC(check_desc(d, "hsb_sim_create"));
     const long n = (long)d.size[0] * d.size[1] * d.size[2];
-    if (n > (1L << 31) / 8) {
-        hsb_set_error("hsb_sim_create: %ld cells exceed the 2^28 limit", n);
-        return HSB_ERR_UNSUPPORTED;
-    }
     hsb_sim_s* S = new hsb_sim_s();
     S->d = d;
     S->n = n;
     S->nch = d.ttm ? 5 : 3;
-    const long ny = (long)S->nch * n;
+    S->nslot = 1;
     STRY(cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking));
-    STRY(cudaMalloc(&S->y[0], sizeof(float) * 2 * ny));
-    S->y[1] = S->y[0] + ny;
-    STRY(cudaMalloc(&S->ystage[0], sizeof(float) * 2 * ny));
-    S->ystage[1] = S->ystage[0] + ny;
-    const int nk = (d.solver == SOLVER_DP45) ? 7 : 1;
-    STRY(cudaMalloc(&S->k[0], sizeof(float) * nk * ny));
-    for (int j = 1; j < nk; j++) S->k[j] = S->k[0] + j * ny;
+    const SlotLayout L = slot_layout(d, n);
+    STRY(cudaMalloc(&S->arena, sizeof(float) * L.total));
+    point_slot0(S, L);
     STRY(cudaMalloc(&S->sd, sizeof(HsbSolverDev)));
     STRY(cudaMallocHost(&S->sd_host, sizeof(HsbSolverDev)));
     STRY(cudaMalloc(&S->red, sizeof(double) * (RED_BLOCKS * 8 + 16) + 64));
     STRY(cudaMallocHost(&S->red_host, sizeof(double) * 16));
     STRY(cudaMemsetAsync(S->red, 0, sizeof(double) * (RED_BLOCKS * 8 + 16) + 64, S->st));
     if (d.demag) {
-        STRY(cudaMalloc(&S->hd, sizeof(float) * 3 * n));
-        if (d.thermal && d.solver == SOLVER_DP45) {
-            STRY(cudaMalloc(&S->hd01[0], sizeof(float) * 6 * n));
-            S->hd01[1] = S->hd01[0] + 3 * n;
-        }
         int rc = hsb_demag_plan_create(d.size, d.cellsize, d.pbc, 6, S->st, &S->demag);
         if (rc != HSB_OK) {
             free_sim(S);
@@ -794,6 +905,7 @@ static int stage_buffers(hsb_sim_s* S, long count) {
 }
 
 HSB_EXPORT int hsb_sim_set(hsb_sim_s* S, const char* name, const double* host, int64_t count) {
+    RC(plain_only(S, "hsb_sim_set"));
     if (!S || !name) {
         hsb_set_error("hsb_sim_set: null argument");
         return HSB_ERR_INVALID;
@@ -841,6 +953,7 @@ HSB_EXPORT int hsb_sim_set(hsb_sim_s* S, const char* name, const double* host, i
 }
 
 HSB_EXPORT int hsb_sim_get(hsb_sim_s* S, const char* name, double* host, int64_t count) {
+    RC(plain_only(S, "hsb_sim_get"));
     if (!S || !name || !host) {
         hsb_set_error("hsb_sim_get: null argument");
         return HSB_ERR_INVALID;
@@ -920,6 +1033,7 @@ HSB_EXPORT int hsb_sim_sync(hsb_sim_s* S) {
 
 HSB_EXPORT int hsb_sim_status(hsb_sim_s* S, double* t, double* dt, int64_t* steps, int64_t* attempts,
                               int64_t* rejects, double* err, int32_t* status) {
+    RC(plain_only(S, "hsb_sim_status"));
     if (!S) return HSB_ERR_INVALID;
     RC(get_sd(S));
     const HsbSolverDev* h = S->sd_host;
@@ -934,6 +1048,7 @@ HSB_EXPORT int hsb_sim_status(hsb_sim_s* S, double* t, double* dt, int64_t* step
 }
 
 HSB_EXPORT int hsb_sim_set_time(hsb_sim_s* S, double t, double dt) {
+    RC(plain_only(S, "hsb_sim_set_time"));
     if (!S) return HSB_ERR_INVALID;
     RC(get_sd(S));
     S->sd_host->t = t;
@@ -968,6 +1083,7 @@ static int reduce_terms(hsb_sim_s* S, double* out8) {
 // out[5] kernel launches per attempt.  Averaged over `reps` attempts (each a real step of
 // the simulation; the state advances).  out[6] accepted steps during the profile.
 HSB_EXPORT int hsb_sim_profile(hsb_sim_s* S, int reps, double* out) {
+    RC(plain_only(S, "hsb_sim_profile"));
     if (!S || !out || reps < 1) return HSB_ERR_INVALID;
     RC(get_sd(S));
     const long long step0 = S->sd_host->step;
@@ -1004,6 +1120,7 @@ HSB_EXPORT int hsb_sim_profile(hsb_sim_s* S, int reps, double* out) {
 
 // Kernel launches enqueued per attempt (per step for the fixed-step methods).
 HSB_EXPORT int hsb_sim_launches_per_attempt(hsb_sim_s* S, int* n) {
+    RC(plain_only(S, "hsb_sim_launches_per_attempt"));
     if (!S || !n) return HSB_ERR_INVALID;
     if (!S->graph) {
         S->launches = 0;
@@ -1022,6 +1139,7 @@ HSB_EXPORT int hsb_sim_launches_per_attempt(hsb_sim_s* S, int* n) {
 }
 
 HSB_EXPORT int hsb_sim_energy(hsb_sim_s* S, double* energy) {
+    RC(plain_only(S, "hsb_sim_energy"));
     if (!S || !energy) return HSB_ERR_INVALID;
     double r[8];
     RC(reduce_terms(S, r));
@@ -1032,9 +1150,324 @@ HSB_EXPORT int hsb_sim_energy(hsb_sim_s* S, double* energy) {
 }
 
 HSB_EXPORT int hsb_sim_average_m(hsb_sim_s* S, double* avg3) {
+    RC(plain_only(S, "hsb_sim_average_m"));
     if (!S || !avg3) return HSB_ERR_INVALID;
     double r[8];
     RC(reduce_terms(S, r));
     for (int c = 0; c < 3; c++) avg3[c] = r[5 + c] / (double)S->n;
+    return HSB_OK;
+}
+
+// ------------------------------------------------------------------ batches of simulations
+// A batch ("size class") advances up to nslot independent simulations of one grid size with
+// the same kernels: each slot has its own arena (state, stages, demag field), physics
+// (HsbPhys) and solver word (HsbSolverDev), and every launch covers all slots (blockIdx.z).
+// Slots are admitted and read back while the others keep running; a slot that reached its
+// end time, or is empty, costs one early-returning block per launch.  The class fixes the
+// grid size, boundary conditions, solver and its tolerance, channel count (two-temperature
+// model or not), demag on/off and the cell's aspect ratio (the demag tensor of a grid of
+// cells depends only on their shape, so one spectrum serves every slot); everything else
+// (Ms0, lex, cell size, damping, field, anisotropy, temperature, LLB or LLG, seed) is per slot.
+static bool same_aspect(const double* a, const double* b) {
+    for (int i = 1; i < 3; i++) {
+        const double ra = a[i] / a[0], rb = b[i] / b[0];
+        if (fabs(ra - rb) > 1e-9 * fabs(rb)) return false;
+    }
+    return true;
+}
+
+static int batch_check_class(const hsb_sim_desc& d, int32_t nslot, const char* who) {
+    RC(check_desc(d, who));
+    if (nslot < 1 || nslot > 65535) {
+        hsb_set_error("%s: nslot = %d outside [1, 65535]", who, nslot);
+        return HSB_ERR_INVALID;
+    }
+    if (d.size[2] % 4 != 0) {
+        hsb_set_error("%s: batched kernels need the a2 (user x) size to be a multiple of 4, got %d", who,
+                      d.size[2]);
+        return HSB_ERR_UNSUPPORTED;
+    }
+    return HSB_OK;
+}
+
+// Device bytes a batch of `nslot` slots of this class holds (arenas, demag spectra and plan,
+// solver words, physics, reduction scratch); host-pinned staging is not counted.
+HSB_EXPORT int hsb_batch_footprint(const hsb_sim_desc* cls, int32_t nslot, int64_t* bytes) {
+    if (!cls || !bytes) return HSB_ERR_INVALID;
+    RC(batch_check_class(*cls, nslot, "hsb_batch_footprint"));
+    const hsb_sim_desc& d = *cls;
+    const long n = (long)d.size[0] * d.size[1] * d.size[2];
+    const SlotLayout L = slot_layout(d, n);
+    int64_t b = (int64_t)nslot * L.total * (int64_t)sizeof(float);
+    b += (int64_t)nslot * (sizeof(HsbSolverDev) + sizeof(HsbPhys));
+    b += sizeof(double) * (RED_BLOCKS * 8 + 16) + 64;
+    if (d.demag) {
+        int Lg[3];
+        for (int a = 0; a < 3; a++) Lg[a] = (d.size[a] > 1 && d.pbc[a] == 0) ? 2 * d.size[a] : d.size[a];
+        const long C2 = Lg[2] / 2 + 1;
+        const long x1 = 3L * d.size[0] * C2 * d.size[1] * 8;
+        b += (int64_t)(nslot + 1) * x1;                                   // batch spectra + the plan's own
+        b += (int64_t)C2 * (Lg[1] / 2 + 1) * (Lg[0] / 2 + 1) * 6 * 4;      // kernel spectrum
+        int twL = Lg[0] > Lg[1] ? Lg[0] : Lg[1];
+        if (Lg[2] > twL) twL = Lg[2];
+        b += (int64_t)twL * 8;
+    }
+    *bytes = b;
+    return HSB_OK;
+}
+
+HSB_EXPORT int hsb_batch_create(const hsb_sim_desc* cls, int32_t nslot, hsb_sim_s** out) {
+    if (!cls || !out) {
+        hsb_set_error("hsb_batch_create: null argument");
+        return HSB_ERR_INVALID;
+    }
+    *out = nullptr;
+    const hsb_sim_desc& d = *cls;
+    RC(batch_check_class(d, nslot, "hsb_batch_create"));
+    const long n = (long)d.size[0] * d.size[1] * d.size[2];
+    hsb_sim_s* S = new hsb_sim_s();
+    S->d = d;
+    S->n = n;
+    S->nch = d.ttm ? 5 : 3;
+    S->nslot = nslot;
+    S->batched = true;
+    STRY(cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking));
+    const SlotLayout L = slot_layout(d, n);
+    STRY(cudaMalloc(&S->arena, sizeof(float) * L.total * nslot));
+    point_slot0(S, L);
+    STRY(cudaMalloc(&S->sd, sizeof(HsbSolverDev) * nslot));
+    STRY(cudaMallocHost(&S->sd_host, sizeof(HsbSolverDev) * nslot));
+    memset(S->sd_host, 0, sizeof(HsbSolverDev) * nslot);
+    STRY(cudaMemsetAsync(S->sd, 0, sizeof(HsbSolverDev) * nslot, S->st));
+    STRY(cudaMalloc(&S->phys_dev, sizeof(HsbPhys) * nslot));
+    fill_phys(S);
+    S->phys_h.assign(nslot, S->P);
+    STRY(cudaMemcpyAsync(S->phys_dev, S->phys_h.data(), sizeof(HsbPhys) * nslot, cudaMemcpyHostToDevice, S->st));
+    STRY(cudaMalloc(&S->red, sizeof(double) * (RED_BLOCKS * 8 + 16) + 64));
+    STRY(cudaMallocHost(&S->red_host, sizeof(double) * 16));
+    STRY(cudaEventCreateWithFlags(&S->done_ev, cudaEventDisableTiming));
+    if (d.demag) {
+        int rc = hsb_demag_plan_create(d.size, d.cellsize, d.pbc, 6, S->st, &S->demag);
+        if (rc != HSB_OK) {
+            free_sim(S);
+            return rc;
+        }
+        const long xb = hsb_demag_x1_bytes(S->demag);
+        if (xb == 0) {
+            hsb_set_error("hsb_batch_create: no batched FFT kernels for padded size (%d, %d, %d)",
+                          d.size[0], d.size[1], d.size[2]);
+            free_sim(S);
+            return HSB_ERR_UNSUPPORTED;
+        }
+        STRY(cudaMalloc(&S->X1b, xb * nslot));
+        S->x1_stride = xb / (long)sizeof(float2);
+    }
+    S->bt.stride = S->slot_stride;
+    S->bt.phys = S->phys_dev;
+    S->bt.nslot = nslot;
+    const long tot = n * nslot;
+    S->graph_steps = tot < 65536 ? 16 : (tot < 1048576 ? 8 : 4);
+    if (d.solver == SOLVER_DP45) S->graph_steps = tot < 65536 ? 8 : 4;
+    S->initialized = true;
+    STRY(cudaStreamSynchronize(S->st));
+    *out = S;
+    return HSB_OK;
+}
+
+static int batch_slot_ok(hsb_sim_s* B, int32_t slot, const char* who) {
+    if (!B || !B->batched) {
+        hsb_set_error("%s: not a batch handle", who);
+        return HSB_ERR_INVALID;
+    }
+    if (slot < 0 || slot >= B->nslot) {
+        hsb_set_error("%s: slot %d outside [0, %d)", who, slot, B->nslot);
+        return HSB_ERR_INVALID;
+    }
+    return HSB_OK;
+}
+
+// Load one simulation into a free slot: its descriptor (same class), initial magnetization
+// (3 x ncell FP64, program order; the temperatures of a two-temperature class start at the
+// descriptor's bath temperature) and end time.  Enqueued on the batch's stream; the slot
+// starts stepping with the next hsb_batch_launch.  Host arrays may be reused on return.
+HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* desc, const double* m,
+                               double t_stop) {
+    RC(batch_slot_ok(B, slot, "hsb_batch_admit"));
+    if (!desc || !m || !(t_stop > 0)) {
+        hsb_set_error("hsb_batch_admit: need a descriptor, m and t_stop > 0");
+        return HSB_ERR_INVALID;
+    }
+    const hsb_sim_desc& d = *desc;
+    const hsb_sim_desc& c = B->d;
+    RC(check_desc(d, "hsb_batch_admit"));
+    for (int a = 0; a < 3; a++) {
+        if (d.size[a] != c.size[a] || d.pbc[a] != c.pbc[a]) {
+            hsb_set_error("hsb_batch_admit: grid size / boundaries differ from the class");
+            return HSB_ERR_INVALID;
+        }
+    }
+    if (d.solver != c.solver || d.ttm != c.ttm || d.demag != c.demag || (d.thermal && !c.thermal) ||
+        (c.solver == SOLVER_DP45 && d.rtol != c.rtol)) {
+        hsb_set_error("hsb_batch_admit: solver, tolerance, two-temperature model, demag or thermal field differ "
+                      "from the class");
+        return HSB_ERR_INVALID;
+    }
+    if (c.demag && !same_aspect(d.cellsize, c.cellsize)) {
+        hsb_set_error("hsb_batch_admit: cell aspect ratio differs from the class (the demag spectrum is shared)");
+        return HSB_ERR_INVALID;
+    }
+    const long n = B->n;
+    const long ny = (long)B->nch * n;
+    // pinned staging per slot: a copy from pageable memory may wait for the running graphs
+    static_assert(sizeof(HsbPhys) % 8 == 0 && sizeof(HsbSolverDev) % 8 == 0, "staging layout");
+    const size_t per = sizeof(float) * ny + sizeof(HsbPhys) + sizeof(HsbSolverDev);
+    if (!B->stage_pin) HSB_CUDA_TRY(cudaMallocHost(&B->stage_pin, per * B->nslot));
+    unsigned char* base = (unsigned char*)B->stage_pin + per * slot;
+    float* hy = (float*)base;
+    HsbPhys* hp = (HsbPhys*)(base + sizeof(float) * ny);
+    HsbSolverDev* hs = (HsbSolverDev*)(base + sizeof(float) * ny + sizeof(HsbPhys));
+    // the previous use of this staging (an earlier admission into this slot) completed
+    // before that slot could finish, so it is free to overwrite
+    for (long i = 0; i < 3 * n; i++) hy[i] = (float)m[i];
+    for (long i = 3 * n; i < ny; i++) hy[i] = (float)d.temperature;
+    phys_from_desc(d, B->nch, n, *hp);
+    B->phys_h[slot] = *hp;
+    memset(hs, 0, sizeof(HsbSolverDev));
+    hs->dt = d.dt < t_stop ? d.dt : t_stop;
+    hs->mindt = d.mindt > 0 ? d.mindt : 1e-22;
+    hs->maxdt = d.maxdt > 0 ? d.maxdt : 1e-9;
+    hs->step_stop = -1;
+    hs->t_stop = t_stop;
+    hs->prep = 1;
+    float* y0 = B->y[0] + (long)slot * B->slot_stride;
+    HSB_CUDA_TRY(cudaMemcpyAsync(y0, hy, sizeof(float) * ny, cudaMemcpyHostToDevice, B->st));
+    HSB_CUDA_TRY(cudaMemcpyAsync(B->phys_dev + slot, hp, sizeof(HsbPhys), cudaMemcpyHostToDevice, B->st));
+    HSB_CUDA_TRY(cudaMemcpyAsync(B->sd + slot, hs, sizeof(HsbSolverDev), cudaMemcpyHostToDevice, B->st));
+    B->nprep++;
+    return HSB_OK;
+}
+
+// First-stage data of the newly admitted slots (DP45: demag of y0 with a thermal field,
+// else k1 = f(y0)), gated on their `prep` word, then switch them to active.
+static int prepare_slots(hsb_sim_s* B) {
+    if (!B->nprep) return HSB_OK;
+    B->prep_mode = true;
+    int rc = HSB_OK;
+    if (B->d.solver == SOLVER_DP45) {
+        if (B->d.thermal) {
+            if (B->demag) rc = run_demag(B, nullptr, 0, nullptr, 0);
+        } else {
+            float* hd = B->demag ? B->hd : nullptr;
+            rc = run_demag(B, nullptr, 0, hd, -1);
+            if (rc == HSB_OK) {
+                StageArgs A = empty_args();
+                A.ys = pair(B->y[0], B->y[1], SEL_CUR);
+                A.hd = fixed(hd);
+                A.ytherm = A.ys;
+                A.kout = pair(B->k[0], B->k[6], SEL_K1);
+                A.kself_w = 1.0f;
+                rc = L_stage(B, A);
+            }
+        }
+    }
+    B->prep_mode = false;
+    RC(rc);
+    RC(hsb_launch_activate_prepped(B->sd, B->nslot, B->st));
+    B->nprep = 0;
+    return HSB_OK;
+}
+
+// Enqueue `graphs` launches of the class graph (each a fixed number of attempts for every
+// slot), then a copy of all solver words to the host; hsb_batch_poll reports completion.
+HSB_EXPORT int hsb_batch_launch(hsb_sim_s* B, int32_t graphs) {
+    if (!B || !B->batched || graphs < 0) {
+        hsb_set_error("hsb_batch_launch: bad argument");
+        return HSB_ERR_INVALID;
+    }
+    RC(prepare_slots(B));
+    RC(build_graph(B));
+    for (int g = 0; g < graphs; g++) HSB_CUDA_TRY(cudaGraphLaunch(B->graph, B->st));
+    HSB_CUDA_TRY(cudaMemcpyAsync(B->sd_host, B->sd, sizeof(HsbSolverDev) * B->nslot, cudaMemcpyDeviceToHost,
+                                 B->st));
+    HSB_CUDA_TRY(cudaEventRecord(B->done_ev, B->st));
+    B->launched = true;
+    return HSB_OK;
+}
+
+// *done = 1 once everything enqueued by the last hsb_batch_launch has finished.
+HSB_EXPORT int hsb_batch_poll(hsb_sim_s* B, int32_t* done) {
+    if (!B || !B->batched || !done) return HSB_ERR_INVALID;
+    if (!B->launched) {
+        *done = 1;
+        return HSB_OK;
+    }
+    cudaError_t e = cudaEventQuery(B->done_ev);
+    if (e == cudaErrorNotReady) {
+        *done = 0;
+        return HSB_OK;
+    }
+    HSB_CUDA_TRY(e);
+    *done = 1;
+    return HSB_OK;
+}
+
+// Solver state of a slot as of the end of the last launch (waits for it).
+HSB_EXPORT int hsb_batch_slot_status(hsb_sim_s* B, int32_t slot, double* t, double* dt, int64_t* steps,
+                                     int64_t* attempts, int64_t* rejects, int32_t* status, int32_t* active) {
+    RC(batch_slot_ok(B, slot, "hsb_batch_slot_status"));
+    if (B->launched) HSB_CUDA_TRY(cudaEventSynchronize(B->done_ev));
+    const HsbSolverDev* h = B->sd_host + slot;
+    if (t) *t = h->t;
+    if (dt) *dt = h->dt;
+    if (steps) *steps = h->step;
+    if (attempts) *attempts = h->attempts;
+    if (rejects) *rejects = h->rejects;
+    if (status) *status = h->status;
+    if (active) *active = h->active | h->prep;
+    return HSB_OK;
+}
+
+// Copy a slot's current m / Te / Tl to the host (FP64, program order); waits for the stream.
+HSB_EXPORT int hsb_batch_slot_get(hsb_sim_s* B, int32_t slot, const char* name, double* host, int64_t count) {
+    RC(batch_slot_ok(B, slot, "hsb_batch_slot_get"));
+    if (!name || !host) {
+        hsb_set_error("hsb_batch_slot_get: null argument");
+        return HSB_ERR_INVALID;
+    }
+    int first, nc;
+    RC(channel_of(B, name, &first, &nc));
+    if (count != (int64_t)nc * B->n) {
+        hsb_set_error("hsb_batch_slot_get(%s): expected %ld values, got %ld", name, (long)nc * B->n, (long)count);
+        return HSB_ERR_INVALID;
+    }
+    RC(stage_buffers(B, count));
+    HsbSolverDev h;
+    HSB_CUDA_TRY(cudaMemcpyAsync(&h, B->sd + slot, sizeof(HsbSolverDev), cudaMemcpyDeviceToHost, B->st));
+    HSB_CUDA_TRY(cudaStreamSynchronize(B->st));
+    const float* src = B->y[h.cur] + (long)slot * B->slot_stride + (long)first * B->n;
+    k_f2d<<<hsb_grid_1d(count, 256), 256, 0, B->st>>>(src, B->stage_d, count);
+    HSB_CUDA_TRY(cudaGetLastError());
+    HSB_CUDA_TRY(cudaMemcpyAsync(host, B->stage_d, sizeof(double) * count, cudaMemcpyDeviceToHost, B->st));
+    HSB_CUDA_TRY(cudaStreamSynchronize(B->st));
+    return HSB_OK;
+}
+
+// Stop a slot (it stays inactive until the next admission into it).
+HSB_EXPORT int hsb_batch_release(hsb_sim_s* B, int32_t slot) {
+    RC(batch_slot_ok(B, slot, "hsb_batch_release"));
+    HSB_CUDA_TRY(cudaMemsetAsync(&B->sd[slot].active, 0, sizeof(int), B->st));
+    HSB_CUDA_TRY(cudaMemsetAsync(&B->sd[slot].prep, 0, sizeof(int), B->st));
+    HSB_CUDA_TRY(cudaStreamSynchronize(B->st));
+    return HSB_OK;
+}
+
+HSB_EXPORT int hsb_batch_destroy(hsb_sim_s* B) { return hsb_sim_destroy(B); }
+
+// Slots, attempts of every slot per class-graph launch, cells per slot.
+HSB_EXPORT int hsb_batch_info(hsb_sim_s* B, int32_t* nslot, int32_t* attempts_per_graph, int64_t* ncell) {
+    if (!B || !B->batched) return HSB_ERR_INVALID;
+    if (nslot) *nslot = B->nslot;
+    if (attempts_per_graph) *attempts_per_graph = B->graph_steps;
+    if (ncell) *ncell = B->n;
     return HSB_OK;
 }

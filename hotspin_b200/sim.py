@@ -121,6 +121,90 @@ class Simulation:
         return np.array(list(a))
 
 
+class Batch:
+    """A size class of simulations advanced together (hsb_batch_* in include/hotspin_b200.h).
+
+    ``cls`` holds the class-wide descriptor fields (size, pbc, cellsize for the cell's aspect
+    ratio, solver, rtol, demag, ttm, thermal); slots are loaded with ``admit``.
+    """
+
+    def __init__(self, nslot, **cls):
+        self._lib = _lib.load()
+        self.desc = make_desc(**cls)
+        self.size = tuple(self.desc.size)
+        self.ncell = int(np.prod(self.size))
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.hsb_batch_create(ctypes.byref(self.desc), int(nslot), ctypes.byref(h)),
+                   "hsb_batch_create")
+        self._h = h
+        ns, ap, nc = _lib.c_i32(), _lib.c_i32(), _lib.c_i64()
+        _lib.check(self._lib.hsb_batch_info(h, ctypes.byref(ns), ctypes.byref(ap), ctypes.byref(nc)),
+                   "hsb_batch_info")
+        self.nslot, self.attempts_per_graph = ns.value, ap.value
+
+    @staticmethod
+    def footprint(nslot, **cls):
+        lib = _lib.load()
+        d = make_desc(**cls)
+        b = _lib.c_i64()
+        _lib.check(lib.hsb_batch_footprint(ctypes.byref(d), int(nslot), ctypes.byref(b)), "hsb_batch_footprint")
+        return b.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hsb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def admit(self, slot, m, t_stop, **kw):
+        """Load a simulation (descriptor keywords as for Simulation) with initial m into `slot`."""
+        d = make_desc(**kw)
+        a = np.ascontiguousarray(m, dtype=np.float64)
+        if a.size != 3 * self.ncell:
+            raise ValueError("m must hold 3 x %d values" % self.ncell)
+        _lib.check(self._lib.hsb_batch_admit(self._h, int(slot), ctypes.byref(d), a.ctypes.data_as(_lib.c_dp),
+                                             float(t_stop)), "hsb_batch_admit")
+
+    def launch(self, graphs=1):
+        _lib.check(self._lib.hsb_batch_launch(self._h, int(graphs)), "hsb_batch_launch")
+
+    def poll(self):
+        d = _lib.c_i32()
+        _lib.check(self._lib.hsb_batch_poll(self._h, ctypes.byref(d)), "hsb_batch_poll")
+        return bool(d.value)
+
+    def slot_status(self, slot):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        st, at, rj = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        s, a = ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(self._lib.hsb_batch_slot_status(self._h, int(slot), ctypes.byref(t), ctypes.byref(dt),
+                                                   ctypes.byref(st), ctypes.byref(at), ctypes.byref(rj),
+                                                   ctypes.byref(s), ctypes.byref(a)), "hsb_batch_slot_status")
+        return dict(t=t.value, dt=dt.value, steps=st.value, attempts=at.value, rejects=rj.value,
+                    status=s.value, active=bool(a.value))
+
+    def slot_get(self, slot, name="m"):
+        ncomp = {"m": 3, "Te": 1, "Tl": 1}[name]
+        out = np.empty((ncomp,) + self.size if ncomp > 1 else self.size, dtype=np.float64)
+        _lib.check(self._lib.hsb_batch_slot_get(self._h, int(slot), name.encode(), out.ctypes.data_as(_lib.c_dp),
+                                                out.size), "hsb_batch_slot_get(%s)" % name)
+        return out
+
+    def release(self, slot):
+        _lib.check(self._lib.hsb_batch_release(self._h, int(slot)), "hsb_batch_release")
+
+
 def demag_plan(size, cellsize, pbc=(0, 0, 0), accuracy=6, stream=None):
     """Create a demag plan; returns an opaque handle (ctypes.c_void_p)."""
     lib = _lib.load()

@@ -150,6 +150,43 @@ int hsb_average_m_noalloc(const float* m, int64_t ncell, double* avg3, void* str
 /* The handle's CUDA stream (cudaStream_t) for callers that interleave their own work. */
 void* hsb_sim_stream(hsb_sim sim);
 
+/* ---- Batches of simulations (no reference counterpart: hotspin runs one simulation per
+ * process, engine/engine.go).  A batch is a size class: up to nslot independent simulations
+ * of one grid size, boundary conditions, solver (and tolerance), channel count and cell
+ * aspect ratio, advanced together by the same kernels (one grid plane per slot) and CUDA
+ * graph.  Per slot: Ms0, lex, cell size, damping, field, anisotropy, temperature, LLB/LLG
+ * (llb, normalize), thermal field and seed.  Not supported in batches: masks, a2 sizes that
+ * are not multiples of 4, padded sizes outside the fast FFT kernels.
+ *
+ * A slot's trajectory is independent of what the other slots hold: every kernel reads and
+ * writes only its own slot's arena and solver word.  A serving loop admits requests into free
+ * slots (hsb_batch_admit), launches (hsb_batch_launch, asynchronous), polls for completion
+ * (hsb_batch_poll), reads each slot's progress (hsb_batch_slot_status; active = 0 once its
+ * end time is reached) and collects results (hsb_batch_slot_get).  One host thread per batch
+ * handle; different handles may be driven from one thread and overlap on the GPU. */
+typedef struct hsb_batch_s* hsb_batch;
+/* Device bytes of a batch with `nslot` slots of the class `cls` (admission by footprint). */
+int hsb_batch_footprint(const hsb_sim_desc* cls, int32_t nslot, int64_t* bytes);
+int hsb_batch_create(const hsb_sim_desc* cls, int32_t nslot, hsb_batch* out);
+int hsb_batch_destroy(hsb_batch b);
+/* nslot, attempts of every slot per graph launch, cells per slot */
+int hsb_batch_info(hsb_batch b, int32_t* nslot, int32_t* attempts_per_graph, int64_t* ncell);
+/* Load a simulation into a free slot: descriptor of the same class, initial m (3 x ncell
+ * FP64, program order), end time t_stop (s).  Enqueued; host arrays may be reused at once. */
+int hsb_batch_admit(hsb_batch b, int32_t slot, const hsb_sim_desc* desc, const double* m, double t_stop);
+/* Prepare newly admitted slots, enqueue `graphs` launches of the class graph and a copy of
+ * every slot's solver state to the host.  Returns without waiting. */
+int hsb_batch_launch(hsb_batch b, int32_t graphs);
+/* *done = 1 when everything the last hsb_batch_launch enqueued has finished. */
+int hsb_batch_poll(hsb_batch b, int32_t* done);
+/* A slot's solver state as of the end of the last launch (waits for it). */
+int hsb_batch_slot_status(hsb_batch b, int32_t slot, double* t, double* dt, int64_t* steps,
+                          int64_t* attempts, int64_t* rejects, int32_t* status, int32_t* active);
+/* A slot's m / Te / Tl (FP64, program order). */
+int hsb_batch_slot_get(hsb_batch b, int32_t slot, const char* name, double* host, int64_t count);
+/* Stop a slot until its next admission. */
+int hsb_batch_release(hsb_batch b, int32_t slot);
+
 /* Demag convolution on caller-owned FP32 device arrays (SoA [3][N0][N1][N2]):
  * H (A/m) = Ms0 * K (*) (m * mask); mask may be NULL.  The plan builds the Kernel_Arne
  * tensor (kernel_magnetostatic.go:25-241) on the GPU in FP64 (accuracy as the reference,
