@@ -358,6 +358,7 @@ struct SlotStrides {
     int sel;            // ints between slots' selector / active words
     const float* scale; // per-slot output scale (null: the launch's scale)
     int scale_stride;
+    long kern;          // floats between slots' kernel spectra (0: one shared spectrum)
 };
 
 // R2C along a2 for TY rows per block, B lanes per row; M = L2/2 packed complex points.
@@ -531,6 +532,7 @@ __global__ void __launch_bounds__(384) k_yz4(float2* __restrict__ X1, int N0, in
     const int sl = blockIdx.z;
     if (active && !active[sl * ss.sel]) return;
     X1 += sl * ss.x1;
+    kern += sl * ss.kern;
     constexpr int A = Split<L1>::A, B = Split<L1>::B, SS = Slot<L1>::S;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw);
@@ -715,14 +717,79 @@ static const int XTHREADS = 256;
 static const int SMEM_TILE_BUDGET = 72 * 1024;
 
 // FP64 transform of the kernel and extraction (setup only).
-static int build_kernel_spectrum(hsb_demag_plan_s* P, int accuracy, cudaStream_t st) {
+// FP64 device scratch of one kernel-spectrum evaluation (Kernel_Arne octant, one expanded
+// component, its transform, the imaginary-part maximum).
+struct hsb_demag_spec_s {
+    double* Kc;
+    double* full;
+    double2* X;
+    double2* tw64;
+    double* dmax;
+};
+
+static void spec_free(hsb_demag_spec_s* s) {
+    if (!s) return;
+    cudaFree(s->Kc);
+    cudaFree(s->full);
+    cudaFree(s->X);
+    cudaFree(s->tw64);
+    cudaFree(s->dmax);
+    delete s;
+}
+
+static long spec_nfold(const hsb_demag_plan_s* P) {
+    return (long)(P->L[0] / 2 + 1) * (P->L[1] / 2 + 1) * (P->L[2] / 2 + 1);
+}
+
+long hsb_demag_spectrum_scratch_bytes(hsb_demag_plan P) {
+    const long vol = (long)P->L[0] * P->L[1] * P->L[2];
+    return (long)sizeof(double) * 6 * spec_nfold(P) + (long)sizeof(double) * vol +
+           (long)sizeof(double2) * (long)P->L[0] * P->C2 * P->L[1] + (long)sizeof(double2) * P->twL + 256;
+}
+
+int hsb_demag_spectrum_scratch_create(hsb_demag_plan P, hsb_demag_spec_s** out) {
+    hsb_demag_spec_s* s = new hsb_demag_spec_s();
+    const long vol = (long)P->L[0] * P->L[1] * P->L[2];
+#define STRY2(x)                                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (x);                                                           \
+        if (e_ != cudaSuccess) {                                                        \
+            hsb_set_error("demag spectrum scratch: %s: %s", #x, cudaGetErrorString(e_)); \
+            spec_free(s);                                                               \
+            return e_ == cudaErrorMemoryAllocation ? HSB_ERR_NOMEM : HSB_ERR_CUDA;      \
+        }                                                                               \
+    } while (0)
+    STRY2(cudaMalloc(&s->Kc, sizeof(double) * 6 * spec_nfold(P)));
+    STRY2(cudaMalloc(&s->full, sizeof(double) * vol));
+    STRY2(cudaMalloc(&s->X, sizeof(double2) * (long)P->L[0] * P->C2 * P->L[1]));
+    STRY2(cudaMalloc(&s->dmax, sizeof(double)));
+#undef STRY2
+    if (make_twiddles<double2>(P->twL, &s->tw64) != HSB_OK) {
+        spec_free(s);
+        return HSB_ERR_CUDA;
+    }
+    *out = s;
+    return HSB_OK;
+}
+
+void hsb_demag_spectrum_scratch_destroy(hsb_demag_spec_s* s) { spec_free(s); }
+
+long hsb_demag_kern_floats(hsb_demag_plan P) {
+    return (long)P->C2 * (P->L[1] / 2 + 1) * (P->L[0] / 2 + 1) * 6;
+}
+
+// Enqueue the FP64 Kernel_Arne tensor of the plan's grid for cells of size `cs` and the
+// extraction of its FP32 folded spectrum into `kern` (hsb_demag_kern_floats floats).  The
+// scratch's imaginary-part maximum is reset first and holds this evaluation's afterwards.
+int hsb_demag_spectrum_enqueue(hsb_demag_plan P, const double* cs, int accuracy, hsb_demag_spec_s* s, float* kern,
+                               cudaStream_t st) {
     const int L0 = P->L[0], L1 = P->L[1], L2 = P->L[2];
-    const int h0 = L0 / 2, h1 = L1 / 2, h2 = L2 / 2;
+    const int h0 = L0 / 2, h1 = L1 / 2;
     const int C2 = P->C2;
     ArneGeom g;
     for (int a = 0; a < 3; a++) {
         g.size[a] = P->L[a];
-        g.cs[a] = P->cs[a];
+        g.cs[a] = cs[a];
         g.h[a] = P->L[a] / 2;
         if (P->pbc[a] == 0) {
             g.r1[a] = -(long)((P->L[a] - 1) / 2);
@@ -733,68 +800,53 @@ static int build_kernel_spectrum(hsb_demag_plan_s* P, int accuracy, cudaStream_t
         }
     }
     if (P->L[2] == 1 && P->pbc[2] == 0) g.r2[2] = 0;
-    g.Lmin = fmin(P->cs[0], fmin(P->cs[1], P->cs[2]));
+    g.Lmin = fmin(cs[0], fmin(cs[1], cs[2]));
     g.accuracy = (double)accuracy;
-    const long nfold = (long)(h0 + 1) * (h1 + 1) * (h2 + 1);
-    double* Kc = nullptr;
-    double* full = nullptr;
-    double2* X = nullptr;
-    double2* tw64 = nullptr;
-    double* dmax = nullptr;
-    int rc = HSB_OK;
-    const long vol = (long)L0 * L1 * L2;
-#define TRY(x)                                  \
-    do {                                        \
-        cudaError_t e_ = (x);                   \
-        if (e_ != cudaSuccess) {                \
-            hsb_set_error("demag setup: %s: %s", #x, cudaGetErrorString(e_)); \
-            rc = HSB_ERR_CUDA;                  \
-            goto done;                          \
-        }                                       \
-    } while (0)
-    TRY(cudaMalloc(&Kc, sizeof(double) * 6 * nfold));
-    TRY(cudaMalloc(&full, sizeof(double) * vol));
-    TRY(cudaMalloc(&X, sizeof(double2) * (long)L0 * C2 * L1));
-    TRY(cudaMalloc(&dmax, sizeof(double)));
-    TRY(cudaMemsetAsync(dmax, 0, sizeof(double), st));
-    if (make_twiddles<double2>(P->twL, &tw64) != HSB_OK) { rc = HSB_ERR_CUDA; goto done; }
-    TRY(hsb_arne_launch(&g, Kc, st));
-    {
-        const int M = L2 / 2;
-        const int TY = pick_tile(M, sizeof(double2), SMEM_TILE_BUDGET, 16);
-        const int smx = 2 * TY * fpad_len(M) * (int)sizeof(double2);
-        TRY(cudaFuncSetAttribute(k_fft_x_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
-        const int TB = pick_tile(L1, sizeof(double2), SMEM_TILE_BUDGET, 16);
-        const int smy = 2 * TB * fpad_len(L1) * (int)sizeof(double2);
-        TRY(cudaFuncSetAttribute(k_fft_cols<double, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smy));
-        const int TK = pick_tile(L0, sizeof(double2), SMEM_TILE_BUDGET, 16);
-        const int smz = 2 * TK * fpad_len(L0) * (int)sizeof(double2);
-        TRY(cudaFuncSetAttribute(k_fft_z<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz));
-        const double scale = 1.0 / ((double)L0 * L1 * L2);
-        for (int comp = 0; comp < 6; comp++) {
-            TRY(hsb_arne_expand_launch(Kc, comp, L0, L1, L2, full, st));
-            dim3 gx(hsb_div_up(L1, TY), L0);
-            k_fft_x_fwd<double><<<gx, XTHREADS, smx, st>>>(full, full, nullptr, 0, nullptr, 0, L0, L1, L2, L2, L1, X,
-                                                               tw64, P->twL, TY, nullptr);
-            const long ncol = (long)L0 * C2;
-            k_fft_cols<double, -1><<<hsb_div_up(ncol, TB), XTHREADS, smy, st>>>(X, L1, L1, X, L1, L1, L1,
-                                                                                  ncol, tw64, P->twL, TB, nullptr);
-            dim3 gz(hsb_div_up(L1, TK), C2);
-            k_fft_z<double><<<gz, XTHREADS, smz, st>>>(X, 1, L0, L0, C2, L1, nullptr, 0, tw64, P->twL, TK, nullptr);
-            k_extract<<<hsb_grid_1d((long)C2 * (h1 + 1) * (h0 + 1), 256), 256, 0, st>>>(X, L0, C2, L1, comp, scale,
-                                                                                         P->kern, dmax);
-            TRY(cudaGetLastError());
-        }
-        TRY(cudaMemcpyAsync(&P->kern_max_imag, dmax, sizeof(double), cudaMemcpyDeviceToHost, st));
-        TRY(cudaStreamSynchronize(st));
+    HSB_CUDA_TRY(cudaMemsetAsync(s->dmax, 0, sizeof(double), st));
+    HSB_CUDA_TRY(hsb_arne_launch(&g, s->Kc, st));
+    const int M = L2 / 2;
+    const int TY = pick_tile(M, sizeof(double2), SMEM_TILE_BUDGET, 16);
+    const int smx = 2 * TY * fpad_len(M) * (int)sizeof(double2);
+    HSB_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
+    const int TB = pick_tile(L1, sizeof(double2), SMEM_TILE_BUDGET, 16);
+    const int smy = 2 * TB * fpad_len(L1) * (int)sizeof(double2);
+    HSB_CUDA_TRY(cudaFuncSetAttribute(k_fft_cols<double, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smy));
+    const int TK = pick_tile(L0, sizeof(double2), SMEM_TILE_BUDGET, 16);
+    const int smz = 2 * TK * fpad_len(L0) * (int)sizeof(double2);
+    HSB_CUDA_TRY(cudaFuncSetAttribute(k_fft_z<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz));
+    const double scale = 1.0 / ((double)L0 * L1 * L2);
+    for (int comp = 0; comp < 6; comp++) {
+        HSB_CUDA_TRY(hsb_arne_expand_launch(s->Kc, comp, L0, L1, L2, s->full, st));
+        dim3 gx(hsb_div_up(L1, TY), L0);
+        k_fft_x_fwd<double><<<gx, XTHREADS, smx, st>>>(s->full, s->full, nullptr, 0, nullptr, 0, L0, L1, L2, L2, L1,
+                                                          s->X, s->tw64, P->twL, TY, nullptr);
+        const long ncol = (long)L0 * C2;
+        k_fft_cols<double, -1><<<hsb_div_up(ncol, TB), XTHREADS, smy, st>>>(s->X, L1, L1, s->X, L1, L1, L1, ncol,
+                                                                              s->tw64, P->twL, TB, nullptr);
+        dim3 gz(hsb_div_up(L1, TK), C2);
+        k_fft_z<double><<<gz, XTHREADS, smz, st>>>(s->X, 1, L0, L0, C2, L1, nullptr, 0, s->tw64, P->twL, TK, nullptr);
+        k_extract<<<hsb_grid_1d((long)C2 * (h1 + 1) * (h0 + 1), 256), 256, 0, st>>>(s->X, L0, C2, L1, comp, scale,
+                                                                                     kern, s->dmax);
+        HSB_CUDA_TRY(cudaGetLastError());
     }
-done:
-#undef TRY
-    cudaFree(Kc);
-    cudaFree(full);
-    cudaFree(X);
-    cudaFree(tw64);
-    cudaFree(dmax);
+    return HSB_OK;
+}
+
+// FP64 transform of the kernel and extraction (plan setup).
+static int build_kernel_spectrum(hsb_demag_plan_s* P, int accuracy, cudaStream_t st) {
+    hsb_demag_spec_s* s = nullptr;
+    int rc = hsb_demag_spectrum_scratch_create(P, &s);
+    if (rc != HSB_OK) return rc;
+    rc = hsb_demag_spectrum_enqueue(P, P->cs, accuracy, s, P->kern, st);
+    if (rc == HSB_OK) {
+        cudaError_t e = cudaMemcpyAsync(&P->kern_max_imag, s->dmax, sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            hsb_set_error("demag setup: %s", cudaGetErrorString(e));
+            rc = HSB_ERR_CUDA;
+        }
+    }
+    spec_free(s);
     return rc;
 }
 
@@ -940,8 +992,9 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     const int L0 = P->L[0], L1 = P->L[1], L2 = P->L[2];
     const int C2 = P->C2;
     const long ncell = (long)N0 * N1 * N2;
-    SlotStrides ss = {0, 0, 0, 0, nullptr, 0};
+    SlotStrides ss = {0, 0, 0, 0, nullptr, 0, 0};
     float2* X1 = P->X1;
+    const float* kern = P->kern;
     int nz = 1;
     if (batch) {
         if (!hsb_demag_x1_bytes(P) || mask || !batch->X1 || batch->nslot < 1) {
@@ -957,6 +1010,10 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
         ss.scale_stride = batch->scale_stride;
         X1 = (float2*)batch->X1;
         nz = batch->nslot;
+        if (batch->kern) {
+            kern = batch->kern;
+            ss.kern = batch->kern_stride;
+        }
     }
     if (io.ev) cudaEventRecord(io.ev[0], st);
     if (P->xfwd4) {
@@ -971,7 +1028,7 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     if (io.ev) cudaEventRecord(io.ev[1], st);
     if (P->yz4) {
         dim3 gyz(C2, 1, nz);
-        P->yz4<<<gyz, P->yz4_threads, P->yz4_smem, st>>>(X1, N0, N1, C2, P->kern, P->tw, P->twL, active, ss);
+        P->yz4<<<gyz, P->yz4_threads, P->yz4_smem, st>>>(X1, N0, N1, C2, kern, P->tw, P->twL, active, ss);
     } else if (P->fused) {
         switch (P->lz) {
 #define RUNYZ(LZ) case LZ: k_fft_yz_conv<LZ><<<C2, yz_threads<LZ>::value, P->smem_yz, st>>>(P->X1, N0, N1, L1, C2, P->kern, P->tw, P->twL, active); break;

@@ -45,6 +45,8 @@ struct HsbDemagBatch {
     long x1_stride;            // complex elements between slots' spectra
     const float* scale;
     int scale_stride;          // floats
+    const float* kern;         // per-slot kernel spectra (null: the plan's own for every slot)
+    long kern_stride;          // floats
 };
 
 // `active` (device, nullable): when it points to 0 every kernel returns at once, so a
@@ -53,6 +55,16 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
                      cudaStream_t st, const int* active, const HsbDemagBatch* batch = nullptr);
 // Bytes of one slot's spectrum scratch; 0 when the plan has no batched (fast) kernels.
 long hsb_demag_x1_bytes(hsb_demag_plan P);
+
+// Kernel spectra for other cell sizes on the plan's grid (a batch gives every slot its own,
+// exactly as a plan created for that slot's cells would hold).
+struct hsb_demag_spec_s;
+long hsb_demag_kern_floats(hsb_demag_plan P);
+long hsb_demag_spectrum_scratch_bytes(hsb_demag_plan P);
+int hsb_demag_spectrum_scratch_create(hsb_demag_plan P, hsb_demag_spec_s** out);
+void hsb_demag_spectrum_scratch_destroy(hsb_demag_spec_s* s);
+int hsb_demag_spectrum_enqueue(hsb_demag_plan P, const double* cellsize, int accuracy, hsb_demag_spec_s* s,
+                               float* kern, cudaStream_t st);
 extern "C" int hsb_demag_plan_create(const int* size, const double* cellsize, const int* pbc,
                                      int accuracy, void* stream, hsb_demag_plan* out);
 extern "C" int hsb_demag_plan_destroy(hsb_demag_plan P);

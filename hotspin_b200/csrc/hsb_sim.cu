@@ -85,6 +85,9 @@ struct hsb_sim_s {
     std::vector<HsbPhys> phys_h;
     void* X1b;          // batched: per-slot demag spectra
     long x1_stride;     // complex elements
+    float* kernb;       // batched: per-slot demag kernel spectra (each slot's own cell size)
+    long kern_floats;
+    hsb_demag_spec_s* spec;  // batched: FP64 scratch of the kernel-spectrum evaluation
     BatchArgs bt;
     bool prep_mode;     // enqueueing the preparation of newly admitted slots
     int nprep;          // slots admitted since the last launch
@@ -313,6 +316,8 @@ static int run_demag(hsb_sim_s* S, const float* m, int msel, float* h, int hsel,
         b.x1_stride = S->x1_stride;
         b.scale = &S->phys_dev[0].ms0;
         b.scale_stride = (int)(sizeof(HsbPhys) / sizeof(float));
+        b.kern = S->kernb;
+        b.kern_stride = S->kern_floats;
         rc = hsb_demag_launch(S->demag, io, nullptr, 1.0f, S->st, gate, &b);
     } else {
         rc = hsb_demag_launch(S->demag, io, S->msat_mask, (float)S->d.msat0T0, S->st, gate);
@@ -767,6 +772,8 @@ static void free_sim(hsb_sim_s* S) {
     cudaFree(S->arena);
     cudaFree(S->phys_dev);
     cudaFree(S->X1b);
+    cudaFree(S->kernb);
+    if (S->spec) hsb_demag_spectrum_scratch_destroy(S->spec);
     if (S->done_ev) cudaEventDestroy(S->done_ev);
     cudaFree(S->msat_mask);
     cudaFree(S->lex_mask);
@@ -1165,17 +1172,8 @@ HSB_EXPORT int hsb_sim_average_m(hsb_sim_s* S, double* avg3) {
 // Slots are admitted and read back while the others keep running; a slot that reached its
 // end time, or is empty, costs one early-returning block per launch.  The class fixes the
 // grid size, boundary conditions, solver and its tolerance, channel count (two-temperature
-// model or not), demag on/off and the cell's aspect ratio (the demag tensor of a grid of
-// cells depends only on their shape, so one spectrum serves every slot); everything else
-// (Ms0, lex, cell size, damping, field, anisotropy, temperature, LLB or LLG, seed) is per slot.
-static bool same_aspect(const double* a, const double* b) {
-    for (int i = 1; i < 3; i++) {
-        const double ra = a[i] / a[0], rb = b[i] / b[0];
-        if (fabs(ra - rb) > 1e-9 * fabs(rb)) return false;
-    }
-    return true;
-}
-
+// model or not) and demag on/off; everything else (Ms0, lex, cell size and with it the demag
+// kernel spectrum, damping, field, anisotropy, temperature, LLB or LLG, seed) is per slot.
 static int batch_check_class(const hsb_sim_desc& d, int32_t nslot, const char* who) {
     RC(check_desc(d, who));
     if (nslot < 1 || nslot > 65535) {
@@ -1207,10 +1205,13 @@ HSB_EXPORT int hsb_batch_footprint(const hsb_sim_desc* cls, int32_t nslot, int64
         const long C2 = Lg[2] / 2 + 1;
         const long x1 = 3L * d.size[0] * C2 * d.size[1] * 8;
         b += (int64_t)(nslot + 1) * x1;                                   // batch spectra + the plan's own
-        b += (int64_t)C2 * (Lg[1] / 2 + 1) * (Lg[0] / 2 + 1) * 6 * 4;      // kernel spectrum
+        b += (int64_t)(nslot + 1) * C2 * (Lg[1] / 2 + 1) * (Lg[0] / 2 + 1) * 6 * 4;  // kernel spectra
         int twL = Lg[0] > Lg[1] ? Lg[0] : Lg[1];
         if (Lg[2] > twL) twL = Lg[2];
         b += (int64_t)twL * 8;
+        // FP64 scratch of the per-slot kernel evaluation
+        const int64_t nfold = (int64_t)(Lg[0] / 2 + 1) * (Lg[1] / 2 + 1) * (Lg[2] / 2 + 1);
+        b += 8 * 6 * nfold + 8 * (int64_t)Lg[0] * Lg[1] * Lg[2] + 16 * (int64_t)Lg[0] * C2 * Lg[1] + 16 * twL + 256;
     }
     *bytes = b;
     return HSB_OK;
@@ -1261,6 +1262,13 @@ HSB_EXPORT int hsb_batch_create(const hsb_sim_desc* cls, int32_t nslot, hsb_sim_
         }
         STRY(cudaMalloc(&S->X1b, xb * nslot));
         S->x1_stride = xb / (long)sizeof(float2);
+        S->kern_floats = hsb_demag_kern_floats(S->demag);
+        STRY(cudaMalloc(&S->kernb, sizeof(float) * S->kern_floats * nslot));
+        rc = hsb_demag_spectrum_scratch_create(S->demag, &S->spec);
+        if (rc != HSB_OK) {
+            free_sim(S);
+            return rc;
+        }
     }
     S->bt.stride = S->slot_stride;
     S->bt.phys = S->phys_dev;
@@ -1312,10 +1320,6 @@ HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* d
                       "from the class");
         return HSB_ERR_INVALID;
     }
-    if (c.demag && !same_aspect(d.cellsize, c.cellsize)) {
-        hsb_set_error("hsb_batch_admit: cell aspect ratio differs from the class (the demag spectrum is shared)");
-        return HSB_ERR_INVALID;
-    }
     const long n = B->n;
     const long ny = (long)B->nch * n;
     // pinned staging per slot: a copy from pageable memory may wait for the running graphs
@@ -1343,6 +1347,12 @@ HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* d
     HSB_CUDA_TRY(cudaMemcpyAsync(y0, hy, sizeof(float) * ny, cudaMemcpyHostToDevice, B->st));
     HSB_CUDA_TRY(cudaMemcpyAsync(B->phys_dev + slot, hp, sizeof(HsbPhys), cudaMemcpyHostToDevice, B->st));
     HSB_CUDA_TRY(cudaMemcpyAsync(B->sd + slot, hs, sizeof(HsbSolverDev), cudaMemcpyHostToDevice, B->st));
+    if (B->demag) {
+        // this slot's own demag tensor (the reference evaluates Kernel_Arne in physical units,
+        // so cells of equal shape but different size can round to different quadratures)
+        RC(hsb_demag_spectrum_enqueue(B->demag, d.cellsize, 6, B->spec, B->kernb + (long)slot * B->kern_floats,
+                                      B->st));
+    }
     B->nprep++;
     return HSB_OK;
 }

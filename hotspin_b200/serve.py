@@ -2,10 +2,10 @@
 
 hotspin runs one simulation per process (``engine/engine.go``); serving many independent
 LLG/LLB solves on one GPU is new here.  Requests arrive over time; each belongs to a size
-class (grid size, boundaries, solver and tolerance, channel count, demag, thermal field,
-cell aspect ratio).  A class is one ``Batch``: up to ``nslot`` slots advanced together by
-the same kernels and one captured CUDA graph per class, on its own stream, so classes
-overlap on the GPU.  The loop
+class (grid size, boundaries, solver and tolerance, channel count, demag, thermal field).
+A class is one ``Batch``: up to ``nslot`` slots advanced together by the same kernels and
+one captured CUDA graph per class, on its own stream, so classes overlap on the GPU.  Each
+slot has its own physics, cell size and demag kernel.  The loop
 
 * admits arrived requests into free slots of their class, creating the class when the
   device-memory budget (``Batch.footprint``: state arenas, RK stages, demag spectra and plan)
@@ -66,14 +66,12 @@ CLASS_KEYS = ("size", "pbc", "solver", "rtol", "ttm", "demag", "thermal")
 
 
 def class_key(desc):
-    """Size-class key: what one batch must share (the cell aspect ratio included)."""
-    cs = desc.get("cellsize", (1.0, 1.0, 1.0))
-    aspect = (round(cs[1] / cs[0], 9), round(cs[2] / cs[0], 9))
+    """Size-class key: what one batch must share."""
     vals = []
     for k in CLASS_KEYS:
         v = desc.get(k, 0)
         vals.append(tuple(v) if isinstance(v, (list, tuple)) else v)
-    return tuple(vals) + (aspect,)
+    return tuple(vals)
 
 
 def class_desc(desc):

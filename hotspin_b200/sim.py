@@ -124,8 +124,9 @@ class Simulation:
 class Batch:
     """A size class of simulations advanced together (hsb_batch_* in include/hotspin_b200.h).
 
-    ``cls`` holds the class-wide descriptor fields (size, pbc, cellsize for the cell's aspect
-    ratio, solver, rtol, demag, ttm, thermal); slots are loaded with ``admit``.
+    ``cls`` holds the class-wide descriptor fields (size, pbc, solver, rtol, demag, ttm,
+    thermal; plus valid defaults for the rest); slots are loaded with ``admit``, each with its
+    own descriptor (cell size and demag kernel included).
     """
 
     def __init__(self, nslot, **cls):

@@ -152,10 +152,10 @@ void* hsb_sim_stream(hsb_sim sim);
 
 /* ---- Batches of simulations (no reference counterpart: hotspin runs one simulation per
  * process, engine/engine.go).  A batch is a size class: up to nslot independent simulations
- * of one grid size, boundary conditions, solver (and tolerance), channel count and cell
- * aspect ratio, advanced together by the same kernels (one grid plane per slot) and CUDA
- * graph.  Per slot: Ms0, lex, cell size, damping, field, anisotropy, temperature, LLB/LLG
- * (llb, normalize), thermal field and seed.  Not supported in batches: masks, a2 sizes that
+ * of one grid size, boundary conditions, solver (and tolerance) and channel count, advanced
+ * together by the same kernels (one grid plane per slot) and CUDA graph.  Per slot: Ms0, lex,
+ * cell size (each slot gets the demag kernel of its own cells, evaluated at admission), damping,
+ * field, anisotropy, temperature, LLB/LLG (llb, normalize), thermal field and seed.  Not supported in batches: masks, a2 sizes that
  * are not multiples of 4, padded sizes outside the fast FFT kernels.
  *
  * A slot's trajectory is independent of what the other slots hold: every kernel reads and

@@ -78,6 +78,7 @@ def test_batch_matches_plain_handle():
             st = sim.status()
         dm = float(np.abs(mix[q][0] - m).max())
         assert dm <= 1e-5, (q, dm, st, mix[q][1])
+        assert st["steps"] == mix[q][1]["steps"]
         assert np.isfinite(mix[q][0]).all()
 
 
@@ -86,7 +87,7 @@ def test_batch_rejects_other_class():
         d = dict(REQS[0][0], size=(1, 32, 32))
         with pytest.raises(Exception):
             b.admit(0, np.zeros((3, 1, 32, 32)), 1e-12, **d)
-        d = dict(REQS[0][0], cellsize=(2e-9, 2e-9, 3e-9))
+        d = dict(REQS[0][0], solver="rk4")
         with pytest.raises(Exception):
             b.admit(0, REQS[0][1], 1e-12, **d)
 
@@ -96,7 +97,7 @@ def test_footprint_grows_per_slot():
     f8 = Batch.footprint(8, **CLASS)
     assert 4 * f1 < f8 < 8 * f1 + 1
     ncell = int(np.prod(SIZE))
-    # DP45 with a thermal field: 2 states + 2 stage points + 7 stages (3 ch) + 3 demag-field channels
+    # DP45 with a thermal field: 2 states + 2 stage points + 7 stages (3 ch) + 3 + 6 demag-field channels
     assert (f8 - f1) / 7 >= 4 * ncell * (6 + 6 + 21 + 3 + 6)
 
 
