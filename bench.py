@@ -69,7 +69,7 @@ def algorithmic_bytes(kw, fused=True):
     # DP45 attempt with a thermal field: stage 1 + stages 2..6 + stage 7
     stage = 0
     stage += ncell * (nch * 4 + 12 + nch * 4 + nch * 4)               # s1: ys, hd, write k1, y2
-    for s in range(2, 7):
+    for s in range(2, 7):                                              # ys, hd, y0, k1..k(s-1), write k_s, y(s+1)
         stage += ncell * (nch * 4 + 12 + nch * 4 + nch * 4 * (s - 1) + nch * 4 + nch * 4)
     stage += ncell * (nch * 4 + 12 + nch * 4 + nch * 4 * 6 + nch * 4)  # s7: ys, hd, y0(T), k1..k6, k7
     return {"xfwd": ncell * 12 + spec, "yz": 2 * spec + kern, "xinv": spec + ncell * 12,
@@ -228,8 +228,9 @@ def run_ours(args):
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         traffic = json.load(open(tp)).get(dom)
-    names = {"stage": "k_stage<5> (fused RHS + DP45 stage)", "yz": "k_fft_yz_conv<8> (y/z FFT + tensor multiply)",
-             "xfwd": "k_fft_x_fwd<float> (R2C + transpose)", "xinv": "k_fft_x_inv (C2R)"}
+    names = {"stage": "k_stage4<5> (fused RHS + DP45 stage, float4 cells)",
+             "yz": "k_yz4<1024,8> (y/z FFT + tensor multiply + inverse)",
+             "xfwd": "k_xfwd4<512> (R2C + transpose)", "xinv": "k_xinv4<512> (C2R)"}
     roof = {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1), "peak": peak,
             "peak_kind": kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
             "algorithmic_bytes_per_launch": int(byt / nlaunch),

@@ -13,6 +13,7 @@
 // point / the new state, renormalise m, accumulate the error norm).  Storage is FP32 SoA
 // [channel][a0][a1][a2]; the error norm is a max-norm (exact in any precision).
 #include <math.h>
+#include <string.h>
 
 #include "hsb_common.cuh"
 #include "hsb_llg.cuh"
@@ -593,6 +594,319 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const __grid_constant__ HsbPh
     if (bad) atomicOr(&sd->nonfinite, 1u);
 }
 
+// ------------------------------------------------------------------ load-first variant
+// Same right-hand side as k_stage4 with W consecutive cells along a2 per thread, arranged so
+// that a thread's global loads are issued back to back and consumed afterwards: (A) the
+// stage derivatives the stage sums over (a compacted list of the nonzero coefficients, NK
+// known at compile time) and the base state, (B) the state, its six neighbours and the demag
+// field, all without data-dependent branches (an unused neighbour or field reads the cell
+// itself and is discarded by a select).  Stores come last.  Two load round trips per cell
+// instead of one per stage derivative and per stencil direction.  The stage combination is
+// formed as (ybase + dt sum_j c_j k_j) + (dt c_s) k_s; the error estimate as
+// (sum_j e_j k_j) + e_s k_s.
+struct KList {
+    PtrSel p[HSB_MAXK];
+    float c[HSB_MAXK];
+};
+
+template <int W>
+__device__ __forceinline__ void ldw(const float* p, float* v) {
+    if (W == 4) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    } else if (W == 2) {
+        const float2 a = __ldg(reinterpret_cast<const float2*>(p));
+        v[0] = a.x; v[1] = a.y;
+    } else {
+        v[0] = __ldg(p);
+    }
+}
+template <int W>
+__device__ __forceinline__ void stw(float* p, const float* v) {
+    if (W == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    else if (W == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    else *p = v[0];
+}
+
+template <int CH, bool BATCH, int W, int NK>
+__global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
+    k_stagec(const __grid_constant__ HsbPhys P0, const StageArgs A, const KList KL, HsbSolverDev* sd0,
+             const BatchArgs Bt) {
+    const int slot = BATCH ? (int)blockIdx.z : 0;
+    HsbSolverDev* sd = sd0 + slot;
+    if (!A.ungated && !(A.prep_gated ? sd->prep : sd->active)) return;
+    const HsbPhys& P = BATCH ? Bt.phys[slot] : P0;
+    const long off = BATCH ? (long)slot * Bt.stride : 0;
+    const int normalize = BATCH ? (A.normalize && P.normalize) : A.normalize;
+    const double t = sd->t;
+    const double dt = sd->dt;
+    const long long step = sd->step;
+    const float* ys = resolve_off(A.ys, sd, off);
+    const float* hdp = resolve_off(A.hd, sd, off);
+    const float* ythp = resolve_off(A.ytherm, sd, off);
+    float* kout = resolve_off(A.kout, sd, off);
+    const float* kaccp = resolve_off(A.kacc, sd, off);
+    float* ynext = resolve_off(A.ynext, sd, off);
+    const float* ybasep = resolve_off(A.ybase, sd, off);
+    const float* yerr0p = resolve_off(A.yerr0, sd, off);
+    const float* kl[NK > 0 ? NK : 1];
+#pragma unroll
+    for (int j = 0; j < NK; j++) kl[j] = resolve_off(KL.p[j], sd, off);
+    // absent inputs read valid memory (the state) and are discarded
+    const bool has_hd = hdp != nullptr, has_kacc = kaccp != nullptr;
+    const bool form_y = ynext != nullptr;
+    const bool form_e = !form_y && A.err;
+    const float* hd = has_hd ? hdp : ys;
+    const float* kacc = has_kacc ? kaccp : ys;
+    const float* ybase = (form_y && ybasep) ? ybasep : ys;
+    const float* yerr0 = yerr0p ? yerr0p : ys;
+    const bool th_field = (CH >= 5) && P.thermal && ythp != nullptr;
+    const float* yth = th_field ? ythp : ys;
+    const double ts = t + (double)A.tfrac * dt;
+    const float fdt = (float)dt;
+    const long n = P.ncell;
+    const long s1 = P.N2, s0 = (long)P.N1 * P.N2;
+    const long ngroups = n / W;
+    const double dte = dt > P.cutoff_dt ? dt : P.cutoff_dt;
+    const float th_amp = (float)(P.th_pre / dte);
+    float laser_t = 0.f;
+    if (CH >= 5 && P.laser_p0 != 0.f) {
+        const float tt = (float)(ts - (double)P.laser_t0);
+        laser_t = P.laser_p0 * expf(-P.laser_c * tt * tt);
+    }
+    float emax = 0.f;
+    bool bad = false;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < ngroups; g += (long)gridDim.x * blockDim.x) {
+        const long i = g * W;
+        const int a2 = (int)(i % P.N2);
+        const long r = i / P.N2;
+        const int a1 = (int)(r % P.N1);
+        const int a0 = (int)(r / P.N1);
+        // ---- (A) stage derivatives and base state
+        float acc[CH][W];
+        {
+            float kv[NK > 0 ? NK : 1][CH][W];
+#pragma unroll
+            for (int j = 0; j < NK; j++)
+#pragma unroll
+                for (int c = 0; c < CH; c++) ldw<W>(kl[j] + c * n + i, kv[j][c]);
+            float bv[CH][W];
+#pragma unroll
+            for (int c = 0; c < CH; c++) ldw<W>(ybase + c * n + i, bv[c]);
+#pragma unroll
+            for (int c = 0; c < CH; c++)
+#pragma unroll
+                for (int q = 0; q < W; q++) {
+                    float sum = 0.f;
+#pragma unroll
+                    for (int j = 0; j < NK; j++) sum += KL.c[j] * kv[j][c][q];
+                    acc[c][q] = form_y ? bv[c][q] + fdt * sum : sum;
+                }
+        }
+        // ---- (B) state, neighbours, demag field
+        float y[CH][W], H[3][W], lapE[W], lapL[W];
+        float ye[CH >= 5 ? 2 : 1][W], thT[W], ka[CH][W];
+        {
+            float hv[3][W], nb[4][CH][W], sl[CH], sr[CH];
+#pragma unroll
+            for (int c = 0; c < CH; c++) ldw<W>(ys + c * n + i, y[c]);
+#pragma unroll
+            for (int c = 0; c < 3; c++) ldw<W>(hd + c * n + i, hv[c]);
+            long nidx[4];
+            {
+                const long im0 = i + (long)(nb_lo(a0, P.N0, P.pbc0) - a0) * s0;
+                const long ip0 = i + (long)(nb_hi(a0, P.N0, P.pbc0) - a0) * s0;
+                const long im1 = i + (long)(nb_lo(a1, P.N1, P.pbc1) - a1) * s1;
+                const long ip1 = i + (long)(nb_hi(a1, P.N1, P.pbc1) - a1) * s1;
+                nidx[0] = im0;
+                nidx[1] = ip0;
+                nidx[2] = im1;
+                nidx[3] = ip1;
+            }
+#pragma unroll
+            for (int d = 0; d < 4; d++)
+#pragma unroll
+                for (int c = 0; c < CH; c++) {
+                    // temperature neighbours only where that diffusion term is on
+                    const float kc = c < 3 ? 1.f : (c == 3 ? P.ke_c[d >> 1] : P.kl_c[d >> 1]);
+                    const long ix = (c < 3 || kc != 0.f) ? nidx[d] : i;
+                    ldw<W>(ys + c * n + ix, nb[d][c]);
+                }
+            const long il = i + (long)(nb_lo(a2, P.N2, P.pbc2) - a2);
+            const long ir = (i + W - 1) + (long)(nb_hi(a2 + W - 1, P.N2, P.pbc2) - (a2 + W - 1));
+#pragma unroll
+            for (int c = 0; c < CH; c++) {
+                sl[c] = __ldg(ys + c * n + il);
+                sr[c] = __ldg(ys + c * n + ir);
+            }
+            if (CH >= 5) {
+#pragma unroll
+                for (int c = 3; c < CH; c++) ldw<W>(yerr0 + c * n + i, ye[c - 3]);
+                ldw<W>(yth + 3 * n + i, thT);
+            }
+#pragma unroll
+            for (int c = 0; c < CH; c++) ldw<W>(kacc + c * n + i, ka[c]);
+            // consume
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int q = 0; q < W; q++) H[c][q] = (has_hd ? hv[c][q] : 0.f) + P.bext[c];
+#pragma unroll
+            for (int q = 0; q < W; q++) lapE[q] = lapL[q] = 0.f;
+#pragma unroll
+            for (int dd = 0; dd < 2; dd++) {
+                const float cx = P.ex_c[dd];
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+#pragma unroll
+                    for (int q = 0; q < W; q++)
+                        H[c][q] += cx * ((nb[2 * dd][c][q] + nb[2 * dd + 1][c][q]) - (y[c][q] + y[c][q]));
+                if (CH >= 5) {
+#pragma unroll
+                    for (int q = 0; q < W; q++) {
+                        lapE[q] += P.ke_c[dd] * ((nb[2 * dd][3][q] + nb[2 * dd + 1][3][q]) - (y[3][q] + y[3][q]));
+                        lapL[q] += P.kl_c[dd] * ((nb[2 * dd][4 % CH][q] + nb[2 * dd + 1][4 % CH][q]) -
+                                                 (y[4 % CH][q] + y[4 % CH][q]));
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CH; c++) {
+                const float cx = c < 3 ? P.ex_c[2] : (c == 3 ? P.ke_c[2] : P.kl_c[2]);
+#pragma unroll
+                for (int q = 0; q < W; q++) {
+                    const float left = q == 0 ? sl[c] : y[c][q - 1];
+                    const float right = q == W - 1 ? sr[c] : y[c][q + 1];
+                    const float v = cx * ((left + right) - (y[c][q] + y[c][q]));
+                    if (c < 3) H[c][q] += v;
+                    else if (c == 3) lapE[q] += v;
+                    else lapL[q] += v;
+                }
+            }
+            if (!th_field) {
+#pragma unroll
+                for (int q = 0; q < W; q++) thT[q] = P.T_uniform;
+            }
+        }
+        float k[CH][W];
+#pragma unroll
+        for (int q = 0; q < W; q++) {
+            const float mx = y[0][q], my = y[1][q], mz = y[2][q];
+            float hx = H[0][q], hy = H[1][q], hz = H[2][q];
+            if (P.ku_pre != 0.f) {
+                const float mu = mx * P.uhat[0] + my * P.uhat[1] + mz * P.uhat[2];
+                hx += P.ku_pre * mu * P.u[0];
+                hy += P.ku_pre * mu * P.u[1];
+                hz += P.ku_pre * mu * P.u[2];
+            }
+            const float Ts = (CH >= 5) ? y[3 % CH][q] : P.T_uniform;
+            if (P.llb) {
+                const float am = sqrtf(mx * mx + my * my + mz * mz);
+                if (am > 1e-30f && Ts > 0.f) {
+                    const float b = P.lf_b / Ts;
+                    float Wv, dW;
+                    mfa_w(P, am * b, Wv, dW);
+                    const float mult = P.lf_pre * Ts * (Wv - am) / dW / am;
+                    hx += mult * mx;
+                    hy += mult * my;
+                    hz += mult * mz;
+                }
+            }
+            if (P.thermal && thT[q] > 0.f) {
+                const float amp = sqrtf(th_amp * thT[q]);
+                float gg[3];
+                philox_normals3((uint32_t)(i + q), (uint64_t)step, P.seed_lo, P.seed_hi, gg);
+                hx += amp * sqrtf(P.lam[0]) * gg[0];
+                hy += amp * sqrtf(P.lam[1]) * gg[1];
+                hz += amp * sqrtf(P.lam[2]) * gg[2];
+            }
+            const float gm = P.gamma;
+            k[0][q] = gm * (-hy * mz + hz * my) + gm * P.lam[0] * hx;
+            k[1][q] = gm * (-hz * mx + hx * mz) + gm * P.lam[1] * hy;
+            k[2][q] = gm * (-hx * my + hy * mx) + gm * P.lam[2] * hz;
+            if (CH >= 5) {
+                const float Te = y[3 % CH][q], Tl = y[4 % CH][q];
+                float Qe = lapE[q] + P.g_ep * (Tl - Te);
+                if (laser_t != 0.f) {
+                    float q2 = laser_t;
+                    if (P.laser_inv2s2 != 0.f) {
+                        const float yy = ((float)a1 + 0.5f - 0.5f * (float)P.N1) * P.cs1;
+                        const float xx = ((float)(a2 + q) + 0.5f - 0.5f * (float)P.N2) * P.cs2;
+                        q2 *= expf(-(xx * xx + yy * yy) * P.laser_inv2s2);
+                    }
+                    Qe += q2;
+                }
+                const float Ce = P.gamma_e * Te;
+                k[3 % CH][q] = (Ce == 0.f) ? 0.f : Qe / Ce;
+                const float Ql = lapL[q] + P.g_ep * (Te - Tl);
+                k[4 % CH][q] = (P.c_l == 0.f) ? 0.f : Ql / P.c_l;
+            }
+        }
+        // ---- stores and the error norm
+        if (kout) {
+#pragma unroll
+            for (int c = 0; c < CH; c++) {
+                float v[W];
+#pragma unroll
+                for (int q = 0; q < W; q++) v[q] = A.kself_w * k[c][q] + (has_kacc ? A.kacc_w * ka[c][q] : 0.f);
+                stw<W>(kout + c * n + i, v);
+            }
+        }
+        if (form_y) {
+            const float cs = fdt * A.cself;
+#pragma unroll
+            for (int c = 0; c < CH; c++)
+#pragma unroll
+                for (int q = 0; q < W; q++) acc[c][q] += cs * k[c][q];
+            if (normalize) {
+#pragma unroll
+                for (int q = 0; q < W; q++) {
+                    const float l2 = acc[0][q] * acc[0][q] + acc[1][q] * acc[1][q] + acc[2][q] * acc[2][q];
+                    const float inv = (l2 == 0.f) ? 0.f : rsqrtf(l2);
+                    acc[0][q] *= inv;
+                    acc[1][q] *= inv;
+                    acc[2][q] *= inv;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CH; c++) {
+#pragma unroll
+                for (int q = 0; q < W; q++) bad |= !isfinite(acc[c][q]);
+                stw<W>(ynext + c * n + i, acc[c]);
+            }
+        } else if (form_e) {
+#pragma unroll
+            for (int c = 0; c < CH; c++)
+#pragma unroll
+                for (int q = 0; q < W; q++) acc[c][q] += A.ceself * k[c][q];
+#pragma unroll
+            for (int q = 0; q < W; q++) {
+                float em = fmaxf(fabsf(acc[0][q]), fmaxf(fabsf(acc[1][q]), fabsf(acc[2][q]))) * fdt / A.rtol;
+                if (!(em == em)) bad = true;
+                emax = fmaxf(emax, em);
+            }
+            if (CH >= 5) {
+#pragma unroll
+                for (int c = 3; c < CH; c++) {
+#pragma unroll
+                    for (int q = 0; q < W; q++) {
+                        const float sc = A.rtol * fmaxf(fabsf(ye[c - 3][q]), fabsf(y[c][q]));
+                        const float ec = fabsf(acc[c][q]) * fdt;
+                        const float em = sc > 0.f ? ec / sc : (ec > 0.f ? INFINITY : 0.f);
+                        if (!(em == em)) bad = true;
+                        emax = fmaxf(emax, em);
+                    }
+                }
+            }
+        }
+    }
+    if (A.err) {
+        emax = warp_max_f(emax);
+        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&sd->err_acc, emax);
+    }
+    if (bad) atomicOr(&sd->nonfinite, 1u);
+}
+
 // Next stage point / new state without a right-hand-side evaluation:
 // ynext = ybase + dt * sum_j ck[j] kin[j] (renormalised in LLG mode).
 template <int CH, bool BATCH>
@@ -694,13 +1008,69 @@ __global__ void k_fixed_advance(HsbSolverDev* sd0, int nslot) {
 }
 
 // ------------------------------------------------------------------------------ launchers
+// Stage-kernel variant for grids without masks: 0 = k_stage4, 1 / 2 / 4 = k_stagec with 1 / 2 /
+// 4 cells per thread (the load-first form).  Set by hsb_set_stage_variant (tuning sweeps).
+static int g_stage_variant = 2;
+
+HSB_EXPORT int hsb_set_stage_variant(int v) {
+    const int old = g_stage_variant;
+    if (v == 0 || v == 1 || v == 2 || v == 4) g_stage_variant = v;
+    return old;
+}
+
+template <int CH, bool BATCH, int W>
+static void launch_c(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt, int nslot,
+                     cudaStream_t st) {
+    // compacted list of the stage derivatives the launch sums over, nonzero coefficients only
+    KList KL;
+    memset(&KL, 0, sizeof(KL));
+    const bool form_y = A.ynext.p[0] || A.ynext.p[1];
+    int nk = 0;
+    for (int j = 0; j < HSB_MAXK; j++) {
+        const float c = form_y ? (j < A.nk ? A.ck[j] : 0.f) : (A.err ? A.ce[j] : 0.f);
+        if (c != 0.f) {
+            KL.p[nk] = A.kin[j];
+            KL.c[nk] = c;
+            nk++;
+        }
+    }
+    const int threads = 256;
+    const int per_sm = W == 1 ? 3 : (W == 2 ? 2 : 1);
+    long g = (P.ncell / W + threads - 1) / threads;
+    const long cap = (long)hsb_sm_count() * per_sm;
+    dim3 grid((unsigned)(g < cap ? g : cap), 1, (unsigned)nslot);
+    switch (nk) {
+#define KC(m) case m: k_stagec<CH, BATCH, W, m><<<grid, threads, 0, st>>>(P, A, KL, sd, Bt); break;
+        KC(0) KC(1) KC(2) KC(3) KC(4) KC(5) KC(6) KC(7)
+#undef KC
+    }
+}
+
+template <int CH, bool BATCH>
+static void launch_vec(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt, int nslot,
+                       cudaStream_t st) {
+    const int v = (A.err && (A.ynext.p[0] || A.ynext.p[1])) ? 0 : g_stage_variant;
+    if (v == 0) {
+        const int threads = 256;
+        long g = (P.ncell / 4 + threads - 1) / threads;
+        const long cap = (long)hsb_sm_count() * 2;
+        dim3 grid((unsigned)(g < cap ? g : cap), 1, (unsigned)nslot);
+        k_stage4<CH, BATCH><<<grid, threads, 0, st>>>(P, A, sd, Bt);
+    } else if (v == 1) {
+        launch_c<CH, BATCH, 1>(P, A, sd, Bt, nslot, st);
+    } else if (v == 2) {
+        launch_c<CH, BATCH, 2>(P, A, sd, Bt, nslot, st);
+    } else {
+        launch_c<CH, BATCH, 4>(P, A, sd, Bt, nslot, st);
+    }
+}
+
 int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st) {
     const int threads = 256;
     if (P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask) {
-        const int grid = hsb_grid_1d(P.ncell / 4, threads, 2);
         BatchArgs nb = {0, nullptr, 1};
-        if (P.nch == 5) k_stage4<5, false><<<grid, threads, 0, st>>>(P, A, sd, nb);
-        else k_stage4<3, false><<<grid, threads, 0, st>>>(P, A, sd, nb);
+        if (P.nch == 5) launch_vec<5, false>(P, A, sd, nb, 1, st);
+        else launch_vec<3, false>(P, A, sd, nb, 1, st);
         return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
     }
     const int grid = hsb_grid_1d(P.ncell, threads, 8);
@@ -728,12 +1098,10 @@ int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st) {
 int hsb_launch_stage_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
                              cudaStream_t st) {
     const int threads = 256;
+    (void)threads;
     if (P.N2 % 4 != 0 || P.msat_mask || P.lex_mask) return HSB_ERR_UNSUPPORTED;
-    long g = (P.ncell / 4 + threads - 1) / threads;
-    const long cap = (long)hsb_sm_count() * 2;
-    dim3 grid((unsigned)(g < cap ? g : cap), 1, (unsigned)Bt.nslot);
-    if (P.nch == 5) k_stage4<5, true><<<grid, threads, 0, st>>>(P, A, sd, Bt);
-    else k_stage4<3, true><<<grid, threads, 0, st>>>(P, A, sd, Bt);
+    if (P.nch == 5) launch_vec<5, true>(P, A, sd, Bt, Bt.nslot, st);
+    else launch_vec<3, true>(P, A, sd, Bt, Bt.nslot, st);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }
 

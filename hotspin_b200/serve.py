@@ -266,7 +266,7 @@ def equilibrium_m_half(T, Tc):
     return 0.5 * (lo + hi)
 
 
-def make_requests(n=256, rate=50.0, seed=7, t_end=50e-12, sides=(32, 64, 128, 256, 512), layers=(1, 2),
+def make_requests(n=256, rate=50.0, seed=4, t_end=50e-12, sides=(32, 64, 128, 256, 512), layers=(1, 2),
                   llb_min_T=300.0, tc=630.0, a_ex=1.3e-11, rtol=1e-5):
     """Poisson stream of independent LLG/LLB requests with seeded parameters.
 
