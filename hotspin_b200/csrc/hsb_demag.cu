@@ -368,7 +368,8 @@ __global__ void __launch_bounds__(256) k_xfwd4(const float* __restrict__ in0, co
                                                const float* __restrict__ mask, long in_cstride,
                                                int planes_per_comp, int N1, int N2, int ldo,
                                                float2* __restrict__ out, const float2* __restrict__ tw, int twL,
-                                               int TY, const int* __restrict__ active, const SlotStrides ss) {
+                                               const float2* __restrict__ tw4, int TY,
+                                               const int* __restrict__ active, const SlotStrides ss) {
     const int sl = blockIdx.z;
     if (active && !active[sl * ss.sel]) return;
     in0 += sl * ss.in;
@@ -419,7 +420,7 @@ __global__ void __launch_bounds__(256) k_xfwd4(const float* __restrict__ in0, co
             v[n1] = make_float2(a, b);
         }
     }
-    fft4<M, -1>(v, slot, lane, tw, twL);
+    fft4<M, -1>(v, slot, lane, tw4);
     // natural order Z[k] into the slot
 #pragma unroll
     for (int j = 0; j < A; j++) slot[fft4_out_index<M>(lane, j)] = v[j];
@@ -458,7 +459,8 @@ template <int M>
 __global__ void __launch_bounds__(256) k_xinv4(const float2* __restrict__ in, int ldi, int planes_per_comp, int N1,
                                                int N2, float* __restrict__ out0, float* __restrict__ out1,
                                                const int* __restrict__ osel, int oinv, long out_cstride,
-                                               float scale, const float2* __restrict__ tw, int twL, int TY,
+                                               float scale, const float2* __restrict__ tw, int twL,
+                                               const float2* __restrict__ tw4, int TY,
                                                const int* __restrict__ active, const SlotStrides ss) {
     const int sl = blockIdx.z;
     if (active && !active[sl * ss.sel]) return;
@@ -503,7 +505,7 @@ __global__ void __launch_bounds__(256) k_xinv4(const float2* __restrict__ in, in
         v[n1] = make_float2(sA.x - wd.y, sA.y + wd.x);
     }
     __syncwarp();
-    fft4<M, +1>(v, slot, lane, tw, twL);
+    fft4<M, +1>(v, slot, lane, tw4);
     float* out = (osel && ((*osel) ^ oinv)) ? out1 : out0;
     if (r < ny) {
         float* dst = out + comp * out_cstride + ((long)a0 * N1 + y0 + r) * N2;
@@ -527,12 +529,12 @@ __global__ void __launch_bounds__(256) k_xinv4(const float2* __restrict__ in, in
 // 3*N0 sequences of length L1 (B lanes each), z in registers (LZ = L0 <= 16).
 template <int L1, int LZ>
 __global__ void __launch_bounds__(384) k_yz4(float2* __restrict__ X1, int N0, int N1, int C2,
-                                             const float* __restrict__ kern, const float2* __restrict__ tw,
-                                             int twL, const int* __restrict__ active, const SlotStrides ss) {
+                                             const float* __restrict__ kern4, const float2* __restrict__ tw4,
+                                             const int* __restrict__ active, const SlotStrides ss) {
     const int sl = blockIdx.z;
     if (active && !active[sl * ss.sel]) return;
     X1 += sl * ss.x1;
-    kern += sl * ss.kern;
+    kern4 += sl * ss.kern;
     constexpr int A = Split<L1>::A, B = Split<L1>::B, SS = Slot<L1>::S;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw);
@@ -552,7 +554,7 @@ __global__ void __launch_bounds__(384) k_yz4(float2* __restrict__ X1, int N0, in
         const int n = B * n1 + lane;
         v[n1] = (n < N1) ? src[n] : make_float2(0.f, 0.f);
     }
-    fft4<L1, -1>(v, slot, lane, tw, twL, wmask);
+    fft4<L1, -1>(v, slot, lane, tw4, wmask);
 #pragma unroll
     for (int j = 0; j < A; j++) slot[fft4_out_index<L1>(lane, j)] = v[j];
     __syncthreads();
@@ -567,14 +569,17 @@ __global__ void __launch_bounds__(384) k_yz4(float2* __restrict__ X1, int N0, in
         for (int c = 0; c < 3; c++) fft_reg64<LZ, -1>(w[c]);
         const int f1 = k1 > h1 ? L1 - k1 : k1;
         const float s1 = k1 > h1 ? -1.f : 1.f;
-        const float* Kb = kern + ((long)kx * (h1 + 1) + f1) * (h0 + 1) * 6;
+        // kern4 layout [kx][f0][component][f1]: consecutive k1 read consecutive words
+        const float* Kb = kern4 + (long)kx * (h0 + 1) * 6 * (h1 + 1) + f1;
 #pragma unroll
         for (int k0 = 0; k0 < LZ; k0++) {
             const int f0 = k0 > h0 ? LZ - k0 : k0;
             const float s0 = k0 > h0 ? -1.f : 1.f;
-            const float* K = Kb + f0 * 6;
-            const float kxx = __ldg(K + KXX), kyy = __ldg(K + KYY), kzz = __ldg(K + KZZ);
-            const float kyz = s1 * __ldg(K + KYZ), kxz = s0 * __ldg(K + KXZ), kxy = s0 * s1 * __ldg(K + KXY);
+            const float* K = Kb + (long)f0 * 6 * (h1 + 1);
+            const long cs = h1 + 1;
+            const float kxx = __ldg(K + KXX * cs), kyy = __ldg(K + KYY * cs), kzz = __ldg(K + KZZ * cs);
+            const float kyz = s1 * __ldg(K + KYZ * cs), kxz = s0 * __ldg(K + KXZ * cs),
+                        kxy = s0 * s1 * __ldg(K + KXY * cs);
             const float2 m0 = w[0][k0], m1 = w[1][k0], m2 = w[2][k0];
             w[0][k0] = make_float2(kxx * m0.x + kxy * m1.x + kxz * m2.x, kxx * m0.y + kxy * m1.y + kxz * m2.y);
             w[1][k0] = make_float2(kxy * m0.x + kyy * m1.x + kyz * m2.x, kxy * m0.y + kyy * m1.y + kyz * m2.y);
@@ -592,7 +597,7 @@ __global__ void __launch_bounds__(384) k_yz4(float2* __restrict__ X1, int N0, in
 #pragma unroll
     for (int n1 = 0; n1 < A; n1++) v[n1] = slot[B * n1 + lane];
     __syncwarp(wmask);
-    fft4<L1, +1>(v, slot, lane, tw, twL, wmask);
+    fft4<L1, +1>(v, slot, lane, tw4, wmask);
     float2* dst = X1 + ((long)col * C2 + kx) * N1;
 #pragma unroll
     for (int j = 0; j < A; j++) {
@@ -603,10 +608,10 @@ __global__ void __launch_bounds__(384) k_yz4(float2* __restrict__ X1, int N0, in
 
 // Dispatch tables for the fast kernels.
 typedef void (*xfwd4_fn)(const float*, const float*, const int*, int, const float*, long, int, int, int, int,
-                         float2*, const float2*, int, int, const int*, const SlotStrides);
+                         float2*, const float2*, int, const float2*, int, const int*, const SlotStrides);
 typedef void (*xinv4_fn)(const float2*, int, int, int, int, float*, float*, const int*, int, long, float,
-                         const float2*, int, int, const int*, const SlotStrides);
-typedef void (*yz4_fn)(float2*, int, int, int, const float*, const float2*, int, const int*, const SlotStrides);
+                         const float2*, int, const float2*, int, const int*, const SlotStrides);
+typedef void (*yz4_fn)(float2*, int, int, int, const float*, const float2*, const int*, const SlotStrides);
 
 static xfwd4_fn xfwd4_for(int M, int* B, int* S) {
     switch (M) {
@@ -647,7 +652,8 @@ static yz4_fn yz4_for(int L1, int LZ, int* B, int* S) {
 // ------------------------------------------------------------------------------ extract
 // Real part of the folded octant of one transformed component, scaled, into kern.
 __global__ void k_extract(const double2* __restrict__ X, int L0, int C2, int L1, int comp,
-                          double scale, float* __restrict__ kern, double* __restrict__ maximag) {
+                          double scale, float* __restrict__ kern, float* __restrict__ kern4,
+                          double* __restrict__ maximag) {
     const int h0 = L0 / 2, h1 = L1 / 2;
     const long tot = (long)C2 * (h1 + 1) * (h0 + 1);
     double mi = 0;
@@ -656,7 +662,9 @@ __global__ void k_extract(const double2* __restrict__ X, int L0, int C2, int L1,
         const int f1 = (int)((q / (h0 + 1)) % (h1 + 1));
         const int kx = (int)(q / ((long)(h0 + 1) * (h1 + 1)));
         const double2 v = X[((long)f0 * C2 + kx) * L1 + f1];
-        kern[q * 6 + comp] = (float)(v.x * scale);
+        const float kv = (float)(v.x * scale);
+        if (kern) kern[q * 6 + comp] = kv;
+        if (kern4) kern4[(((long)kx * (h0 + 1) + f0) * 6 + comp) * (h1 + 1) + f1] = kv;
         mi = fmax(mi, fabs(v.y * scale));
     }
     mi = warp_max_d(mi);
@@ -674,6 +682,9 @@ struct hsb_demag_plan_s {
     int fused;          // 1 = single yz kernel
     int lz;             // compile-time z length for the fused kernel
     float* kern;        // [C2][L1/2+1][L0/2+1][6]
+    float* kern4;       // the same values as [C2][L0/2+1][6][L1/2+1] (fast y/z kernel)
+    float2* tw4x;       // four-step twiddle matrices of the x (length L2/2) and y (L1) transforms
+    float2* tw4y;
     float2* X1;         // [3][N0][C2][N1]
     float2* X2;         // multipass: [3][N0][C2][L1]
     float2* tw;
@@ -710,6 +721,22 @@ static int make_twiddles(int twL, C** out) {
     }
     HSB_CUDA_TRY(cudaMalloc((void**)out, sizeof(C) * twL));
     HSB_CUDA_TRY(cudaMemcpy(*out, h.data(), sizeof(C) * twL, cudaMemcpyHostToDevice));
+    return HSB_OK;
+}
+
+// Four-step twiddle matrix of length L: [k1 B + n2] = the table entry tw[(n2 k1 mod L) twL / L],
+// computed by the same expression as make_twiddles so both give identical values.
+static int make_tw4(int L, int B, int twL, float2** out) {
+    const int A = L / B, ts = twL / L;
+    std::vector<float2> h((size_t)A * B);
+    for (int k1 = 0; k1 < A; k1++)
+        for (int n2 = 0; n2 < B; n2++) {
+            const int j = ((n2 * k1) & (L - 1)) * ts;
+            const double a = -2.0 * M_PI * (double)j / (double)twL;
+            h[(size_t)k1 * B + n2] = make_float2((float)cos(a), (float)sin(a));
+        }
+    HSB_CUDA_TRY(cudaMalloc((void**)out, sizeof(float2) * h.size()));
+    HSB_CUDA_TRY(cudaMemcpy(*out, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
     return HSB_OK;
 }
 
@@ -779,10 +806,11 @@ long hsb_demag_kern_floats(hsb_demag_plan P) {
 }
 
 // Enqueue the FP64 Kernel_Arne tensor of the plan's grid for cells of size `cs` and the
-// extraction of its FP32 folded spectrum into `kern` (hsb_demag_kern_floats floats).  The
+// extraction of its FP32 folded spectrum into `kern` and / or `kern4` (the fast y/z kernel's
+// layout; either may be null; hsb_demag_kern_floats floats each).  The
 // scratch's imaginary-part maximum is reset first and holds this evaluation's afterwards.
 int hsb_demag_spectrum_enqueue(hsb_demag_plan P, const double* cs, int accuracy, hsb_demag_spec_s* s, float* kern,
-                               cudaStream_t st) {
+                               float* kern4, cudaStream_t st) {
     const int L0 = P->L[0], L1 = P->L[1], L2 = P->L[2];
     const int h0 = L0 / 2, h1 = L1 / 2;
     const int C2 = P->C2;
@@ -826,7 +854,7 @@ int hsb_demag_spectrum_enqueue(hsb_demag_plan P, const double* cs, int accuracy,
         dim3 gz(hsb_div_up(L1, TK), C2);
         k_fft_z<double><<<gz, XTHREADS, smz, st>>>(s->X, 1, L0, L0, C2, L1, nullptr, 0, s->tw64, P->twL, TK, nullptr);
         k_extract<<<hsb_grid_1d((long)C2 * (h1 + 1) * (h0 + 1), 256), 256, 0, st>>>(s->X, L0, C2, L1, comp, scale,
-                                                                                     kern, s->dmax);
+                                                                                     kern, kern4, s->dmax);
         HSB_CUDA_TRY(cudaGetLastError());
     }
     return HSB_OK;
@@ -837,7 +865,7 @@ static int build_kernel_spectrum(hsb_demag_plan_s* P, int accuracy, cudaStream_t
     hsb_demag_spec_s* s = nullptr;
     int rc = hsb_demag_spectrum_scratch_create(P, &s);
     if (rc != HSB_OK) return rc;
-    rc = hsb_demag_spectrum_enqueue(P, P->cs, accuracy, s, P->kern, st);
+    rc = hsb_demag_spectrum_enqueue(P, P->cs, accuracy, s, P->kern, P->kern4, st);
     if (rc == HSB_OK) {
         cudaError_t e = cudaMemcpyAsync(&P->kern_max_imag, s->dmax, sizeof(double), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -935,6 +963,8 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
         if (xf && B > 0) {
             P->xfwd4 = xf;
             P->xinv4 = xinv4_for(M);
+            rc = make_tw4(M, B, P->twL, &P->tw4x);
+            if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }
             P->x4_rows = 256 / B;
             P->x4_threads = 256;
             P->x4_smem = P->x4_rows * S * (int)sizeof(float2);
@@ -945,6 +975,9 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
         yz4_fn yf = (L0 <= 16) ? yz4_for(L1, L0, &By, &Sy) : nullptr;
         if (yf && 3 * N0 * By <= 384 && 3 * N0 * Sy * (int)sizeof(float2) <= 110 * 1024) {
             P->yz4 = yf;
+            PTRY(cudaMalloc(&P->kern4, sizeof(float) * kcount));
+            rc = make_tw4(L1, By, P->twL, &P->tw4y);
+            if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }
             P->yz4_threads = 3 * N0 * By;
             P->yz4_smem = 3 * N0 * Sy * (int)sizeof(float2);
             PTRY(cudaFuncSetAttribute(P->yz4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->yz4_smem));
@@ -963,6 +996,9 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
 HSB_EXPORT int hsb_demag_plan_destroy(hsb_demag_plan P) {
     if (!P) return HSB_OK;
     cudaFree(P->kern);
+    cudaFree(P->kern4);
+    cudaFree(P->tw4x);
+    cudaFree(P->tw4y);
     cudaFree(P->X1);
     cudaFree(P->X2);
     cudaFree(P->tw);
@@ -994,7 +1030,7 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     const long ncell = (long)N0 * N1 * N2;
     SlotStrides ss = {0, 0, 0, 0, nullptr, 0, 0};
     float2* X1 = P->X1;
-    const float* kern = P->kern;
+    const float* kern = P->kern4;
     int nz = 1;
     if (batch) {
         if (!hsb_demag_x1_bytes(P) || mask || !batch->X1 || batch->nslot < 1) {
@@ -1019,7 +1055,7 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     if (P->xfwd4) {
         dim3 gx(hsb_div_up(N1, P->x4_rows), 3 * N0, nz);
         P->xfwd4<<<gx, P->x4_threads, P->x4_smem, st>>>(io.m[0], io.m[1], io.msel, io.minv, mask, ncell, N0, N1, N2,
-                                                        N1, X1, P->tw, P->twL, P->x4_rows, active, ss);
+                                                        N1, X1, P->tw, P->twL, P->tw4x, P->x4_rows, active, ss);
     } else {
         dim3 gx(hsb_div_up(N1, P->TYx), 3 * N0);
         k_fft_x_fwd<float><<<gx, XTHREADS, P->smem_x, st>>>(io.m[0], io.m[1], io.msel, io.minv, mask, ncell, N0, N1,
@@ -1028,7 +1064,7 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     if (io.ev) cudaEventRecord(io.ev[1], st);
     if (P->yz4) {
         dim3 gyz(C2, 1, nz);
-        P->yz4<<<gyz, P->yz4_threads, P->yz4_smem, st>>>(X1, N0, N1, C2, kern, P->tw, P->twL, active, ss);
+        P->yz4<<<gyz, P->yz4_threads, P->yz4_smem, st>>>(X1, N0, N1, C2, kern, P->tw4y, active, ss);
     } else if (P->fused) {
         switch (P->lz) {
 #define RUNYZ(LZ) case LZ: k_fft_yz_conv<LZ><<<C2, yz_threads<LZ>::value, P->smem_yz, st>>>(P->X1, N0, N1, L1, C2, P->kern, P->tw, P->twL, active); break;
@@ -1049,7 +1085,7 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     if (P->xinv4) {
         dim3 gi(hsb_div_up(N1, P->x4_rows), 3 * N0, nz);
         P->xinv4<<<gi, P->x4_threads, P->x4_smem, st>>>(X1, N1, N0, N1, N2, io.h[0], io.h[1], io.hsel, io.hinv,
-                                                        ncell, ms0, P->tw, P->twL, P->x4_rows, active, ss);
+                                                        ncell, ms0, P->tw, P->twL, P->tw4x, P->x4_rows, active, ss);
     } else {
         dim3 gi(hsb_div_up(N1, P->TYxi), 3 * N0);
         k_fft_x_inv<<<gi, XTHREADS, P->smem_xi, st>>>(P->X1, N1, N0, N1, N2, L2, io.h[0], io.h[1], io.hsel, io.hinv,

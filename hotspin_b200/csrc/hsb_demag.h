@@ -45,7 +45,7 @@ struct HsbDemagBatch {
     long x1_stride;            // complex elements between slots' spectra
     const float* scale;
     int scale_stride;          // floats
-    const float* kern;         // per-slot kernel spectra (null: the plan's own for every slot)
+    const float* kern;         // per-slot kernel spectra, fast y/z layout (null: the plan's own)
     long kern_stride;          // floats
 };
 
@@ -64,7 +64,7 @@ long hsb_demag_spectrum_scratch_bytes(hsb_demag_plan P);
 int hsb_demag_spectrum_scratch_create(hsb_demag_plan P, hsb_demag_spec_s** out);
 void hsb_demag_spectrum_scratch_destroy(hsb_demag_spec_s* s);
 int hsb_demag_spectrum_enqueue(hsb_demag_plan P, const double* cellsize, int accuracy, hsb_demag_spec_s* s,
-                               float* kern, cudaStream_t st);
+                               float* kern, float* kern4, cudaStream_t st);
 extern "C" int hsb_demag_plan_create(const int* size, const double* cellsize, const int* pbc,
                                      int accuracy, void* stream, hsb_demag_plan* out);
 extern "C" int hsb_demag_plan_destroy(hsb_demag_plan P);

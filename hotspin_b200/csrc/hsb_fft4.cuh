@@ -7,7 +7,9 @@
 //   4. lane t runs the B-point FFTs of the A/B columns k1 = t + B i  (in registers)
 // giving X[k1 + A k2]; lane t ends with v[i B + k2] = X[(t + B i) + A k2].
 // One shared-memory round trip per transform instead of log_R(L) Stockham passes, all
-// indices compile-time.  Twiddles come from a per-plan table tw[j] = exp(-2 pi i j / twL).
+// indices compile-time.  The step-2 twiddles come from a per-plan matrix
+// tw4[k1 B + n2] = exp(-2 pi i n2 k1 / L), so the B lanes of a sequence read B consecutive
+// entries per k1 (one coalesced load instead of B scattered ones).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -101,17 +103,16 @@ template <int L> struct Slot {
 
 // Four-step transform of one sequence (see header).  `lane` in [0, B); all B lanes of
 // the sequence, and every existing lane of the warp (`wmask`), must call it.
-// `tw`: table with twL entries.
+// `tw4`: the A x B twiddle matrix of length L.
 template <int L, int DIR>
-__device__ __forceinline__ void fft4(float2 (&v)[Split<L>::A], float2* slot, int lane, const float2* __restrict__ tw,
-                                     int twL, unsigned wmask = 0xffffffffu) {
+__device__ __forceinline__ void fft4(float2 (&v)[Split<L>::A], float2* slot, int lane,
+                                     const float2* __restrict__ tw4, unsigned wmask = 0xffffffffu) {
     constexpr int A = Split<L>::A, B = Split<L>::B;
     fft_reg64<A, DIR>(v);
     if (B > 1) {
-        const int ts = twL / L;
 #pragma unroll
         for (int k1 = 1; k1 < A; k1++) {
-            float2 w = __ldg(&tw[((lane * k1) & (L - 1)) * ts]);
+            float2 w = __ldg(&tw4[k1 * B + lane]);
             if (DIR > 0) w.y = -w.y;
             const float2 a = v[k1];
             v[k1] = make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);

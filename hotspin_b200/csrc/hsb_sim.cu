@@ -1350,8 +1350,8 @@ HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* d
     if (B->demag) {
         // this slot's own demag tensor (the reference evaluates Kernel_Arne in physical units,
         // so cells of equal shape but different size can round to different quadratures)
-        RC(hsb_demag_spectrum_enqueue(B->demag, d.cellsize, 6, B->spec, B->kernb + (long)slot * B->kern_floats,
-                                      B->st));
+        RC(hsb_demag_spectrum_enqueue(B->demag, d.cellsize, 6, B->spec, nullptr,
+                                      B->kernb + (long)slot * B->kern_floats, B->st));
     }
     B->nprep++;
     return HSB_OK;
