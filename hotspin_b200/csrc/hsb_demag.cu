@@ -26,6 +26,9 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "hsb_common.cuh"
@@ -697,6 +700,8 @@ struct hsb_demag_plan_s {
     xinv4_fn xinv4;
     yz4_fn yz4;
     int x4_rows, x4_threads, x4_smem, yz4_threads, yz4_smem;
+    int x4_S;           // slot stride of the x kernels
+    int x4i_rows, x4i_threads, x4i_smem;  // inverse x kernel (tuned separately)
 };
 
 // Largest power-of-two tile (<= cap) whose ping-pong buffers of `per_item` padded complex
@@ -878,6 +883,100 @@ static int build_kernel_spectrum(hsb_demag_plan_s* P, int accuracy, cudaStream_t
     return rc;
 }
 
+// Launch-shape tuning of the fast x kernels: block sizes of 64, 128 and 256 threads (rows of
+// the transform per block = threads / lanes per row) are timed on the plan's own buffers
+// and the fastest kept, per kernel.  Every shape computes each row identically, so the
+// choice changes timing only.  Results are cached per grid size for the process.
+struct XTune {
+    int f, i;
+};
+static std::mutex g_xtune_mu;
+static std::map<std::tuple<int, int, int>, XTune> g_xtune;
+
+static int tune_x(hsb_demag_plan_s* P, cudaStream_t st) {
+    if (!P->xfwd4) return HSB_OK;
+    const int N0 = P->N[0], N1 = P->N[1], N2 = P->N[2];
+    const auto key = std::make_tuple(N0, N1, N2);
+    const int B = 256 / P->x4_rows;
+    XTune best = {256, 256};
+    bool found = false;
+    {
+        std::lock_guard<std::mutex> lk(g_xtune_mu);
+        auto it = g_xtune.find(key);
+        if (it != g_xtune.end()) {
+            best = it->second;
+            found = true;
+        }
+    }
+    if (!found) {
+        const long ncell = (long)N0 * N1 * N2;
+        float* m = nullptr;
+        float* H = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        int rc = HSB_OK;
+        SlotStrides ss = {0, 0, 0, 0, nullptr, 0, 0};
+        float bf = 1e30f, bi = 1e30f;
+        if (cudaMalloc(&m, sizeof(float) * 3 * ncell) != cudaSuccess ||
+            cudaMalloc(&H, sizeof(float) * 3 * ncell) != cudaSuccess ||
+            cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+            cudaMemsetAsync(m, 0, sizeof(float) * 3 * ncell, st) != cudaSuccess) {
+            rc = HSB_ERR_CUDA;
+        }
+        for (int th = 64; th <= 256 && rc == HSB_OK; th *= 2) {
+            const int rows = th / B;
+            if (rows < 1) continue;
+            const int smem = rows * P->x4_S * (int)sizeof(float2);
+            dim3 g(hsb_div_up(N1, rows), 3 * N0);
+            for (int which = 0; which < 2; which++) {
+                float best_ms = 1e30f;
+                for (int rep = 0; rep < 4; rep++) {
+                    cudaEventRecord(e0, st);
+                    if (which == 0)
+                        P->xfwd4<<<g, th, smem, st>>>(m, m, nullptr, 0, nullptr, ncell, N0, N1, N2, N1, P->X1, P->tw,
+                                                      P->twL, P->tw4x, rows, nullptr, ss);
+                    else
+                        P->xinv4<<<g, th, smem, st>>>(P->X1, N1, N0, N1, N2, H, H, nullptr, 0, ncell, 1.0f, P->tw,
+                                                      P->twL, P->tw4x, rows, nullptr, ss);
+                    cudaEventRecord(e1, st);
+                    if (cudaEventSynchronize(e1) != cudaSuccess) {
+                        rc = HSB_ERR_CUDA;
+                        break;
+                    }
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (rep > 0 && ms < best_ms) best_ms = ms;   // first launch is a warm-up
+                }
+                if (which == 0 && best_ms < bf) {
+                    bf = best_ms;
+                    best.f = th;
+                }
+                if (which == 1 && best_ms < bi) {
+                    bi = best_ms;
+                    best.i = th;
+                }
+            }
+        }
+        if (cudaGetLastError() != cudaSuccess) rc = HSB_ERR_CUDA;
+        cudaFree(m);
+        cudaFree(H);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (rc != HSB_OK) {
+            hsb_set_error("hsb_demag_plan_create: x-kernel tuning failed");
+            return rc;
+        }
+        std::lock_guard<std::mutex> lk(g_xtune_mu);
+        g_xtune[key] = best;
+    }
+    P->x4_threads = best.f;
+    P->x4_rows = best.f / B;
+    P->x4_smem = P->x4_rows * P->x4_S * (int)sizeof(float2);
+    P->x4i_threads = best.i;
+    P->x4i_rows = best.i / B;
+    P->x4i_smem = P->x4i_rows * P->x4_S * (int)sizeof(float2);
+    return HSB_OK;
+}
+
 HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, const int* pbc,
                                      int accuracy, void* stream, hsb_demag_plan* out) {
     if (!size || !cellsize || !pbc || !out) {
@@ -968,6 +1067,10 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
             P->x4_rows = 256 / B;
             P->x4_threads = 256;
             P->x4_smem = P->x4_rows * S * (int)sizeof(float2);
+            P->x4_S = S;
+            P->x4i_rows = P->x4_rows;
+            P->x4i_threads = P->x4_threads;
+            P->x4i_smem = P->x4_smem;
             PTRY(cudaFuncSetAttribute(P->xfwd4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->x4_smem));
             PTRY(cudaFuncSetAttribute(P->xinv4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->x4_smem));
         }
@@ -985,6 +1088,7 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
     }
 #undef PTRY
     rc = build_kernel_spectrum(P, accuracy, st);
+    if (rc == HSB_OK) rc = tune_x(P, st);
     if (rc != HSB_OK) {
         hsb_demag_plan_destroy(P);
         return rc;
@@ -1083,9 +1187,9 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     }
     if (io.ev) cudaEventRecord(io.ev[2], st);
     if (P->xinv4) {
-        dim3 gi(hsb_div_up(N1, P->x4_rows), 3 * N0, nz);
-        P->xinv4<<<gi, P->x4_threads, P->x4_smem, st>>>(X1, N1, N0, N1, N2, io.h[0], io.h[1], io.hsel, io.hinv,
-                                                        ncell, ms0, P->tw, P->twL, P->tw4x, P->x4_rows, active, ss);
+        dim3 gi(hsb_div_up(N1, P->x4i_rows), 3 * N0, nz);
+        P->xinv4<<<gi, P->x4i_threads, P->x4i_smem, st>>>(X1, N1, N0, N1, N2, io.h[0], io.h[1], io.hsel, io.hinv,
+                                                          ncell, ms0, P->tw, P->twL, P->tw4x, P->x4i_rows, active, ss);
     } else {
         dim3 gi(hsb_div_up(N1, P->TYxi), 3 * N0);
         k_fft_x_inv<<<gi, XTHREADS, P->smem_xi, st>>>(P->X1, N1, N0, N1, N2, L2, io.h[0], io.h[1], io.hsel, io.hinv,
