@@ -66,6 +66,23 @@ __device__ __forceinline__ void mfa_w(const HsbPhys& P, float x, float& W, float
     }
 }
 
+// The longitudinal-field multiplier n kB T (W(am b) - am) / (mu0 Ms0 W'(am b) am), b = lf_b / T.
+// For J = 1/2 above the series range it uses e = expm1(-2x): tanh x = -e / (2 + e) and
+// 1 / cosh^2 x = 4 (1 + e) / (2 + e)^2, the same values as mfa_w's forms with one
+// transcendental instead of two.
+__device__ __forceinline__ float mfa_mult(const HsbPhys& P, float am, float Ts) {
+    const float x = am * (P.lf_b / Ts);
+    if (!P.lf_langevin && P.lf_lpre == 1.0f && P.lf_gpre == 2.0f && fabsf(x) >= P.lf_lim) {
+        const float e = expm1f(-2.0f * x);
+        const float d = 2.0f + e;
+        const float W = -e / d;
+        return P.lf_pre * Ts * (W - am) * d * d / (4.0f * (1.0f + e) * am);
+    }
+    float W, dW;
+    mfa_w(P, x, W, dW);
+    return P.lf_pre * Ts * (W - am) / dW / am;
+}
+
 template <int CH>
 __device__ __forceinline__ void load_ch(const float* __restrict__ y, long n, long i, float* v) {
 #pragma unroll
@@ -678,10 +695,12 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
     bool bad = false;
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < ngroups; g += (long)gridDim.x * blockDim.x) {
         const long i = g * W;
-        const int a2 = (int)(i % P.N2);
-        const long r = i / P.N2;
-        const int a1 = (int)(r % P.N1);
-        const int a0 = (int)(r / P.N1);
+        const unsigned iu = (unsigned)i;
+        const unsigned ru = hsb_fastdiv(iu, P.div2_mul, P.div2_shr);
+        const int a2 = (int)(iu - ru * (unsigned)P.N2);
+        const unsigned a0u = hsb_fastdiv(ru, P.div1_mul, P.div1_shr);
+        const int a1 = (int)(ru - a0u * (unsigned)P.N1);
+        const int a0 = (int)a0u;
         // ---- (A) stage derivatives and base state
         float acc[CH][W];
         {
@@ -803,10 +822,7 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
             if (P.llb) {
                 const float am = sqrtf(mx * mx + my * my + mz * mz);
                 if (am > 1e-30f && Ts > 0.f) {
-                    const float b = P.lf_b / Ts;
-                    float Wv, dW;
-                    mfa_w(P, am * b, Wv, dW);
-                    const float mult = P.lf_pre * Ts * (Wv - am) / dW / am;
+                    const float mult = mfa_mult(P, am, Ts);
                     hx += mult * mx;
                     hy += mult * my;
                     hz += mult * mz;

@@ -43,7 +43,34 @@ struct HsbPhys {
     float cs1, cs2;
     int normalize;       // renormalise m at stage formation (LLG mode); used by batched launches
     float ms0;           // Ms0 (A/m), the demag scale of this simulation
+    // division of a cell index (< 2^31) by N2 and by N1 as a multiply-high and shift
+    // (round-up reciprocal, Granlund & Montgomery 1994): q = umulhi(x, mul) >> shr
+    unsigned div2_mul, div2_shr, div1_mul, div1_shr;
 };
+
+// Quotient by the divisor encoded in (mul, shr); mul == 0 encodes a divisor of 1.
+__host__ __device__ __forceinline__ unsigned hsb_fastdiv(unsigned x, unsigned mul, unsigned shr) {
+#ifdef __CUDA_ARCH__
+    return mul ? (__umulhi(x, mul) >> shr) : x;
+#else
+    return mul ? (unsigned)(((unsigned long long)x * mul) >> 32) >> shr : x;
+#endif
+}
+
+// Multiplier and shift for dividing indices below 2^31 by d >= 1: with l = ceil(log2 d),
+// mul = ceil(2^(31 + l) / d) and shr = l - 1, so that q = floor(x mul / 2^(32 + shr)).
+inline void hsb_fastdiv_init(unsigned d, unsigned* mul, unsigned* shr) {
+    if (d <= 1) {
+        *mul = 0;
+        *shr = 0;
+        return;
+    }
+    unsigned l = 0;
+    while ((1ull << l) < d) l++;
+    const unsigned long long p = 31 + l;
+    *mul = (unsigned)(((1ull << p) + d - 1) / d);
+    *shr = (unsigned)(p - 32);
+}
 
 // Batched launches: slot = blockIdx.z; every per-slot buffer of slot s lives at the slot-0
 // address + s * stride (one arena per slot), physics and solver state per slot.

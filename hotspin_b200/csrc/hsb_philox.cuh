@@ -39,8 +39,7 @@ __device__ __forceinline__ void philox_normals3(uint32_t cell, uint64_t step, ui
     float s0, c0;
     sincospif(2.0f * philox_u01(c[1]), &s0, &c0);
     const float r1 = sqrtf(-2.0f * logf(philox_u01(c[2])));
-    float s1, c1;
-    sincospif(2.0f * philox_u01(c[3]), &s1, &c1);
+    const float c1 = cospif(2.0f * philox_u01(c[3]));
     g[0] = r0 * c0;
     g[1] = r0 * s0;
     g[2] = r1 * c1;

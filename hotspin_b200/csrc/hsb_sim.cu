@@ -711,6 +711,8 @@ static void phys_from_desc(const hsb_sim_desc& d, int nch, long ncell, HsbPhys& 
     P.cs2 = (float)d.cellsize[2];
     P.normalize = d.normalize;
     P.ms0 = (float)d.msat0T0;
+    hsb_fastdiv_init((unsigned)P.N2, &P.div2_mul, &P.div2_shr);
+    hsb_fastdiv_init((unsigned)P.N1, &P.div1_mul, &P.div1_shr);
 }
 
 static void fill_phys(hsb_sim_s* S) {
