@@ -679,6 +679,8 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
     const float* yerr0 = yerr0p ? yerr0p : ys;
     const bool th_field = (CH >= 5) && P.thermal && ythp != nullptr;
     const float* yth = th_field ? ythp : ys;
+    float* hth = resolve_off(A.hth, sd, off);
+    const int hmode = hth ? A.hth_mode : 0;      // 0 generate, 1 generate + store, 2 load
     const double ts = t + (double)A.tfrac * dt;
     const float fdt = (float)dt;
     const long n = P.ncell;
@@ -724,8 +726,12 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
         }
         // ---- (B) state, neighbours, demag field
         float y[CH][W], H[3][W], lapE[W], lapL[W];
-        float ye[CH >= 5 ? 2 : 1][W], thT[W], ka[CH][W];
+        float ye[CH >= 5 ? 2 : 1][W], thT[W], ka[CH][W], hthv[3][W];
         {
+            if (hmode == 2) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) ldw<W>(hth + c * n + i, hthv[c]);
+            }
             float hv[3][W], nb[4][CH][W], sl[CH], sr[CH];
 #pragma unroll
             for (int c = 0; c < CH; c++) ldw<W>(ys + c * n + i, y[c]);
@@ -828,13 +834,28 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
                     hz += mult * mz;
                 }
             }
-            if (P.thermal && thT[q] > 0.f) {
-                const float amp = sqrtf(th_amp * thT[q]);
-                float gg[3];
-                philox_normals3((uint32_t)(i + q), (uint64_t)step, P.seed_lo, P.seed_hi, gg);
-                hx += amp * sqrtf(P.lam[0]) * gg[0];
-                hy += amp * sqrtf(P.lam[1]) * gg[1];
-                hz += amp * sqrtf(P.lam[2]) * gg[2];
+            if (hmode == 2) {
+                hx += hthv[0][q];
+                hy += hthv[1][q];
+                hz += hthv[2][q];
+            } else {
+                float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+                if (P.thermal && thT[q] > 0.f) {
+                    const float amp = sqrtf(th_amp * thT[q]);
+                    float gg[3];
+                    philox_normals3((uint32_t)(i + q), (uint64_t)step, P.seed_lo, P.seed_hi, gg);
+                    t0 = amp * sqrtf(P.lam[0]) * gg[0];
+                    t1 = amp * sqrtf(P.lam[1]) * gg[1];
+                    t2 = amp * sqrtf(P.lam[2]) * gg[2];
+                }
+                hx += t0;
+                hy += t1;
+                hz += t2;
+                if (hmode == 1) {
+                    hthv[0][q] = t0;
+                    hthv[1][q] = t1;
+                    hthv[2][q] = t2;
+                }
             }
             const float gm = P.gamma;
             k[0][q] = gm * (-hy * mz + hz * my) + gm * P.lam[0] * hx;
@@ -859,6 +880,10 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
             }
         }
         // ---- stores and the error norm
+        if (hmode == 1) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) stw<W>(hth + c * n + i, hthv[c]);
+        }
         if (kout) {
 #pragma unroll
             for (int c = 0; c < CH; c++) {
@@ -1079,6 +1104,12 @@ static void launch_vec(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, c
     } else {
         launch_c<CH, BATCH, 4>(P, A, sd, Bt, nslot, st);
     }
+}
+
+// True when stage launches of this simulation run the load-first kernel, which is the one
+// that can keep the step's thermal field (StageArgs.hth_mode).
+bool hsb_stage_keeps_thermal(const HsbPhys& P) {
+    return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask && g_stage_variant != 0;
 }
 
 int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st) {

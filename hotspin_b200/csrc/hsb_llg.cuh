@@ -133,4 +133,8 @@ struct StageArgs {
     float rtol;
     int ungated;             // run even when the solver is inactive (state queries)
     int prep_gated;          // gate on HsbSolverDev.prep instead of .active (batched slot preparation)
+    // thermal field of the step (the same in every stage of an attempt): 0 = generate it,
+    // 1 = generate it and store it to hth, 2 = read it from hth (load-first kernel only)
+    int hth_mode;
+    PtrSel hth;              // [3][ncell]
 };

@@ -18,6 +18,7 @@
 #include "hsb_llg.cuh"
 
 int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st);
+bool hsb_stage_keeps_thermal(const HsbPhys& P);
 int hsb_launch_combine(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st);
 int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st);
 int hsb_launch_fixed_advance(HsbSolverDev* sd, cudaStream_t st);
@@ -98,6 +99,7 @@ struct hsb_sim_s {
     float* k[8];        // stage derivatives
     float* hd;          // demag field of the stage point
     float* hd01[2];     // demag field of y[0], y[1] (DP45 with a thermal field)
+    float* hth;         // thermal field of the current step (kept across its stages)
     float* msat_mask;
     float* lex_mask;
     HsbSolverDev* sd;   // device [nslot]
@@ -145,7 +147,7 @@ static PtrSel none() { return fixed(nullptr); }
 static StageArgs empty_args() {
     StageArgs A;
     memset(&A, 0, sizeof(A));
-    A.ys = A.hd = A.ytherm = A.kout = A.kacc = A.ynext = A.ybase = A.yerr0 = none();
+    A.ys = A.hd = A.ytherm = A.kout = A.kacc = A.ynext = A.ybase = A.yerr0 = A.hth = none();
     for (int j = 0; j < HSB_MAXK; j++) A.kin[j] = none();
     A.rtol = 1.0f;
     return A;
@@ -363,6 +365,14 @@ static int L_control(hsb_sim_s* S) {
     if (S->batched) return hsb_launch_dp45_control_batched(S->sd, S->nslot, S->st);
     return hsb_launch_dp45_control(S->sd, S->st);
 }
+// Thermal field of the step: generated and kept by the attempt's first stage, read by the
+// others (only the load-first stage kernel keeps it).
+static void thermal_keep(hsb_sim_s* S, StageArgs& A, bool first) {
+    if (!S->hth || !hsb_stage_keeps_thermal(S->P)) return;
+    A.hth = fixed(S->hth);
+    A.hth_mode = first ? 1 : 2;
+}
+
 static int L_advance(hsb_sim_s* S) {
     if (S->batched) return hsb_launch_fixed_advance_batched(S->sd, S->nslot, S->st);
     return hsb_launch_fixed_advance(S->sd, S->st);
@@ -407,6 +417,7 @@ static int enqueue_attempt(hsb_sim_s* S) {
             A.ybase = YC;
             A.cself = 1.0f;
             A.normalize = norm;
+            thermal_keep(S, A, true);
             RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
             RC(run_demag(S, ya, -1, hd, -1));
             StageArgs B = empty_args();
@@ -421,6 +432,7 @@ static int enqueue_attempt(hsb_sim_s* S) {
             B.ck[0] = -0.5f;
             B.cself = 0.5f;
             B.normalize = norm;
+            thermal_keep(S, B, false);
             RC(timed(S, PROF_STAGE, [&] { return L_stage(S, B); }));
             RC(timed(S, PROF_OTHER, [&] { return L_advance(S); }));
             break;
@@ -454,6 +466,7 @@ static int enqueue_attempt(hsb_sim_s* S) {
                     A.ck[0] = 1.0f / 6.0f;
                     A.cself = 1.0f / 6.0f;
                 }
+                thermal_keep(S, A, s == 0);
                 RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
             }
             RC(timed(S, PROF_OTHER, [&] { return L_advance(S); }));
@@ -480,6 +493,7 @@ static int enqueue_attempt(hsb_sim_s* S) {
                 A.ybase = YC;
                 A.cself = (float)DPA[1][0];
                 A.normalize = norm;
+                thermal_keep(S, A, true);
                 RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
             } else {
                 StageArgs A = empty_args();
@@ -511,6 +525,7 @@ static int enqueue_attempt(hsb_sim_s* S) {
                 }
                 A.cself = (float)DPA[s + 1][s];
                 A.normalize = norm;
+                if (th) thermal_keep(S, A, false);
                 RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
                 float* t = cur;
                 cur = other;
@@ -541,6 +556,7 @@ static int enqueue_attempt(hsb_sim_s* S) {
             A.ceself = (float)DPE[6];
             A.yerr0 = YC;
             A.rtol = (float)S->d.rtol;
+            if (th) thermal_keep(S, A, false);
             RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
             RC(timed(S, PROF_OTHER, [&] { return L_control(S); }));
             break;
@@ -723,7 +739,7 @@ static void fill_phys(hsb_sim_s* S) {
 
 // Offsets (floats) of one slot's buffers in its arena.
 struct SlotLayout {
-    long y, ystage, k, hd, hd01, total;
+    long y, ystage, k, hd, hd01, hth, total;
     int nk;
 };
 static SlotLayout slot_layout(const hsb_sim_desc& d, long n) {
@@ -748,6 +764,11 @@ static SlotLayout slot_layout(const hsb_sim_desc& d, long n) {
             o += al(6 * n);
         }
     }
+    L.hth = -1;
+    if (d.thermal && d.solver != SOLVER_EULER) {
+        L.hth = o;
+        o += al(3 * n);
+    }
     L.total = o;
     return L;
 }
@@ -763,6 +784,7 @@ static void point_slot0(hsb_sim_s* S, const SlotLayout& L) {
     S->hd = L.hd >= 0 ? a + L.hd : nullptr;
     S->hd01[0] = L.hd01 >= 0 ? a + L.hd01 : nullptr;
     S->hd01[1] = L.hd01 >= 0 ? S->hd01[0] + 3 * S->n : nullptr;
+    S->hth = L.hth >= 0 ? a + L.hth : nullptr;
     S->slot_stride = L.total;
 }
 
