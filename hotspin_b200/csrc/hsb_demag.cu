@@ -366,7 +366,7 @@ struct SlotStrides {
 
 // R2C along a2 for TY rows per block, B lanes per row; M = L2/2 packed complex points.
 template <int M>
-__global__ void __launch_bounds__(256) k_xfwd4(const float* __restrict__ in0, const float* __restrict__ in1,
+__global__ void __launch_bounds__(256, 3) k_xfwd4(const float* __restrict__ in0, const float* __restrict__ in1,
                                                const int* __restrict__ isel, int iinv,
                                                const float* __restrict__ mask, long in_cstride,
                                                int planes_per_comp, int N1, int N2, int ldo,
@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(256) k_xfwd4(const float* __restrict__ in0, co
 
 // C2R along a2 with transposed input; writes the first N2 reals times `scale`.
 template <int M>
-__global__ void __launch_bounds__(256) k_xinv4(const float2* __restrict__ in, int ldi, int planes_per_comp, int N1,
+__global__ void __launch_bounds__(256, 3) k_xinv4(const float2* __restrict__ in, int ldi, int planes_per_comp, int N1,
                                                int N2, float* __restrict__ out0, float* __restrict__ out1,
                                                const int* __restrict__ osel, int oinv, long out_cstride,
                                                float scale, const float2* __restrict__ tw, int twL,
@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(256) k_xinv4(const float2* __restrict__ in, in
 // Fused y FFT + z FFT + symmetric tensor multiply + inverse z + inverse y for one kx column;
 // 3*N0 sequences of length L1 (B lanes each), z in registers (LZ = L0 <= 16).
 template <int L1, int LZ>
-__global__ void __launch_bounds__(384) k_yz4(float2* __restrict__ X1, int N0, int N1, int C2,
+__global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restrict__ X1, int N0, int N1, int C2,
                                              const float* __restrict__ kern4, const float2* __restrict__ tw4,
                                              const int* __restrict__ active, const SlotStrides ss) {
     const int sl = blockIdx.z;
