@@ -365,7 +365,9 @@ struct SlotStrides {
 };
 
 // R2C along a2 for TY rows per block, B lanes per row; M = L2/2 packed complex points.
-template <int M>
+// PR: the row is zero-padded to twice its length (open boundary), so the upper half of
+// the packed input is zero.
+template <int M, bool PR>
 __global__ void __launch_bounds__(256, 3) k_xfwd4(const float* __restrict__ in0, const float* __restrict__ in1,
                                                const int* __restrict__ isel, int iinv,
                                                const float* __restrict__ mask, long in_cstride,
@@ -401,7 +403,7 @@ __global__ void __launch_bounds__(256, 3) k_xfwd4(const float* __restrict__ in0,
         for (int n1 = 0; n1 < A; n1++) {
             const int n = B * n1 + lane;
             float a = 0.f, b = 0.f;
-            if (r < ny && 2 * n < N2) {
+            if (!(PR && n1 >= A / 2) && r < ny && 2 * n < N2) {
                 if (even) {
                     const float2 t = __ldg(reinterpret_cast<const float2*>(src) + n);
                     a = t.x;
@@ -423,7 +425,7 @@ __global__ void __launch_bounds__(256, 3) k_xfwd4(const float* __restrict__ in0,
             v[n1] = make_float2(a, b);
         }
     }
-    fft4<M, -1>(v, slot, lane, tw4);
+    fft4<M, -1, PR, false>(v, slot, lane, tw4);
     // natural order Z[k] into the slot
 #pragma unroll
     for (int j = 0; j < A; j++) slot[fft4_out_index<M>(lane, j)] = v[j];
@@ -458,7 +460,8 @@ __global__ void __launch_bounds__(256, 3) k_xfwd4(const float* __restrict__ in0,
 }
 
 // C2R along a2 with transposed input; writes the first N2 reals times `scale`.
-template <int M>
+// PR: only the first half of the row is kept (open boundary).
+template <int M, bool PR>
 __global__ void __launch_bounds__(256, 3) k_xinv4(const float2* __restrict__ in, int ldi, int planes_per_comp, int N1,
                                                int N2, float* __restrict__ out0, float* __restrict__ out1,
                                                const int* __restrict__ osel, int oinv, long out_cstride,
@@ -508,7 +511,7 @@ __global__ void __launch_bounds__(256, 3) k_xinv4(const float2* __restrict__ in,
         v[n1] = make_float2(sA.x - wd.y, sA.y + wd.x);
     }
     __syncwarp();
-    fft4<M, +1>(v, slot, lane, tw4);
+    fft4<M, +1, false, PR>(v, slot, lane, tw4);
     float* out = (osel && ((*osel) ^ oinv)) ? out1 : out0;
     if (r < ny) {
         float* dst = out + comp * out_cstride + ((long)a0 * N1 + y0 + r) * N2;
@@ -530,7 +533,9 @@ __global__ void __launch_bounds__(256, 3) k_xinv4(const float2* __restrict__ in,
 
 // Fused y FFT + z FFT + symmetric tensor multiply + inverse z + inverse y for one kx column;
 // 3*N0 sequences of length L1 (B lanes each), z in registers (LZ = L0 <= 16).
-template <int L1, int LZ>
+// PR: y and z are zero-padded to twice their lengths (open boundaries): the upper halves of
+// the forward inputs are zero and only the lower halves of the inverse outputs are kept.
+template <int L1, int LZ, bool PR>
 __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restrict__ X1, int N0, int N1, int C2,
                                              const float* __restrict__ kern4, const float2* __restrict__ tw4,
                                              const int* __restrict__ active, const SlotStrides ss) {
@@ -555,9 +560,9 @@ __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restric
 #pragma unroll
     for (int n1 = 0; n1 < A; n1++) {
         const int n = B * n1 + lane;
-        v[n1] = (n < N1) ? src[n] : make_float2(0.f, 0.f);
+        v[n1] = (!(PR && n1 >= A / 2) && n < N1) ? src[n] : make_float2(0.f, 0.f);
     }
-    fft4<L1, -1>(v, slot, lane, tw4, wmask);
+    fft4<L1, -1, PR, false>(v, slot, lane, tw4, wmask);
 #pragma unroll
     for (int j = 0; j < A; j++) slot[fft4_out_index<L1>(lane, j)] = v[j];
     __syncthreads();
@@ -567,9 +572,11 @@ __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restric
 #pragma unroll
         for (int c = 0; c < 3; c++)
 #pragma unroll
-            for (int z = 0; z < LZ; z++) w[c][z] = (z < N0) ? sm[(c * N0 + z) * SS + k1] : make_float2(0.f, 0.f);
+            for (int z = 0; z < LZ; z++)
+                w[c][z] = (!(PR && LZ > 1 && z >= LZ / 2) && z < N0) ? sm[(c * N0 + z) * SS + k1]
+                                                                       : make_float2(0.f, 0.f);
 #pragma unroll
-        for (int c = 0; c < 3; c++) fft_reg64<LZ, -1>(w[c]);
+        for (int c = 0; c < 3; c++) fft_reg64<LZ, -1, PR && (LZ > 1), false>(w[c]);
         const int f1 = k1 > h1 ? L1 - k1 : k1;
         const float s1 = k1 > h1 ? -1.f : 1.f;
         // kern4 layout [kx][f0][component][f1]: consecutive k1 read consecutive words
@@ -589,7 +596,7 @@ __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restric
             w[2][k0] = make_float2(kxz * m0.x + kyz * m1.x + kzz * m2.x, kxz * m0.y + kyz * m1.y + kzz * m2.y);
         }
 #pragma unroll
-        for (int c = 0; c < 3; c++) fft_reg64<LZ, +1>(w[c]);
+        for (int c = 0; c < 3; c++) fft_reg64<LZ, +1, false, PR && (LZ > 1)>(w[c]);
 #pragma unroll
         for (int c = 0; c < 3; c++)
 #pragma unroll
@@ -600,7 +607,7 @@ __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restric
 #pragma unroll
     for (int n1 = 0; n1 < A; n1++) v[n1] = slot[B * n1 + lane];
     __syncwarp(wmask);
-    fft4<L1, +1>(v, slot, lane, tw4, wmask);
+    fft4<L1, +1, false, PR>(v, slot, lane, tw4, wmask);
     float2* dst = X1 + ((long)col * C2 + kx) * N1;
 #pragma unroll
     for (int j = 0; j < A; j++) {
@@ -616,36 +623,36 @@ typedef void (*xinv4_fn)(const float2*, int, int, int, int, float*, float*, cons
                          const float2*, int, const float2*, int, const int*, const SlotStrides);
 typedef void (*yz4_fn)(float2*, int, int, int, const float*, const float2*, const int*, const SlotStrides);
 
-static xfwd4_fn xfwd4_for(int M, int* B, int* S) {
+static xfwd4_fn xfwd4_for(int M, bool pr, int* B, int* S) {
     switch (M) {
-#define XF(m) case m: *B = Split<m>::B; *S = Slot<m>::S; return k_xfwd4<m>;
+#define XF(m) case m: *B = Split<m>::B; *S = Slot<m>::S; return pr ? k_xfwd4<m, true> : k_xfwd4<m, false>;
         XF(8) XF(16) XF(32) XF(64) XF(128) XF(256) XF(512) XF(1024)
 #undef XF
     }
     return nullptr;
 }
-static xinv4_fn xinv4_for(int M) {
+static xinv4_fn xinv4_for(int M, bool pr) {
     switch (M) {
-#define XI(m) case m: return k_xinv4<m>;
+#define XI(m) case m: return pr ? k_xinv4<m, true> : k_xinv4<m, false>;
         XI(8) XI(16) XI(32) XI(64) XI(128) XI(256) XI(512) XI(1024)
 #undef XI
     }
     return nullptr;
 }
-template <int L1>
+template <int L1, bool PR>
 static yz4_fn yz4_for_z(int LZ) {
     switch (LZ) {
-        case 1: return k_yz4<L1, 1>;
-        case 2: return k_yz4<L1, 2>;
-        case 4: return k_yz4<L1, 4>;
-        case 8: return k_yz4<L1, 8>;
-        case 16: return k_yz4<L1, 16>;
+        case 1: return k_yz4<L1, 1, PR>;
+        case 2: return k_yz4<L1, 2, PR>;
+        case 4: return k_yz4<L1, 4, PR>;
+        case 8: return k_yz4<L1, 8, PR>;
+        case 16: return k_yz4<L1, 16, PR>;
     }
     return nullptr;
 }
-static yz4_fn yz4_for(int L1, int LZ, int* B, int* S) {
+static yz4_fn yz4_for(int L1, int LZ, bool pr, int* B, int* S) {
     switch (L1) {
-#define YZ(l) case l: *B = Split<l>::B; *S = Slot<l>::S; return yz4_for_z<l>(LZ);
+#define YZ(l) case l: *B = Split<l>::B; *S = Slot<l>::S; return pr ? yz4_for_z<l, true>(LZ) : yz4_for_z<l, false>(LZ);
         YZ(16) YZ(32) YZ(64) YZ(128) YZ(256) YZ(512) YZ(1024)
 #undef YZ
     }
@@ -1058,10 +1065,13 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
     {
         // four-step kernels for the FP32 convolution when the lengths fit
         int B = 0, S = 0;
-        xfwd4_fn xf = xfwd4_for(M, &B, &S);
+        // zero-padding pruning where the padded length is twice the grid's
+        const bool prx = P->pbc[2] == 0 && P->N[2] > 1;
+        const bool pryz = P->pbc[1] == 0 && P->N[1] > 1 && (P->N[0] == 1 || P->pbc[0] == 0);
+        xfwd4_fn xf = xfwd4_for(M, prx, &B, &S);
         if (xf && B > 0) {
             P->xfwd4 = xf;
-            P->xinv4 = xinv4_for(M);
+            P->xinv4 = xinv4_for(M, prx);
             rc = make_tw4(M, B, P->twL, &P->tw4x);
             if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }
             P->x4_rows = 256 / B;
@@ -1073,9 +1083,12 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
             P->x4i_smem = P->x4_smem;
             PTRY(cudaFuncSetAttribute(P->xfwd4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->x4_smem));
             PTRY(cudaFuncSetAttribute(P->xinv4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->x4_smem));
+            // prefer shared memory over L1 so that several blocks fit per SM
+            PTRY(cudaFuncSetAttribute(P->xfwd4, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+            PTRY(cudaFuncSetAttribute(P->xinv4, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         }
         int By = 0, Sy = 0;
-        yz4_fn yf = (L0 <= 16) ? yz4_for(L1, L0, &By, &Sy) : nullptr;
+        yz4_fn yf = (L0 <= 16) ? yz4_for(L1, L0, pryz, &By, &Sy) : nullptr;
         if (yf && 3 * N0 * By <= 384 && 3 * N0 * Sy * (int)sizeof(float2) <= 110 * 1024) {
             P->yz4 = yf;
             PTRY(cudaMalloc(&P->kern4, sizeof(float) * kcount));
@@ -1084,6 +1097,7 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
             P->yz4_threads = 3 * N0 * By;
             P->yz4_smem = 3 * N0 * Sy * (int)sizeof(float2);
             PTRY(cudaFuncSetAttribute(P->yz4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->yz4_smem));
+            PTRY(cudaFuncSetAttribute(P->yz4, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         }
     }
 #undef PTRY

@@ -46,7 +46,10 @@ __device__ __forceinline__ constexpr double c64sin(int k) { return c64cos(k - 16
 
 // In-register radix-2 DIT FFT of R = 1..64 points on v[0..R), bit-reversed input order
 // handled by the unrolled permutation; every twiddle is a compile-time constant.
-template <int R, int DIR>
+// ZIN: the upper half of the input is zero (zero padding) — the first stage reduces to
+// copies.  HOUT: only the lower half of the output is wanted — the last stage skips the
+// upper outputs (left unspecified).
+template <int R, int DIR, bool ZIN = false, bool HOUT = false>
 __device__ __forceinline__ void fft_reg64(float2* v) {
     constexpr int B = ilog2c(R);
 #pragma unroll
@@ -61,6 +64,12 @@ __device__ __forceinline__ void fft_reg64(float2* v) {
 #pragma unroll
     for (int st = 1; st <= B; st++) {
         const int len = 1 << st;
+        if (ZIN && R > 1 && st == 1) {
+            // after the bit reversal, v[i + 1] holds input brev(i) + R/2, which is zero
+#pragma unroll
+            for (int i = 0; i < R; i += 2) v[i + 1] = v[i];
+            continue;
+        }
 #pragma unroll
         for (int i = 0; i < R; i += len) {
 #pragma unroll
@@ -79,7 +88,7 @@ __device__ __forceinline__ void fft_reg64(float2* v) {
                     bw = make_float2(b.x * wr - b.y * wi, b.x * wi + b.y * wr);
                 }
                 v[i + k] = make_float2(a.x + bw.x, a.y + bw.y);
-                v[i + k + len / 2] = make_float2(a.x - bw.x, a.y - bw.y);
+                if (!(HOUT && st == B)) v[i + k + len / 2] = make_float2(a.x - bw.x, a.y - bw.y);
             }
         }
     }
@@ -104,11 +113,13 @@ template <int L> struct Slot {
 // Four-step transform of one sequence (see header).  `lane` in [0, B); all B lanes of
 // the sequence, and every existing lane of the warp (`wmask`), must call it.
 // `tw4`: the A x B twiddle matrix of length L.
-template <int L, int DIR>
+// ZIN: inputs L/2..L-1 are zero; HOUT: only outputs 0..L/2-1 are wanted.
+template <int L, int DIR, bool ZIN = false, bool HOUT = false>
 __device__ __forceinline__ void fft4(float2 (&v)[Split<L>::A], float2* slot, int lane,
                                      const float2* __restrict__ tw4, unsigned wmask = 0xffffffffu) {
     constexpr int A = Split<L>::A, B = Split<L>::B;
-    fft_reg64<A, DIR>(v);
+    // n = B n1 + n2 >= L/2 exactly when n1 >= A/2
+    fft_reg64<A, DIR, ZIN>(v);
     if (B > 1) {
 #pragma unroll
         for (int k1 = 1; k1 < A; k1++) {
@@ -124,7 +135,8 @@ __device__ __forceinline__ void fft4(float2 (&v)[Split<L>::A], float2* slot, int
         for (int i = 0; i < A / B; i++) {
 #pragma unroll
             for (int n2 = 0; n2 < B; n2++) v[i * B + n2] = slot[n2 * (A + 1) + lane + B * i];
-            fft_reg64<B, DIR>(v + i * B);
+            // X index (lane + B i) + A k2 >= L/2 exactly when k2 >= B/2
+            fft_reg64<B, DIR, false, HOUT>(v + i * B);
         }
         __syncwarp(wmask);
     }
