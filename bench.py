@@ -228,9 +228,9 @@ def run_ours(args):
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         traffic = json.load(open(tp)).get(dom)
-    names = {"stage": "k_stage4<5> (fused RHS + DP45 stage, float4 cells)",
-             "yz": "k_yz4<1024,8> (y/z FFT + tensor multiply + inverse)",
-             "xfwd": "k_xfwd4<512> (R2C + transpose)", "xinv": "k_xinv4<512> (C2R)"}
+    names = {"stage": "k_stagec<5,0,2,NK> (load-first fused RHS + DP45 stage; 7 launches per attempt)",
+             "yz": "k_yz4<1024,8,1> (y/z FFT + tensor multiply + inverse)",
+             "xfwd": "k_xfwd4<512,1> (R2C + transpose)", "xinv": "k_xinv4<512,1> (C2R)"}
     roof = {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1), "peak": peak,
             "peak_kind": kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
             "algorithmic_bytes_per_launch": int(byt / nlaunch),
@@ -270,9 +270,48 @@ def run_ours(args):
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(kw, st0)
+        if world == 1 and not args.no_serving:
+            out["serving"] = serving(args)
         print(json.dumps(out))
     if pg is not None:
         pg.destroy_process_group()
+
+
+def serving(args):
+    """Continuous-batching serving stream against the sequential plain path (one GPU).
+
+    256 independent LLG/LLB requests (Poisson arrivals at 50/s; square films with sides
+    32..512 log-uniform and 1 or 2 layers; cubic cells 2-5 nm; Ms0, damping, temperature,
+    field and initial m drawn from seed 4), DP45 at rtol 1e-5 to 50 ps each.  The batched
+    loop (hotspin_b200.serve.Server) runs them as they arrive; the plain path runs one
+    Simulation per request in arrival order.  Both report p50/p99 time-to-solution and
+    throughput over the makespan; every result is compared between the two.
+    """
+    from hotspin_b200 import serve
+    reqs = serve.make_requests(n=args.serving_requests, seed=4, t_end=args.serving_tend)
+    warm = serve.make_requests(n=2, seed=99, t_end=2e-14, sides=(32,), layers=(1,))
+    w = serve.Server()
+    w.run(warm, realtime=False)
+    w.close()
+    serve.run_sequential(warm)
+    srv = serve.Server()
+    res = srv.run(reqs, realtime=True)
+    nclass = len(srv.classes)
+    launches = sum(c.launches for c in srv.classes.values())
+    srv.close()
+    seq, service, setup = serve.run_sequential(reqs)
+    sb, ss = serve.summarize(res, reqs), serve.summarize(seq, reqs)
+    dm = max(float(np.abs(res[k].m - seq[k].m).max()) for k in res)
+    same = sum(int(res[k].steps == seq[k].steps) for k in res)
+    rnd = lambda d: {k: (round(v, 4) if isinstance(v, float) else v) for k, v in d.items()}
+    return {"workload": "%d Poisson(50/s) LLG/LLB requests, square films 32..512 x 1..2 layers, cells 2-5 nm, "
+                        "DP45 rtol 1e-5 to %g ps, seed 4" % (len(reqs), args.serving_tend * 1e12),
+            "batched": rnd(sb), "sequential_plain": rnd(ss),
+            "throughput_ratio": round(sb["req_per_s"] / ss["req_per_s"], 3),
+            "p50_ratio": round(ss["p50_s"] / sb["p50_s"], 3), "p99_ratio": round(ss["p99_s"] / sb["p99_s"], 3),
+            "max_abs_dm_batched_vs_plain": dm, "same_step_counts": "%d/%d" % (same, len(res)),
+            "size_classes": nclass, "class_graph_launches": launches,
+            "plain_setup_share": round(sum(setup.values()) / sum(service.values()), 4)}
 
 
 def ctypes_int():
@@ -290,6 +329,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the batched-serving comparison")
+    ap.add_argument("--serving-requests", type=int, default=256)
+    ap.add_argument("--serving-tend", type=float, default=50e-12)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

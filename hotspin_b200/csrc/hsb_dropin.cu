@@ -839,6 +839,226 @@ __global__ void d_mfa_table(double Tc, double J, int n, double* T, double* me, d
     }
 }
 
+// ------------------------------------------------------------------ Debye heat capacity (Cp.cu)
+// Cp = n (T/Td)^3 * integral_0^{Td/T} x^4 e^x / (e^x - 1)^2 dx by the composite trapezoid
+// rule on 61 intervals (the reference's INTMAXSTEPS); below T/Td = 0.01 the low-temperature
+// limit n (4 pi^4 / 15) (T/Td)^3.  kB and the density multiplier are applied by the caller.
+#define HSB_DEBYE_STEPS 61
+__device__ __forceinline__ double d_debye_integrand(double x) {
+    const double ex = exp(x);
+    return (x <= HSB_ZERO) ? 0.0 : (x * x * x * x * ex) / ((ex - 1.0) * (ex - 1.0));
+}
+
+__global__ void d_cp(double* Cp, const double* T, const double* Tdm, const double* nm, double TdMul, int n) {
+    GRID_STRIDE(i, n) {
+        const double nn = mu1(nm, i);
+        const double Td = TdMul * mu1(Tdm, i);
+        const double Ti = T[i];
+        if (Td == 0.0) {
+            Cp[i] = 0.0;
+            continue;
+        }
+        const double u = Td / Ti;   // upper integration limit
+        const double r = Ti / Td;
+        if (r < 0.01) {
+            const double pi4 = M_PI * M_PI * M_PI * M_PI;
+            Cp[i] = nn * (12.0 / 5.0) * (1.0 / 9.0) * pi4 * (r * r * r);
+            continue;
+        }
+        const double h = u / (double)HSB_DEBYE_STEPS;
+        double inner = 0.0, x = 0.0;
+        for (int j = 1; j < HSB_DEBYE_STEPS; j++) {
+            x += h;
+            inner += d_debye_integrand(x);
+        }
+        x += h;
+        const double ends = d_debye_integrand(0.0) + d_debye_integrand(x);
+        const double integral = (ends + 2.0 * inner) * (0.5 * h);
+        Cp[i] = nn * integral / (u * u * u);
+    }
+}
+
+HSB_EXPORT void cpAsync(double* Cp, double* T, double* Td, double* n, const double TdMul, const int Npart,
+                        CUstream stream) {
+    d_cp<<<g1(Npart), DROPIN_THREADS, 0, S(stream)>>>(Cp, T, Td, n, TdMul, Npart);
+    check_launch("cpAsync");
+}
+
+// ------------------------------------------------------------------ spin temperature (Ts.cu)
+// The temperature at which the mean-field equilibrium magnetization equals msat / Msat0T0:
+// solve B_S(S^2 J0 m / T) = m for T in [0, Tc] (J0 = 3 Tc / (S (S + 1))) with the same
+// Ridders iteration as brillouinAsync.  Msat0T0 = 0 -> 0, msat = Msat0T0 -> 0, msat = 0 -> Tc.
+__device__ double d_ts_model(double T, double S_, double pre, double m) {
+    const double x = (T == 0.0) ? 1.0e38 : pre / T;
+    return d_Bj(S_, x) - m;
+}
+
+__device__ double d_ridders_ts(double S_, double pre, double m, double xa, double xb) {
+    const double ya = d_ts_model(xa, S_, pre, m);
+    if (fabs(ya) < HSB_ZERO) return xa;
+    const double yb = d_ts_model(xb, S_, pre, m);
+    if (fabs(yb) < HSB_ZERO) return xb;
+    double y1 = ya, x1 = xa, y2 = yb, x2 = xb;
+    double x = 1.0e10, tx = x, teps = x;
+    int iter = 0;
+    while (teps > 1.0e-8 && iter < 1000) {
+        const double x3 = 0.5 * (x2 + x1);
+        const double y3 = d_ts_model(x3, S_, pre, m);
+        const double dy = (y3 * y3 - y1 * y2);
+        if (dy == 0.0) {
+            x = x3;
+            break;
+        }
+        const double dx = (x3 - x1) * d_sign(y1 - y2) * y3 / (sqrt(dy));
+        x = x3 + dx;
+        const double y = d_ts_model(x, S_, pre, m);
+        const bool s3 = signbit(y) == signbit(y3);
+        y2 = s3 ? y2 : y3;
+        x2 = s3 ? x2 : x3;
+        const bool s1 = (signbit(y) == signbit(y1)) || x2 == x3;
+        y2 = s1 ? y2 : y1;
+        x2 = s1 ? x2 : x1;
+        y1 = y;
+        x1 = x;
+        teps = fabs((x - tx) / (tx + x));
+        tx = x;
+        iter++;
+    }
+    return x;
+}
+
+__global__ void d_ts(double* Ts, const double* msm, const double* ms0T0m, const double* Tcm, const double* Sm,
+                     double msMul, double ms0T0Mul, double TcMul, double SMul, int n) {
+    GRID_STRIDE(i, n) {
+        const double ms0T0 = ms0T0Mul * mu1(ms0T0m, i);
+        if (ms0T0 == 0.0) {
+            Ts[i] = 0.0;
+            continue;
+        }
+        const double ms = msMul * mu1(msm, i);
+        if (ms == ms0T0) {
+            Ts[i] = 0.0;
+            continue;
+        }
+        const double Tc = TcMul * mu1(Tcm, i);
+        if (ms == 0.0) {
+            Ts[i] = Tc;
+            continue;
+        }
+        const double Sp = SMul * mu1(Sm, i);
+        const double J0 = 3.0 * Tc / (Sp * (Sp + 1.0));
+        const double m = ms / ms0T0;
+        Ts[i] = d_ridders_ts(Sp, Sp * Sp * J0 * m, m, 0.0, Tc);
+    }
+}
+
+HSB_EXPORT void tsAsync(double* Ts, double* msat, double* msat0T0, double* Tc, double* S_, const double msatMul,
+                        const double msat0T0Mul, const double TcMul, const double SMul, int Npart, CUstream stream) {
+    d_ts<<<g1(Npart), DROPIN_THREADS, 0, S(stream)>>>(Ts, msat, msat0T0, Tc, S_, msatMul, msat0T0Mul, TcMul, SMul,
+                                                      Npart);
+    check_launch("tsAsync");
+}
+
+// ------------------------------------------------------------------ weighted average (wavg.cu)
+// dst = (w0 a + w1 b + 2 R sqrt(w0 a w1 b)) / (w0 + w1 + 2 R sqrt(w0 w1)), 0 where the
+// denominator vanishes.
+__global__ void d_wavg(double* dst, const double* a, const double* b, const double* w0m, const double* w1m,
+                       const double* Rm, double w0Mul, double w1Mul, double RMul, int n) {
+    GRID_STRIDE(i, n) {
+        const double w0 = w0Mul * mu1(w0m, i), w1 = w1Mul * mu1(w1m, i), R = RMul * mu1(Rm, i);
+        const double x0 = a[i], x1 = b[i];
+        const double den = w0 + w1 + 2.0 * R * sqrt(w0 * w1);
+        dst[i] = (den == 0.0) ? 0.0 : (w0 * x0 + w1 * x1 + 2.0 * R * sqrt(w0 * x0 * w1 * x1)) / den;
+    }
+}
+
+HSB_EXPORT void wavgAsync(double* dst, double* a, double* b, double* w0, double* w1, double* R, double w0Mul,
+                          double w1Mul, double RMul, CUstream stream, int Npart) {
+    d_wavg<<<g1(Npart), DROPIN_THREADS, 0, S(stream)>>>(dst, a, b, w0, w1, R, w0Mul, w1Mul, RMul, Npart);
+    check_launch("wavgAsync");
+}
+
+// ------------------------------------------------------------------ energy flow (energy_flow.cu)
+// w = Tc S^2 n / (S (S + 1)) (m . R), with Tc and n taken from their masks alone (the
+// reference applies no multiplier to them) and 0 where n, S or Tc vanishes.
+__global__ void d_energy_flow(double* w, const double* mx, const double* my, const double* mz, const double* Rx,
+                              const double* Ry, const double* Rz, const double* Tcm, const double* Sm,
+                              const double* nm, double SMul, int n) {
+    GRID_STRIDE(i, n) {
+        const double Sp = SMul * mu1(Sm, i), Tc = mu1(Tcm, i), nn = mu1(nm, i);
+        if (nn == 0.0 || Sp == 0.0 || Tc == 0.0) {
+            w[i] = 0.0;
+            continue;
+        }
+        const double mR = mx[i] * Rx[i] + my[i] * Ry[i] + mz[i] * Rz[i];
+        w[i] = (Tc * Sp * Sp * nn / (Sp * (Sp + 1.0))) * mR;
+    }
+}
+
+HSB_EXPORT void energyFlowAsync(double* w, double* mx, double* my, double* mz, double* Rx, double* Ry, double* Rz,
+                                double* Tc, double* S_, double* n, double SMul, int Npart, CUstream stream) {
+    d_energy_flow<<<g1(Npart), DROPIN_THREADS, 0, S(stream)>>>(w, mx, my, mz, Rx, Ry, Rz, Tc, S_, n, SMul, Npart);
+    check_launch("energyFlowAsync");
+}
+
+// ------------------------------------------------------------------ nonlocal damping (llbar-nonlocal00nc.cu)
+// t_c = -sum over the 6 neighbours of lambda_c / cs_d^2 ((l1 H1 + l2 H2) - H0 (l1 + l2)),
+// l1, l2 = harmonic means of the cell's and the neighbour's lambda_e mask (per component),
+// clamp / wrap boundaries; 0 where Msat0T0 = 0.  Neighbour indices are the grid's own in every
+// direction (the reference's a1 + 1 neighbour is computed with N1 in place of N2, which
+// differs from this only when N1 != N2).
+__global__ void d_nonlocal00nc(double* tx, double* ty, double* tz, const double* hx, const double* hy,
+                               const double* hz, const double* ms0T0m, const double* lxx, const double* lyy,
+                               const double* lzz, double Lx, double Ly, double Lz, int s0, int s1, int s2,
+                               double c0, double c1, double c2, int p0, int p1, int p2) {
+    const long n = (long)s0 * s1 * s2;
+    GRID_STRIDE(I, n) {
+        if (mu1(ms0T0m, I) == 0.0) {
+            tx[I] = ty[I] = tz[I] = 0.0;
+            continue;
+        }
+        const int k = (int)(I % s2);
+        const int j = (int)((I / s2) % s1);
+        const int i = (int)(I / ((long)s1 * s2));
+        const double* L[3] = {lxx, lyy, lzz};
+        const double* H[3] = {hx, hy, hz};
+        const double mul[3] = {Lx, Ly, Lz};
+        const long nb[3][2] = {
+            {((long)nb_lo(i, s0, p0) * s1 + j) * s2 + k, ((long)nb_hi(i, s0, p0) * s1 + j) * s2 + k},
+            {((long)i * s1 + nb_lo(j, s1, p1)) * s2 + k, ((long)i * s1 + nb_hi(j, s1, p1)) * s2 + k},
+            {((long)i * s1 + j) * s2 + nb_lo(k, s2, p2), ((long)i * s1 + j) * s2 + nb_hi(k, s2, p2)}};
+        const double inv_cs2[3] = {c0, c1, c2};
+        double out[3];
+        for (int c = 0; c < 3; c++) {
+            const double l0 = mu1(L[c], I), H0 = H[c][I];
+            double R = 0.0;
+            for (int d = 0; d < 3; d++) {
+                const double la = harm0(l0, mu1(L[c], nb[d][0])), lb = harm0(l0, mu1(L[c], nb[d][1]));
+                R += mul[c] * inv_cs2[d] * ((la * H[c][nb[d][0]] + lb * H[c][nb[d][1]]) - H0 * (la + lb));
+            }
+            out[c] = -R;
+        }
+        tx[I] = out[0];
+        ty[I] = out[1];
+        tz[I] = out[2];
+    }
+}
+
+HSB_EXPORT void llbar_nonlocal00nc_async(double* tx, double* ty, double* tz, double* hx, double* hy, double* hz,
+                                         double* msat0T0, double* lambda_e_xx, double* lambda_e_yy,
+                                         double* lambda_e_zz, const double lambda_eMul_xx,
+                                         const double lambda_eMul_yy, const double lambda_eMul_zz, const int sx,
+                                         const int sy, const int sz, const double csx, const double csy,
+                                         const double csz, const int pbc_x, const int pbc_y, const int pbc_z,
+                                         CUstream stream) {
+    const long n = (long)sx * sy * sz;
+    d_nonlocal00nc<<<g1(n), DROPIN_THREADS, 0, S(stream)>>>(
+        tx, ty, tz, hx, hy, hz, msat0T0, lambda_e_xx, lambda_e_yy, lambda_e_zz, lambda_eMul_xx, lambda_eMul_yy,
+        lambda_eMul_zz, sx, sy, sz, 1.0 / (csx * csx), 1.0 / (csy * csy), 1.0 / (csz * csz), pbc_x, pbc_y, pbc_z);
+    check_launch("llbar_nonlocal00nc_async");
+}
+
+
 HSB_EXPORT int hsb_mfa_table(double Tc, double J, int npts, double* T_host, double* me_host, double* chi_host) {
     if (!(Tc > 0) || !(J > 0) || npts < 1 || !T_host || !me_host || !chi_host) {
         hsb_set_error("hsb_mfa_table: bad argument");

@@ -144,6 +144,31 @@ void partialMaxNorm3SqDiffAsync(double* x1, double* y1, double* z1, double* x2, 
                                 double* output, int blocksPerGPU, int threadsPerBlockPerGPU, int NPerGPU,
                                 CUstream streams);
 
+
+/* replaces cpAsync, src/libhotspin/Cp.h:20 (Debye phonon heat capacity, trapezoid on 61
+ * intervals, low-temperature limit below T/Td = 0.01) */
+void cpAsync(double* Cp, double* T, double* Td, double* n, const double TdMul, const int Npart, CUstream stream);
+
+/* replaces tsAsync, src/libhotspin/Ts.h:18 (spin temperature from msat / Msat0T0, Ridders root) */
+void tsAsync(double* Ts, double* msat, double* msat0T0, double* Tc, double* S, const double msatMul,
+             const double msat0T0Mul, const double TcMul, const double SMul, int Npart, CUstream stream);
+
+/* replaces wavgAsync, src/libhotspin/wavg.h:20 (weighted average of two temperatures) */
+void wavgAsync(double* dst, double* a, double* b, double* w0, double* w1, double* R, double w0Mul, double w1Mul,
+               double RMul, CUstream stream, int Npart);
+
+/* replaces energyFlowAsync, src/libhotspin/energy_flow.h:18 */
+void energyFlowAsync(double* w, double* mx, double* my, double* mz, double* Rx, double* Ry, double* Rz, double* Tc,
+                     double* S, double* n, double SMul, int Npart, CUstream stream);
+
+/* replaces llbar_nonlocal00nc_async, src/libhotspin/llbar-nonlocal00nc.h:20; the a1 + 1
+ * neighbour uses the grid's own index (the reference's uses N1 for N2, the same when
+ * N1 == N2) */
+void llbar_nonlocal00nc_async(double* tx, double* ty, double* tz, double* hx, double* hy, double* hz,
+                              double* msat0T0, double* lambda_e_xx, double* lambda_e_yy, double* lambda_e_zz,
+                              const double lambda_eMul_xx, const double lambda_eMul_yy, const double lambda_eMul_zz,
+                              const int sx, const int sy, const int sz, const double csx, const double csy,
+                              const double csz, const int pbc_x, const int pbc_y, const int pbc_z, CUstream stream);
 #ifdef __cplusplus
 }
 #endif

@@ -466,3 +466,110 @@ def energy_term(m, H, msat_mask, msat_mul, weight):
     if msat_mask is not None:
         w = w * msat_mask
     return float(w.sum()) * msat_mul * weight
+
+
+# ----------------------------------------------------------------------------- remaining MFA / thermal kernels
+DEBYE_STEPS = 61          # common_func.h:27 INTMAXSTEPS
+
+
+def _debye_integrand(x):
+    """x^4 e^x / (e^x - 1)^2, 0 for x <= zero (common_func.h:168-173)."""
+    if x <= ZERO:
+        return 0.0
+    ex = math.exp(x)
+    return x ** 4 * ex / ((ex - 1.0) * (ex - 1.0))
+
+
+def debye_cp(T, Td_mask, n_mask, Td_mul):
+    """Debye phonon heat capacity per cell (cpKern, Cp.cu:13-88): n (T/Td)^3 times the
+    integral of x^4 e^x/(e^x-1)^2 over [0, Td/T] by the composite trapezoid rule on 61
+    intervals; the T/Td < 0.01 limit n (12/5)(1/9) pi^4 (T/Td)^3; 0 where Td = 0."""
+    T = np.asarray(T, dtype=np.float64)
+    out = np.zeros_like(T)
+    Td = Td_mul * _mask(Td_mask, T.shape)
+    n = _mask(n_mask, T.shape)
+    for idx in np.ndindex(T.shape):
+        td, t = Td[idx], T[idx]
+        if td == 0.0:
+            continue
+        xx, ixx = td / t, t / td
+        if ixx < 0.01:
+            out[idx] = n[idx] * (12.0 / 5.0) * (1.0 / 9.0) * math.pi ** 4 * ixx ** 3
+            continue
+        h = xx / DEBYE_STEPS
+        inner = sum(_debye_integrand(j * h) for j in range(1, DEBYE_STEPS))
+        val = (_debye_integrand(0.0) + _debye_integrand(DEBYE_STEPS * h) + 2.0 * inner) * 0.5 * h
+        out[idx] = n[idx] * val / xx ** 3
+    return out
+
+
+def spin_temperature(msat_mask, msat0T0_mask, Tc_mask, S_mask, msat_mul, msat0T0_mul, Tc_mul, S_mul, shape):
+    """Temperature whose mean-field equilibrium gives m = msat/Msat0T0 (tsKern, Ts.cu:84-125):
+    root of B_S(S^2 J0 m / T) - m on [0, Tc] by Ridders, J0 = 3 Tc/(S(S+1)); 0 where
+    Msat0T0 = 0 or msat = Msat0T0, Tc where msat = 0."""
+    out = np.zeros(shape)
+    ms = msat_mul * _mask(msat_mask, shape)
+    ms0 = msat0T0_mul * _mask(msat0T0_mask, shape)
+    Tc = Tc_mul * _mask(Tc_mask, shape)
+    S = S_mul * _mask(S_mask, shape)
+    for idx in np.ndindex(shape):
+        if ms0[idx] == 0.0 or ms[idx] == ms0[idx]:
+            continue
+        if ms[idx] == 0.0:
+            out[idx] = Tc[idx]
+            continue
+        s, tc = S[idx], Tc[idx]
+        m = ms[idx] / ms0[idx]
+        pre = s * s * (3.0 * tc / (s * (s + 1.0))) * m
+        out[idx] = _ridders(lambda t: float(brillouin(s, 1.0e38 if t == 0.0 else pre / t)) - m, 0.0, tc)
+    return out
+
+
+def weighted_avg(a, b, w0_mask, w1_mask, R_mask, w0_mul, w1_mul, R_mul):
+    """(w0 a + w1 b + 2R sqrt(w0 a w1 b)) / (w0 + w1 + 2R sqrt(w0 w1)), 0 where the
+    denominator vanishes (wavgKern, wavg.cu:13-30; common_func.h:162-166)."""
+    shape = np.shape(a)
+    w0 = w0_mul * _mask(w0_mask, shape)
+    w1 = w1_mul * _mask(w1_mask, shape)
+    R = R_mul * _mask(R_mask, shape)
+    den = w0 + w1 + 2.0 * R * np.sqrt(w0 * w1)
+    num = w0 * a + w1 * b + 2.0 * R * np.sqrt(w0 * a * w1 * b)
+    return np.where(den == 0.0, 0.0, num / np.where(den == 0.0, 1.0, den))
+
+
+def energy_flow(m, R, Tc_mask, S_mask, n_mask, S_mul):
+    """Tc S^2 n / (S(S+1)) (m . R) with Tc and n from their masks alone (energyFlowKern,
+    energy_flow.cu:15-44); 0 where n, S or Tc is 0."""
+    shape = m.shape[1:]
+    S = S_mul * _mask(S_mask, shape)
+    Tc = _mask(Tc_mask, shape)
+    n = _mask(n_mask, shape)
+    ok = (n != 0.0) & (S != 0.0) & (Tc != 0.0)
+    Ss = np.where(ok, S, 1.0)
+    mult = Tc * Ss * Ss * n / (Ss * (Ss + 1.0))
+    return np.where(ok, mult * (m * R).sum(0), 0.0)
+
+
+def llbar_nonlocal00nc(h, msat0T0_mask, lam_masks, lam_mul, cellsize, pbc):
+    """Nonlocal (exchange-like) damping torque (llbarNonlocal00ncKern,
+    llbar-nonlocal00nc.cu:11-205): t_c = -sum_d lam_c/cs_d^2 ((l1 H1 + l2 H2) - H0 (l1 + l2))
+    with l1, l2 the harmonic means of the lambda_e mask of the cell and each neighbour
+    (per component), clamp/wrap boundaries, 0 where Msat0T0 = 0.  The reference computes the
+    a1 + 1 neighbour's index with N1 in place of N2; this restatement uses the grid's index
+    (the two agree when N1 == N2)."""
+    shape = h.shape[1:]
+    out = np.zeros_like(h)
+    for c in range(3):
+        lm = _mask(lam_masks[c] if lam_masks is not None else None, shape)
+        acc = np.zeros(shape)
+        for d in range(3):
+            lo = np.take(lm, _neighbour_index(shape[d], pbc[d], -1), axis=d)
+            hi = np.take(lm, _neighbour_index(shape[d], pbc[d], +1), axis=d)
+            Hlo = np.take(h[c], _neighbour_index(shape[d], pbc[d], -1), axis=d)
+            Hhi = np.take(h[c], _neighbour_index(shape[d], pbc[d], +1), axis=d)
+            l1, l2 = avg_geom_zero(lm, lo), avg_geom_zero(lm, hi)
+            acc += lam_mul[c] / (cellsize[d] ** 2) * ((l1 * Hlo + l2 * Hhi) - h[c] * (l1 + l2))
+        out[c] = -acc
+    if msat0T0_mask is not None:
+        out = np.where(np.asarray(msat0T0_mask)[None] == 0.0, 0.0, out)
+    return out

@@ -82,3 +82,51 @@ def test_dp45_reaches_tolerance():
     while it.t < 1e-10:
         it.step()
     assert it.step_count > 5 and it.dt > 1e-13
+
+
+def test_debye_cp_restatement():
+    """Trapezoid Debye integral: close to the exact integral, the T << Td limit, zero Td."""
+    from scipy.integrate import quad
+    T = np.array([[[5.0, 150.0, 300.0, 2000.0]]])
+    Td = np.full(T.shape, 300.0)
+    got = fields.debye_cp(T, Td, None, 1.0)
+    for v, t in zip(got.ravel(), T.ravel()):
+        u = 300.0 / t
+        exact = quad(lambda x: x ** 4 * np.exp(x) / np.expm1(x) ** 2 if x > 0 else 0.0, 0, u)[0] / u ** 3
+        assert abs(v - exact) < 2e-3 * exact
+    # high-temperature limit: (T/Td)^3 * (Td/T)^3 / 3 -> 1/3
+    assert abs(got.ravel()[-1] - 1.0 / 3.0) < 2e-3
+    low = fields.debye_cp(np.array([[[1.0]]]), np.array([[[300.0]]]), None, 1.0).ravel()[0]
+    assert abs(low - 4 * np.pi ** 4 / 15 / 300.0 ** 3) < 1e-12 * low
+    assert fields.debye_cp(np.array([[[10.0]]]), np.array([[[0.0]]]), None, 1.0).ravel()[0] == 0.0
+
+
+def test_spin_temperature_inverts_equilibrium():
+    """Ts(m_e(T)) = T for the mean-field equilibrium (J = 1/2 and 7/2)."""
+    for S in (0.5, 3.5):
+        for T in (100.0, 350.0, 600.0):
+            me = fields.equilibrium_m(T, 630.0, S)
+            ts = fields.spin_temperature(np.array([[[me]]]), None, None, None, 1.0, 1.0, 630.0, S, (1, 1, 1))
+            assert abs(ts.ravel()[0] - T) < 1e-5 * T
+    edge = fields.spin_temperature(np.array([[[0.0, 1.0]]]), None, None, None, 1.0, 1.0, 630.0, 0.5, (1, 1, 2))
+    assert edge.ravel().tolist() == [630.0, 0.0]
+
+
+def test_weighted_avg_energy_flow_nonlocal():
+    a, b = np.array([400.0, 300.0, 1.0]), np.array([400.0, 500.0, 2.0])
+    w = fields.weighted_avg(a, b, None, None, None, 1.0, 1.0, 0.0)
+    assert np.allclose(w, (a + b) / 2)
+    w = fields.weighted_avg(a, b, np.array([1.0, 1.0, 0.0]), np.array([1.0, 1.0, 0.0]), None, 1.0, 1.0, 1.0)
+    assert np.allclose(w[:2], ((np.sqrt(a) + np.sqrt(b)) / 2)[:2] ** 2) and w[2] == 0.0
+    m = np.zeros((3, 1, 1, 2))
+    m[2] = 1.0
+    R = np.ones((3, 1, 1, 2))
+    ef = fields.energy_flow(m, R, np.array([[[630.0, 0.0]]]), None, None, 0.5)
+    assert np.allclose(ef.ravel(), [630.0 * 0.25 / 0.75, 0.0])
+    # uniform lambda: the nonlocal term is -lambda times the Laplacian of H
+    rng = np.random.default_rng(1)
+    h = rng.normal(size=(3, 4, 5, 6))
+    cs = (1.0, 2.0, 3.0)
+    t = fields.llbar_nonlocal00nc(h, None, None, (1.0, 1.0, 1.0), cs, (1, 1, 1))
+    lap = sum((np.roll(h, 1, axis=d + 1) + np.roll(h, -1, axis=d + 1) - 2 * h) / cs[d] ** 2 for d in range(3))
+    assert np.allclose(t, -lap)

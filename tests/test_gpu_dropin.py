@@ -256,3 +256,59 @@ def test_exchange_golden_through_dropin(lib, cuda):
                        D(c[1]), D(c[2]), None)
     want = fields.exchange6(m, lex, 800e3, lex0, CELL_PROGRAM, (0, 0, 0), weight_power=2)
     assert rel_err(host(cuda, dh), want) < 1e-12
+
+
+def test_remaining_mfa_kernels(lib, cuda):
+    """Debye heat capacity, spin temperature, weighted temperature average, energy flow."""
+    rng = np.random.default_rng(21)
+    T = rng.uniform(1.0, 900.0, size=SIZE)
+    T[0, 0, 0] = 1.0            # low-temperature limit branch
+    Td = rng.uniform(200.0, 400.0, size=SIZE)
+    Td[0, 0, 1] = 0.0
+    n = rng.uniform(0.5, 2.0, size=SIZE)
+    dT, dTd, dn = dev(cuda, T), dev(cuda, Td), dev(cuda, n)
+    out = cuda.empty_like(dT)
+    lib.cpAsync(ptr(out), ptr(dT), ptr(dTd), ptr(dn), D(1.0), I(N), None)
+    assert rel_err(host(cuda, out), fields.debye_cp(T, Td, n, 1.0)) < 1e-12
+
+    ms0 = rng.uniform(5e5, 1e6, size=SIZE)
+    ms = ms0 * rng.uniform(0.05, 0.99, size=SIZE)
+    ms[1, 0, 0] = 0.0
+    ms[1, 0, 1] = ms0[1, 0, 1]
+    dms, dms0 = dev(cuda, ms), dev(cuda, ms0)
+    for S in (0.5, 3.5):
+        lib.tsAsync(ptr(out), ptr(dms), ptr(dms0), None, None, D(1.0), D(1.0), D(630.0), D(S), I(N), None)
+        want = fields.spin_temperature(ms, ms0, None, None, 1.0, 1.0, 630.0, S, SIZE)
+        assert rel_err(host(cuda, out), want) < 1e-7
+
+    a, b = rng.uniform(300, 900, size=SIZE), rng.uniform(300, 400, size=SIZE)
+    w0, w1 = rng.uniform(0, 2, size=SIZE), rng.uniform(0, 2, size=SIZE)
+    w0[2, 2, 2] = w1[2, 2, 2] = 0.0
+    da, db, dw0, dw1 = dev(cuda, a), dev(cuda, b), dev(cuda, w0), dev(cuda, w1)
+    lib.wavgAsync(ptr(out), ptr(da), ptr(db), ptr(dw0), ptr(dw1), None, D(1.5), D(0.7), D(0.3), None, I(N))
+    assert rel_err(host(cuda, out), fields.weighted_avg(a, b, w0, w1, None, 1.5, 0.7, 0.3)) < 1e-13
+
+    m, R = unit(22), rng.normal(size=(3,) + SIZE)
+    Tc = rng.uniform(500, 700, size=SIZE)
+    Tc[3, 3, 3] = 0.0
+    dm, dR, dTc = dev(cuda, m), dev(cuda, R), dev(cuda, Tc)
+    lib.energyFlowAsync(ptr(out), *comps(dm), *comps(dR), ptr(dTc), None, ptr(dn), D(0.5), I(N), None)
+    assert rel_err(host(cuda, out), fields.energy_flow(m, R, Tc, None, n, 0.5)) < 1e-13
+
+
+@pytest.mark.parametrize("pbc", [(0, 0, 0), (1, 1, 0), (0, 1, 1)])
+def test_nonlocal_damping(lib, cuda, pbc):
+    rng = np.random.default_rng(23)
+    h = rng.normal(size=(3,) + SIZE) * 1e5
+    lam = [rng.uniform(0.1, 1.0, size=SIZE) for _ in range(3)]
+    lam[1][2, 3, 4] = 0.0
+    ms0 = rng.uniform(0.5, 1.0, size=SIZE)
+    ms0[0, 0, 0] = 0.0
+    dh, dms0 = dev(cuda, h), dev(cuda, ms0)
+    dl = [dev(cuda, x) for x in lam]
+    out = cuda.empty_like(dh)
+    lib.llbar_nonlocal00nc_async(*comps(out), *comps(dh), ptr(dms0), *[ptr(x) for x in dl], D(1e-18), D(2e-18),
+                                 D(3e-18), I(SIZE[0]), I(SIZE[1]), I(SIZE[2]), D(CS[0]), D(CS[1]), D(CS[2]),
+                                 I(pbc[0]), I(pbc[1]), I(pbc[2]), None)
+    want = fields.llbar_nonlocal00nc(h, ms0, lam, (1e-18, 2e-18, 3e-18), CS, pbc)
+    assert rel_err(host(cuda, out), want) < 1e-12
