@@ -189,3 +189,44 @@ def test_thermal_field_statistics(cuda):
     n = Hz.size
     assert abs(Hz.mean()) < 4 * np.sqrt(var / n)
     assert abs(Hz.var() / var - 1) < 4 * np.sqrt(2.0 / n)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 4])
+def test_stage_kernel_variants_agree(cuda, variant):
+    """Every stage-kernel variant integrates the same trajectories as the default one, up to
+    FP32 rounding order: DP45 on TTM + LLB + demag + laser from a state near equilibrium, and
+    fixed-step RK4 with the thermal field.  (Stochastic DP45 runs are compared statistically
+    only: the noise amplitude scales with the accepted dt, and FP32 rounding in the error
+    estimate moves the step sizes.)"""
+    from hotspin_b200 import _lib
+    lib = _lib.load()
+    kw = dict(TTM, size=(2, 16, 32), seed=5, laser_t0=5e-14)
+    size = kw["size"]
+    rng = np.random.default_rng(12)
+    th, ph = np.deg2rad(5.0) * rng.random(size), 2 * np.pi * rng.random(size)
+    me = F.equilibrium_m(300.0, kw["tc"], 0.5)
+    y = {"m": me * np.stack([np.cos(th), np.sin(th) * np.sin(ph), np.sin(th) * np.cos(ph)]),
+         "Te": np.full(size, 300.0), "Tl": np.full(size, 300.0)}
+    runs = [dict(thermal=False, solver="dp45", dt=1e-16, t_end=2e-13),
+            dict(thermal=True, solver="rk4", dt=1e-15, steps=20)]
+    default = lib.hsb_set_stage_variant(2)
+    try:
+        for run in runs:
+            out = {}
+            for v in (2, variant):
+                lib.hsb_set_stage_variant(v)
+                with Simulation(**dict(kw, thermal=run["thermal"]), solver=run["solver"], dt=run["dt"], rtol=1e-5,
+                                mindt=1e-20, maxdt=1e-13) as sim:
+                    for name, val in y.items():
+                        sim.set(name, val)
+                    if "steps" in run:
+                        sim.step(run["steps"])
+                    else:
+                        sim.run_until(run["t_end"])
+                    out[v] = (sim.get("m"), sim.get("Te"), sim.status())
+            (m2, T2, s2), (mv, Tv, sv) = out[2], out[variant]
+            assert s2["t"] == pytest.approx(sv["t"], rel=1e-12)
+            assert np.abs(m2 - mv).max() < 1e-5, run
+            assert np.abs(T2 - Tv).max() < 1e-5 * T2.max(), run
+    finally:
+        lib.hsb_set_stage_variant(default)
