@@ -31,6 +31,12 @@ MU0 = 4e-7 * math.pi
 MUB = 9.27400968202020202e-24
 
 
+# DRAM bytes (read + write) per launch of each kernel family on this workload, from one ncu
+# capture each (dram__bytes_read.sum + dram__bytes_write.sum; stage: the 7 launches of one
+# DP45 attempt averaged; profiles/stage_kernel_512x512x4.md, profiles/demag_fft_kernels_512x512x4.md).
+TRAFFIC_PER_LAUNCH = {"stage": 133_478_000, "yz": 56_891_000, "xfwd": 12_633_000, "xinv": 25_285_000}
+
+
 def workload():
     """Program order: (N0, N1, N2) = (z, y, x)."""
     ms = 8e5
@@ -224,10 +230,7 @@ def run_ours(args):
     byt, tms, nlaunch = per_launch[dom]
     peak, kind = peaks()
     achieved = (byt / nlaunch) / ((tms / nlaunch) / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(dom)
+    traffic = TRAFFIC_PER_LAUNCH.get(dom)
     names = {"stage": "k_stagec<5,0,2,NK> (load-first fused RHS + DP45 stage; 7 launches per attempt)",
              "yz": "k_yz4<1024,8,1> (y/z FFT + tensor multiply + inverse)",
              "xfwd": "k_xfwd4<512,1> (R2C + transpose)", "xinv": "k_xinv4<512,1> (C2R)"}
