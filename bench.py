@@ -157,17 +157,20 @@ def cpu_baseline(kw, state):
                       "NumPy oracle, %.1f s" % (7 * (1 + it.bad_steps), dtw)}
 
 
-def dist_setup():
+def dist_setup(backend="nccl"):
+    """One process per GPU (torchrun environment); replicas only, so the process group carries
+    nothing but the barrier and the max-over-ranks of the timings."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     import torch
-    torch.cuda.set_device(local)
+    if backend == "nccl":
+        torch.cuda.set_device(local)
     pg = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
@@ -177,13 +180,19 @@ def barrier(pg):
         pg.barrier()
 
 
-def max_over_ranks(pg, v):
+def max_over_ranks(pg, v, device="cuda"):
     if pg is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=device)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_value(world, ncell, steps, ms_max):
+    """Mcell-steps/s of all replicas together: every rank advances its own copy of the
+    workload, and the job takes as long as the slowest rank."""
+    return world * ncell * steps / (ms_max / 1e3) / 1e6
 
 
 def run_ours(args):
@@ -216,7 +225,7 @@ def run_ours(args):
     nl = ctypes_int()
     _lib.check(sim._lib.hsb_sim_launches_per_attempt(sim._h, nl), "launches")
     launches = attempts * nl.value
-    value = world * ncell * args.steps / (ms / 1e3) / 1e6
+    value = whole_job_value(world, ncell, args.steps, ms)
     # ---- live per-kernel timing of one attempt (eager launches between CUDA events)
     prof = (ctypes_double * 7)()
     _lib.check(sim._lib.hsb_sim_profile(sim._h, 3, prof), "profile")
