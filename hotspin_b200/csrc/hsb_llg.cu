@@ -1050,12 +1050,20 @@ __global__ void k_fixed_advance(HsbSolverDev* sd0, int nslot) {
 
 // ------------------------------------------------------------------------------ launchers
 // Stage-kernel variant for grids without masks: 0 = k_stage4, 1 / 2 / 4 = k_stagec with 1 / 2 /
-// 4 cells per thread (the load-first form).  Set by hsb_set_stage_variant (tuning sweeps).
-static int g_stage_variant = 2;
+// 4 cells per thread (the load-first form).  Each simulation passes the variant its tuning
+// picked (hsb_sim.cu); hsb_set_stage_variant forces one for every launch (tuning sweeps), -1
+// returns to the per-simulation choice.
+static int g_stage_force = -1;
+static const int STAGE_DEFAULT = 2;
+
+static int stage_variant(int requested) {
+    if (g_stage_force >= 0) return g_stage_force;
+    return requested >= 0 ? requested : STAGE_DEFAULT;
+}
 
 HSB_EXPORT int hsb_set_stage_variant(int v) {
-    const int old = g_stage_variant;
-    if (v == 0 || v == 1 || v == 2 || v == 4) g_stage_variant = v;
+    const int old = g_stage_force;
+    if (v == -1 || v == 0 || v == 1 || v == 2 || v == 4) g_stage_force = v;
     return old;
 }
 
@@ -1089,8 +1097,8 @@ static void launch_c(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, con
 
 template <int CH, bool BATCH>
 static void launch_vec(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt, int nslot,
-                       cudaStream_t st) {
-    const int v = (A.err && (A.ynext.p[0] || A.ynext.p[1])) ? 0 : g_stage_variant;
+                       cudaStream_t st, int variant) {
+    const int v = (A.err && (A.ynext.p[0] || A.ynext.p[1])) ? 0 : stage_variant(variant);
     if (v == 0) {
         const int threads = 256;
         long g = (P.ncell / 4 + threads - 1) / threads;
@@ -1108,16 +1116,19 @@ static void launch_vec(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, c
 
 // True when stage launches of this simulation run the load-first kernel, which is the one
 // that can keep the step's thermal field (StageArgs.hth_mode).
-bool hsb_stage_keeps_thermal(const HsbPhys& P) {
-    return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask && g_stage_variant != 0;
+bool hsb_stage_keeps_thermal(const HsbPhys& P, int variant) {
+    return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask && stage_variant(variant) != 0;
 }
 
-int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st) {
+// True when the stage launches of this geometry can take a variant (no masks, a2 % 4 == 0).
+bool hsb_stage_tunable(const HsbPhys& P) { return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask; }
+
+int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st, int variant) {
     const int threads = 256;
     if (P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask) {
         BatchArgs nb = {0, nullptr, 1};
-        if (P.nch == 5) launch_vec<5, false>(P, A, sd, nb, 1, st);
-        else launch_vec<3, false>(P, A, sd, nb, 1, st);
+        if (P.nch == 5) launch_vec<5, false>(P, A, sd, nb, 1, st, variant);
+        else launch_vec<3, false>(P, A, sd, nb, 1, st, variant);
         return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
     }
     const int grid = hsb_grid_1d(P.ncell, threads, 8);
@@ -1143,12 +1154,10 @@ int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st) {
 // Batched variants: one grid plane per slot (blockIdx.z); Bt.phys / sd are slot arrays.
 // P carries the class-wide geometry (size, channels; masks are not supported in batches).
 int hsb_launch_stage_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
-                             cudaStream_t st) {
-    const int threads = 256;
-    (void)threads;
+                             cudaStream_t st, int variant) {
     if (P.N2 % 4 != 0 || P.msat_mask || P.lex_mask) return HSB_ERR_UNSUPPORTED;
-    if (P.nch == 5) launch_vec<5, true>(P, A, sd, Bt, Bt.nslot, st);
-    else launch_vec<3, true>(P, A, sd, Bt, Bt.nslot, st);
+    if (P.nch == 5) launch_vec<5, true>(P, A, sd, Bt, Bt.nslot, st, variant);
+    else launch_vec<3, true>(P, A, sd, Bt, Bt.nslot, st, variant);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }
 

@@ -10,6 +10,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -17,13 +19,15 @@
 #include "hsb_demag.h"
 #include "hsb_llg.cuh"
 
-int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st);
-bool hsb_stage_keeps_thermal(const HsbPhys& P);
+int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st, int variant = -1);
+bool hsb_stage_keeps_thermal(const HsbPhys& P, int variant);
+bool hsb_stage_tunable(const HsbPhys& P);
+extern "C" int hsb_set_stage_variant(int v);
 int hsb_launch_combine(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st);
 int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st);
 int hsb_launch_fixed_advance(HsbSolverDev* sd, cudaStream_t st);
 int hsb_launch_stage_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
-                             cudaStream_t st);
+                             cudaStream_t st, int variant = -1);
 int hsb_launch_combine_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
                                cudaStream_t st);
 int hsb_launch_dp45_control_batched(HsbSolverDev* sd, int nslot, cudaStream_t st);
@@ -91,6 +95,7 @@ struct hsb_sim_s {
     hsb_demag_spec_s* spec;  // batched: FP64 scratch of the kernel-spectrum evaluation
     BatchArgs bt;
     bool prep_mode;     // enqueueing the preparation of newly admitted slots
+    int stage_variant;  // stage-kernel variant picked by tune_stage (-1: the library default)
     int nprep;          // slots admitted since the last launch
     cudaEvent_t done_ev;
     bool launched;
@@ -354,8 +359,8 @@ static int timed(hsb_sim_s* S, int cat, F&& f) {
 // Launches of one simulation or of a batch of slots.
 static int L_stage(hsb_sim_s* S, StageArgs A) {
     if (S->prep_mode) A.prep_gated = 1;
-    if (S->batched) return hsb_launch_stage_batched(S->P, A, S->sd, S->bt, S->st);
-    return hsb_launch_stage(S->P, A, S->sd, S->st);
+    if (S->batched) return hsb_launch_stage_batched(S->P, A, S->sd, S->bt, S->st, S->stage_variant);
+    return hsb_launch_stage(S->P, A, S->sd, S->st, S->stage_variant);
 }
 static int L_combine(hsb_sim_s* S, const StageArgs& A) {
     if (S->batched) return hsb_launch_combine_batched(S->P, A, S->sd, S->bt, S->st);
@@ -368,7 +373,7 @@ static int L_control(hsb_sim_s* S) {
 // Thermal field of the step: generated and kept by the attempt's first stage, read by the
 // others (only the load-first stage kernel keeps it).
 static void thermal_keep(hsb_sim_s* S, StageArgs& A, bool first) {
-    if (!S->hth || !hsb_stage_keeps_thermal(S->P)) return;
+    if (!S->hth || !hsb_stage_keeps_thermal(S->P, S->stage_variant)) return;
     A.hth = fixed(S->hth);
     A.hth_mode = first ? 1 : 2;
 }
@@ -828,6 +833,82 @@ __global__ void k_fill(float* p, long n, float v) {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) p[i] = v;
 }
 
+// Launch-shape tuning of the stage kernel: the load-first kernel with 1, 2 and 4 cells per
+// thread is timed on a representative stage of this simulation (a DP45 mid-attempt stage with
+// four stage derivatives, or an RK stage with one), ungated, on the simulation's own (zeroed)
+// buffers with its outputs in the stage-point scratch; the fastest is kept.  Every variant
+// computes each cell with the same arithmetic.  Results are cached per geometry, channel
+// count, physics flags, solver and slot count for the process.  The solver words must hold a
+// valid dt; the caller re-uploads them afterwards (a timing launch may flag them).
+static std::mutex g_stune_mu;
+static std::map<std::vector<long>, int> g_stune;
+
+static int tune_stage(hsb_sim_s* S) {
+    S->stage_variant = -1;
+    if (!hsb_stage_tunable(S->P)) return HSB_OK;
+    const hsb_sim_desc& d = S->d;
+    const std::vector<long> key = {S->P.N0, S->P.N1, S->P.N2, S->nch, d.llb, d.thermal, d.solver, d.demag, S->nslot};
+    {
+        std::lock_guard<std::mutex> lk(g_stune_mu);
+        auto it = g_stune.find(key);
+        if (it != g_stune.end()) {
+            S->stage_variant = it->second;
+            return HSB_OK;
+        }
+    }
+    StageArgs A = empty_args();
+    A.ungated = 1;
+    A.ys = fixed(S->y[0]);
+    A.hd = S->demag ? fixed(S->hd) : none();
+    A.ytherm = fixed(S->y[0]);
+    A.tfrac = 0.5f;
+    A.kout = fixed(S->ystage[1]);
+    A.kself_w = 1.0f;
+    A.ynext = fixed(S->ystage[0]);
+    A.ybase = fixed(S->y[0]);
+    A.nk = (d.solver == SOLVER_DP45) ? 4 : 1;
+    for (int j = 0; j < A.nk; j++) {
+        A.kin[j] = fixed(S->k[j]);
+        A.ck[j] = (d.solver == SOLVER_DP45) ? (float)DPA[5][j] : 0.5f;
+    }
+    A.cself = 0.1f;
+    A.normalize = S->batched ? 1 : d.normalize;
+    cudaEvent_t e0, e1;
+    HSB_CUDA_TRY(cudaEventCreate(&e0));
+    HSB_CUDA_TRY(cudaEventCreate(&e1));
+    const int cand[3] = {1, 2, 4};
+    int best = -1;
+    float best_ms = 1e30f;
+    int rc = HSB_OK;
+    for (int c = 0; c < 3 && rc == HSB_OK; c++) {
+        float acc = 0.f;
+        for (int rep = 0; rep < 4 && rc == HSB_OK; rep++) {
+            cudaEventRecord(e0, S->st);
+            rc = S->batched ? hsb_launch_stage_batched(S->P, A, S->sd, S->bt, S->st, cand[c])
+                            : hsb_launch_stage(S->P, A, S->sd, S->st, cand[c]);
+            cudaEventRecord(e1, S->st);
+            if (cudaEventSynchronize(e1) != cudaSuccess) rc = HSB_ERR_CUDA;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) acc += ms;   // the first launch is a warm-up
+        }
+        if (rc == HSB_OK && acc < best_ms) {
+            best_ms = acc;
+            best = cand[c];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != HSB_OK) {
+        hsb_set_error("stage-kernel tuning failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return rc;
+    }
+    S->stage_variant = best;
+    std::lock_guard<std::mutex> lk(g_stune_mu);
+    g_stune[key] = best;
+    return HSB_OK;
+}
+
 static int check_desc(const hsb_sim_desc& d, const char* who) {
     for (int a = 0; a < 3; a++) {
         if (d.size[a] < 1 || d.cellsize[a] <= 0 || d.pbc[a] < 0) {
@@ -876,6 +957,7 @@ HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     STRY(cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking));
     const SlotLayout L = slot_layout(d, n);
     STRY(cudaMalloc(&S->arena, sizeof(float) * L.total));
+    STRY(cudaMemsetAsync(S->arena, 0, sizeof(float) * L.total, S->st));
     point_slot0(S, L);
     STRY(cudaMalloc(&S->sd, sizeof(HsbSolverDev)));
     STRY(cudaMallocHost(&S->sd_host, sizeof(HsbSolverDev)));
@@ -900,6 +982,14 @@ HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     S->sd_host->maxdt = d.maxdt > 0 ? d.maxdt : 1e-9;
     S->sd_host->step_stop = -1;
     S->sd_host->active = 1;
+    STRY(cudaMemcpyAsync(S->sd, S->sd_host, sizeof(HsbSolverDev), cudaMemcpyHostToDevice, S->st));
+    {
+        const int rc = tune_stage(S);
+        if (rc != HSB_OK) {
+            free_sim(S);
+            return rc;
+        }
+    }
     STRY(cudaMemcpyAsync(S->sd, S->sd_host, sizeof(HsbSolverDev), cudaMemcpyHostToDevice, S->st));
     STRY(cudaStreamSynchronize(S->st));
     // launch-bound grids batch more steps per graph launch
@@ -1013,7 +1103,7 @@ HSB_EXPORT int hsb_sim_get(hsb_sim_s* S, const char* name, double* host, int64_t
         A.ytherm = fixed(y);
         A.kout = fixed(S->ystage[1]);
         A.kself_w = 1.0f;
-        RC(hsb_launch_stage(S->P, A, S->sd, S->st));
+        RC(hsb_launch_stage(S->P, A, S->sd, S->st, S->stage_variant));
         src = S->ystage[1];
         nv = (long)S->nch * S->n;
         S->initialized = false;
@@ -1259,6 +1349,7 @@ HSB_EXPORT int hsb_batch_create(const hsb_sim_desc* cls, int32_t nslot, hsb_sim_
     STRY(cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking));
     const SlotLayout L = slot_layout(d, n);
     STRY(cudaMalloc(&S->arena, sizeof(float) * L.total * nslot));
+    STRY(cudaMemsetAsync(S->arena, 0, sizeof(float) * L.total * nslot, S->st));
     point_slot0(S, L);
     STRY(cudaMalloc(&S->sd, sizeof(HsbSolverDev) * nslot));
     STRY(cudaMallocHost(&S->sd_host, sizeof(HsbSolverDev) * nslot));
@@ -1301,6 +1392,18 @@ HSB_EXPORT int hsb_batch_create(const hsb_sim_desc* cls, int32_t nslot, hsb_sim_
     S->graph_steps = tot < 65536 ? 16 : (tot < 1048576 ? 8 : 4);
     if (d.solver == SOLVER_DP45) S->graph_steps = tot < 65536 ? 8 : 4;
     S->initialized = true;
+    {
+        // tune with a valid dt in every solver word, then clear them again (all slots empty)
+        for (int k = 0; k < nslot; k++) S->sd_host[k].dt = d.dt;
+        STRY(cudaMemcpyAsync(S->sd, S->sd_host, sizeof(HsbSolverDev) * nslot, cudaMemcpyHostToDevice, S->st));
+        const int rc = tune_stage(S);
+        if (rc != HSB_OK) {
+            free_sim(S);
+            return rc;
+        }
+        memset(S->sd_host, 0, sizeof(HsbSolverDev) * nslot);
+        STRY(cudaMemsetAsync(S->sd, 0, sizeof(HsbSolverDev) * nslot, S->st));
+    }
     STRY(cudaStreamSynchronize(S->st));
     *out = S;
     return HSB_OK;
@@ -1498,6 +1601,14 @@ HSB_EXPORT int hsb_batch_release(hsb_sim_s* B, int32_t slot) {
 HSB_EXPORT int hsb_batch_destroy(hsb_sim_s* B) { return hsb_sim_destroy(B); }
 
 // Slots, attempts of every slot per class-graph launch, cells per slot.
+// Stage-kernel variant a handle (simulation or batch) runs: picked by the tuning at creation,
+// or forced by hsb_set_stage_variant.
+HSB_EXPORT int hsb_stage_variant_of(hsb_sim_s* S) {
+    if (!S) return -1;
+    const int forced = hsb_set_stage_variant(-2);   // reads the forced value (-2 changes nothing)
+    return forced >= 0 ? forced : (S->stage_variant >= 0 ? S->stage_variant : 2);
+}
+
 HSB_EXPORT int hsb_batch_info(hsb_sim_s* B, int32_t* nslot, int32_t* attempts_per_graph, int64_t* ncell) {
     if (!B || !B->batched) return HSB_ERR_INVALID;
     if (nslot) *nslot = B->nslot;

@@ -147,12 +147,16 @@ int hsb_mfa_equilibrium(double T, double Tc, double J, double* me);
  * scratch: calls that overlap on the GPU race and must be serialised. */
 int hsb_average_m_noalloc(const float* m, int64_t ncell, double* avg3, void* stream);
 
-/* Stage-kernel variant used by subsequently built launches (no reference counterpart; a
- * tuning knob): 0 = four cells per thread, loads as needed; 1 / 2 / 4 = load-first kernel with
- * 1 / 2 / 4 cells per thread (default 2).  All variants compute each cell identically up to
- * FP32 rounding order; other values are ignored.
- * Returns the previous value. */
+/* Stage-kernel variants (no reference counterpart): 0 = four cells per thread, loads as
+ * needed; 1 / 2 / 4 = load-first kernel with 1 / 2 / 4 cells per thread.  Every simulation and
+ * batch times variants 1, 2 and 4 on its own buffers at creation and keeps the fastest
+ * (cached per geometry and physics flags for the process).  hsb_set_stage_variant forces one
+ * variant for launches built afterwards (tuning sweeps); -1 returns to the per-handle choice;
+ * other values change nothing.  Returns the previous forced value (-1 = none).  All variants
+ * compute each cell identically up to FP32 rounding order. */
 int hsb_set_stage_variant(int v);
+/* The variant a handle (simulation or batch) runs. */
+int hsb_stage_variant_of(hsb_sim sim);
 
 /* The handle's CUDA stream (cudaStream_t) for callers that interleave their own work. */
 void* hsb_sim_stream(hsb_sim sim);

@@ -210,6 +210,7 @@ def test_stage_kernel_variants_agree(cuda, variant):
     runs = [dict(thermal=False, solver="dp45", dt=1e-16, t_end=2e-13),
             dict(thermal=True, solver="rk4", dt=1e-15, steps=20)]
     default = lib.hsb_set_stage_variant(2)
+    assert default == -1     # no variant forced outside this test
     try:
         for run in runs:
             out = {}
@@ -230,3 +231,11 @@ def test_stage_kernel_variants_agree(cuda, variant):
             assert np.abs(T2 - Tv).max() < 1e-5 * T2.max(), run
     finally:
         lib.hsb_set_stage_variant(default)
+
+
+def test_stage_tuning_picks_a_variant(cuda):
+    """Each handle runs the stage-kernel variant its creation-time tuning picked."""
+    from hotspin_b200 import _lib
+    lib = _lib.load()
+    with Simulation(**dict(LLG, size=(2, 16, 32)), solver="dp45", dt=1e-15) as sim:
+        assert lib.hsb_stage_variant_of(sim._h) in (1, 2, 4)
