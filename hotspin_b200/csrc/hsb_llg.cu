@@ -1,7 +1,8 @@
 // Fused LLBar / LLB / two-temperature right-hand side and Runge-Kutta stage update.
 //
 // One thread per cell evaluates, in registers, everything hotspin computes with a chain of
-// separate kernels and host syncs per right-hand side (SURVEY call stack CS2):
+// separate kernels and host syncs per right-hand side (engine/quant.go:417-445 walking the
+// updaters of the modules below):
 //   H_eff = H_ex (exchange6.cu:11-127) + H_anis (uniaxialanisotropy.cu:12-52)
 //         + B_ext/mu0 (mod_zeeman.go) + H_demag (input) + H_lf (long_field.cu:13-72)
 //         + H_therm (temperature.cu:14-70 on Philox normals)

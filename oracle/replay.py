@@ -1,6 +1,6 @@
 """Replay of hotspin's per-step call sequence on the reference's own CUDA library.
 
-TEST AND BASELINE INFRASTRUCTURE.  hotspin's host is Go (no toolchain in this image), so
+TEST AND REFERENCE-ARM INFRASTRUCTURE.  hotspin's host is Go (no toolchain in this image), so
 its engine cannot run; its CUDA kernel library can (built from the reference sources by
 ``oracle/ref.mk`` into ``oracle/_ref/libhotspin.so``).  This module issues the calls the Go
 updaters issue for one right-hand side, in their order, each followed by a stream
@@ -18,7 +18,7 @@ synchronisation as the Go code does after almost every call
 cuFFT is called through torch's bindings of the same library (D2Z/Z2D, unnormalised),
 out of place instead of the Go plan's in-place buffer.  The Dormand-Prince step is composed
 from the reference's own madd / linearCombination / partialMaxAbs / divAsync kernels (the
-reference has no RK45); the thermal field's normals come from torch's CUDA
+reference has no RK45: its solvers are euler, heun, rk12, euler-backward and am01); the thermal field's normals come from torch's CUDA
 Philox generator in place of cuRAND's.  The demag kernel spectrum is computed once on the
 host by the oracle's C restatement of Kernel_Arne (setup, not timed).
 """
