@@ -727,7 +727,7 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
         }
         // ---- (B) state, neighbours, demag field
         float y[CH][W], H[3][W], lapE[W], lapL[W];
-        float ye[CH >= 5 ? 2 : 1][W], thT[W], ka[CH][W], hthv[3][W];
+        float thT[W], hthv[3][W];
         {
             if (hmode == 2) {
 #pragma unroll
@@ -765,13 +765,7 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
                 sl[c] = __ldg(ys + c * n + il);
                 sr[c] = __ldg(ys + c * n + ir);
             }
-            if (CH >= 5) {
-#pragma unroll
-                for (int c = 3; c < CH; c++) ldw<W>(yerr0 + c * n + i, ye[c - 3]);
-                ldw<W>(yth + 3 * n + i, thT);
-            }
-#pragma unroll
-            for (int c = 0; c < CH; c++) ldw<W>(kacc + c * n + i, ka[c]);
+            if (CH >= 5 && th_field) ldw<W>(yth + 3 * n + i, thT);
             // consume
 #pragma unroll
             for (int c = 0; c < 3; c++)
@@ -890,7 +884,13 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
             for (int c = 0; c < CH; c++) {
                 float v[W];
 #pragma unroll
-                for (int q = 0; q < W; q++) v[q] = A.kself_w * k[c][q] + (has_kacc ? A.kacc_w * ka[c][q] : 0.f);
+                for (int q = 0; q < W; q++) v[q] = A.kself_w * k[c][q];
+                if (has_kacc) {   // RK4's accumulated stage sum, read only where it exists
+                    float ka[W];
+                    ldw<W>(kacc + c * n + i, ka);
+#pragma unroll
+                    for (int q = 0; q < W; q++) v[q] += A.kacc_w * ka[q];
+                }
                 stw<W>(kout + c * n + i, v);
             }
         }
@@ -930,9 +930,11 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
             if (CH >= 5) {
 #pragma unroll
                 for (int c = 3; c < CH; c++) {
+                    float ye[W];
+                    ldw<W>(yerr0 + c * n + i, ye);
 #pragma unroll
                     for (int q = 0; q < W; q++) {
-                        const float sc = A.rtol * fmaxf(fabsf(ye[c - 3][q]), fabsf(y[c][q]));
+                        const float sc = A.rtol * fmaxf(fabsf(ye[q]), fabsf(y[c][q]));
                         const float ec = fabsf(acc[c][q]) * fdt;
                         const float em = sc > 0.f ? ec / sc : (ec > 0.f ? INFINITY : 0.f);
                         if (!(em == em)) bad = true;
