@@ -237,8 +237,10 @@ __global__ void k_energy(const HsbPhys P, const float* __restrict__ y, const flo
         term[4] = 0;
         if (P.llb && ms != 0.f) {
             const float Ts = (P.nch >= 5) ? y[3 * n + i] : P.T_uniform;
-            const float am = sqrtf(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
-            if (am > 1e-30f && Ts > 0.f) {
+            // |m| in FP64: near equilibrium W(|m| b) - |m| is ~1e-9, so an FP32 |m| (biased by
+            // the rounding of its sum of squares) would dominate this term
+            const double am = sqrt((double)m[0] * m[0] + (double)m[1] * m[1] + (double)m[2] * m[2]);
+            if (am > 1e-30 && Ts > 0.f) {
                 const double b = (double)P.lf_b / Ts, x = am * b;
                 double W, dW;
                 if (P.lf_langevin) {
@@ -1267,6 +1269,19 @@ HSB_EXPORT int hsb_sim_energy(hsb_sim_s* S, double* energy) {
     const double V = S->d.cellsize[0] * S->d.cellsize[1] * S->d.cellsize[2];
     const double pre = V * MU0 * S->d.msat0T0;
     *energy = pre * (r[0] + r[1] + r[2] + r[3] + r[4]);
+    return HSB_OK;
+}
+
+// The energy's terms (J): out5 = Zeeman, exchange, demag, uniaxial anisotropy, MFA
+// longitudinal field (their sum is hsb_sim_energy).
+HSB_EXPORT int hsb_sim_energy_terms(hsb_sim_s* S, double* out5) {
+    RC(plain_only(S, "hsb_sim_energy_terms"));
+    if (!S || !out5) return HSB_ERR_INVALID;
+    double r[8];
+    RC(reduce_terms(S, r));
+    const double V = S->d.cellsize[0] * S->d.cellsize[1] * S->d.cellsize[2];
+    const double pre = V * MU0 * S->d.msat0T0;
+    for (int q = 0; q < 5; q++) out5[q] = pre * r[q];
     return HSB_OK;
 }
 

@@ -115,6 +115,12 @@ class Simulation:
         _lib.check(self._lib.hsb_sim_energy(self._h, ctypes.byref(e)), "hsb_sim_energy")
         return e.value
 
+    def energy_terms(self):
+        """Zeeman, exchange, demag, anisotropy and longitudinal-field energies (J)."""
+        a = (ctypes.c_double * 5)()
+        _lib.check(self._lib.hsb_sim_energy_terms(self._h, a), "hsb_sim_energy_terms")
+        return dict(zip(("zeeman", "exchange", "demag", "anisotropy", "longitudinal"), list(a)))
+
     def average_m(self):
         a = (ctypes.c_double * 3)()
         _lib.check(self._lib.hsb_sim_average_m(self._h, a), "hsb_sim_average_m")

@@ -121,6 +121,9 @@ int hsb_sim_set_time(hsb_sim sim, double t, double dt);
  * FP64 compensated reduction on the device; and the average of m (3 values). */
 int hsb_sim_energy(hsb_sim sim, double* energy);
 int hsb_sim_average_m(hsb_sim sim, double* avg3);
+/* The energy's terms (J): Zeeman, exchange, demag, uniaxial anisotropy, MFA longitudinal
+ * field (mod_energy.go:20-66 per term; their sum is hsb_sim_energy). */
+int hsb_sim_energy_terms(hsb_sim sim, double* out5);
 
 /* Device time of one attempt by kernel family (eager launches between CUDA events on the
  * handle's stream; each profiled attempt is a real step): out[0] fused RHS+stage kernels,
