@@ -305,11 +305,71 @@ def run_ours(args):
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"], out["accuracy"] = cpu_baseline(kw, st0)
+        if world == 1 and not args.no_configs:
+            out["other_configs"] = other_configs()
         if world == 1 and not args.no_serving:
             out["serving"] = serving(args)
         print(json.dumps(out))
     if pg is not None:
         pg.destroy_process_group()
+
+
+def other_configs():
+    """Device throughput of the other single-simulation configurations (synthetic states):
+    config 2 (LLB at 300 K, 256x256x8 of 2 nm, FePt-like, Ku 7e6 along z, lambda 0.1,
+    thermal field, DP45 rtol 1e-5) and config 5 (plain LLG, 1024x1024x32 of 2 nm, alpha 0.5,
+    RK4 20 fs; demag padded to 2048x2048x64 on the multi-pass FFT path)."""
+    import ctypes
+    import torch
+    from hotspin_b200 import _lib
+    from hotspin_b200.sim import Simulation
+    lib = _lib.load()
+    out = {}
+    cases = {
+        "c2_llb_256x256x8_dp45": (dict(size=(8, 256, 256), cellsize=(2e-9,) * 3, msat0T0=1.1e6,
+                                        lex=math.sqrt(2 * 1e-11 / (MU0 * 1.1e6 ** 2)), gamma_ll=2.211e5,
+                                        alpha=(0.1,) * 3, ku=7e6, anis_u=(1.0, 0.0, 0.0), demag=True, llb=True,
+                                        tc=700.0, spin_j=0.5, n_spins=1.1e6 / (2 * MUB * 0.5), temperature=300.0,
+                                        thermal=True, seed=2, solver="dp45", dt=1e-16, rtol=1e-5, mindt=1e-20,
+                                        maxdt=1e-12), 100),
+        "c5_llg_1024x1024x32_rk4": (dict(size=(32, 1024, 1024), cellsize=(2e-9,) * 3, msat0T0=8e5,
+                                          lex=math.sqrt(2 * 1.3e-11 / (MU0 * 8e5 ** 2)),
+                                          gamma_ll=2.211e5 / (1 + 0.25), alpha=(0.5,) * 3, demag=True,
+                                          normalize=True, solver="rk4", dt=20e-15), 20),
+    }
+    for name, (kw, nsteps) in cases.items():
+        size = kw["size"]
+        rng = np.random.default_rng(5)
+        if kw.get("llb"):
+            me = ctypes.c_double()
+            _lib.check(lib.hsb_mfa_equilibrium(300.0, kw["tc"], 0.5, ctypes.byref(me)), "m_e")
+            th = np.deg2rad(5.0) * rng.random(size)
+            ph = 2 * np.pi * rng.random(size)
+            m = me.value * np.stack([np.cos(th), np.sin(th) * np.sin(ph), np.sin(th) * np.cos(ph)])
+        else:
+            m = rng.normal(size=(3,) + size)
+            m /= np.sqrt((m * m).sum(0))
+        with Simulation(**kw) as sim:
+            sim.set("m", m)
+            sim.step(3)
+            stream = torch.cuda.ExternalStream(sim._lib.hsb_sim_stream(sim._h))
+            s0 = sim.status()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.step(nsteps)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            s1 = sim.status()
+            prof = (ctypes.c_double * 7)()
+            _lib.check(lib.hsb_sim_profile(sim._h, 2, prof), "profile")
+        n = int(np.prod(size))
+        out[name] = {"value": round(n * nsteps / (ms / 1e3) / 1e6, 1), "unit": UNIT, "cells": n,
+                     "ms_per_step": round(ms / nsteps, 4), "steps": nsteps,
+                     "attempts": int(s1["attempts"] - s0["attempts"]),
+                     "attempt_ms_by_family": {"stage": round(prof[0], 4), "xfwd": round(prof[1], 4),
+                                              "yz": round(prof[2], 4), "xinv": round(prof[3], 4)}}
+    return out
 
 
 def serving(args):
@@ -365,6 +425,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched-serving comparison")
+    ap.add_argument("--no-configs", action="store_true", help="skip the config 2 / config 5 throughput lines")
     ap.add_argument("--serving-requests", type=int, default=256)
     ap.add_argument("--serving-tend", type=float, default=50e-12)
     args = ap.parse_args()

@@ -453,9 +453,13 @@ __global__ void __launch_bounds__(256, 3) k_xfwd4(const float* __restrict__ in0,
     for (int j = 0; j < A; j++) slot[lane + B * j] = v[j];
     if (lane == 0) slot[M] = xm;
     __syncthreads();
-    for (int e = tid; e < C2 * TY; e += nthr) {
-        const int rr = e % TY, kx = e / TY;
-        if (rr < ny) out[((long)p * C2 + kx) * ldo + y0 + rr] = sm[rr * SS + kx];
+    // transposed store: TY (a power of two, nthr = TY * B) consecutive rows per kx, so a
+    // thread keeps its row and steps kx by B
+    const int rr = tid & (TY - 1);
+    if (rr < ny) {
+        float2* o = out + (long)p * C2 * ldo + y0 + rr;
+        const float2* srow = sm + rr * SS;
+        for (int kx = tid >> (__ffs(TY) - 1); kx < C2; kx += B) o[(long)kx * ldo] = srow[kx];
     }
 }
 
@@ -485,13 +489,24 @@ __global__ void __launch_bounds__(256, 3) k_xinv4(const float2* __restrict__ in,
     const int ny = min(TY, N1 - y0);
     const int comp = p / planes_per_comp;
     const int a0 = p - comp * planes_per_comp;
-    batched_fill<8, float2>(
-        C2 * TY, tid, nthr,
-        [&](int e) {
-            const int rr = e % TY, kx = e / TY;
-            return rr < ny ? in[((long)p * C2 + kx) * ldi + y0 + rr] : make_float2(0.f, 0.f);
-        },
-        [&](int e, float2 v) { sm[(e % TY) * SS + e / TY] = v; });
+    {
+        // transposed load: TY (a power of two, nthr = TY * B) consecutive rows per kx; a
+        // thread keeps its row and steps kx by B, eight loads in flight before the stores
+        const int rr = tid & (TY - 1);
+        const float2* src = in + (long)p * C2 * ldi + y0 + rr;
+        float2* srow = sm + rr * SS;
+        for (int k0 = tid >> (__ffs(TY) - 1); k0 < C2; k0 += 8 * B) {
+            float2 t[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int kx = k0 + u * B;
+                t[u] = (kx < C2 && rr < ny) ? src[(long)kx * ldi] : make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (k0 + u * B < C2) srow[k0 + u * B] = t[u];
+        }
+    }
     __syncthreads();
     float2* slot = sm + r * SS;
     const int ts = twL / L2;
@@ -616,6 +631,229 @@ __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restric
     }
 }
 
+// ------------------------------------------------------------------------------ multi-pass, four-step
+// Register four-step kernels for the three-kernel y / z path (L0 > 16).  Same layouts as the
+// generic k_fft_cols / k_fft_z: X1[col][a1 < N1], X2[col][k1 < L1] with col = (c * N0 + a0) * C2
+// + kx.  Every lane of a block runs the transforms (fft4 synchronises whole warps); lanes
+// past the last column only skip their loads and stores.
+
+// Forward y transform of columns of `nin` values (zero-padded to L): one column per B lanes.
+// PR: nin <= L/2 (open boundary), the upper half of the input is known zero.
+template <int L, bool PR>
+__global__ void __launch_bounds__(256) k_ycolf4(const float2* __restrict__ in, int nin, float2* __restrict__ out,
+                                              long ncol, const float2* __restrict__ tw4,
+                                              const int* __restrict__ active) {
+    if (active && !*active) return;
+    constexpr int A = Split<L>::A, B = Split<L>::B, SS = Slot<L>::S;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x;
+    const int q = tid / B, lane = tid - q * B;
+    const long col = (long)blockIdx.x * (blockDim.x / B) + q;
+    const bool ok = col < ncol;
+    float2* slot = reinterpret_cast<float2*>(smem_raw) + q * SS;
+    const float2* src = in + (ok ? col : 0) * nin;
+    float2 v[A];
+#pragma unroll
+    for (int n1 = 0; n1 < A; n1++) {
+        const int n = B * n1 + lane;
+        v[n1] = (ok && !(PR && n1 >= A / 2) && n < nin) ? __ldg(src + n) : make_float2(0.f, 0.f);
+    }
+    fft4<L, -1, PR, false>(v, slot, lane, tw4);
+    if (ok) {
+        float2* dst = out + col * L;
+#pragma unroll
+        for (int j = 0; j < A; j++) dst[fft4_out_index<L>(lane, j)] = v[j];
+    }
+}
+
+// Inverse y transform of columns of L values, keeping the first `nout`.  PR: nout <= L/2.
+template <int L, bool PR>
+__global__ void __launch_bounds__(256) k_ycoli4(const float2* __restrict__ in, float2* __restrict__ out, int nout,
+                                              long ncol, const float2* __restrict__ tw4,
+                                              const int* __restrict__ active) {
+    if (active && !*active) return;
+    constexpr int A = Split<L>::A, B = Split<L>::B, SS = Slot<L>::S;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x;
+    const int q = tid / B, lane = tid - q * B;
+    const long col = (long)blockIdx.x * (blockDim.x / B) + q;
+    const bool ok = col < ncol;
+    float2* slot = reinterpret_cast<float2*>(smem_raw) + q * SS;
+    const float2* src = in + (ok ? col : 0) * L;
+    float2 v[A];
+#pragma unroll
+    for (int n1 = 0; n1 < A; n1++) v[n1] = ok ? __ldg(src + B * n1 + lane) : make_float2(0.f, 0.f);
+    fft4<L, +1, false, PR>(v, slot, lane, tw4);
+    if (ok) {
+        float2* dst = out + col * nout;
+#pragma unroll
+        for (int j = 0; j < A; j++) {
+            const int n = fft4_out_index<L>(lane, j);
+            if (n < nout) dst[n] = v[j];
+        }
+    }
+}
+
+// L = 2048 with nin <= 1024 (open boundary) as two 1024-point transforms, one warp per
+// column: X[2k] = FFT_1024(x)[k] and X[2k+1] = FFT_1024(x[n] W_2048^n)[k] (the zero upper
+// half removes the second radix-2 input).  tw: the plan's table exp(-2 pi i j / twL).
+__global__ void __launch_bounds__(128, 4) k_ycolf4_2k(const float2* __restrict__ in, int nin, float2* __restrict__ out,
+                                                 long ncol, const float2* __restrict__ tw4, const float2* __restrict__ tw,
+                                                 int twL, const int* __restrict__ active) {
+    if (active && !*active) return;
+    constexpr int L = 1024, A = Split<L>::A, B = Split<L>::B, SS = Slot<L>::S;
+    static_assert(B == 32, "one warp per column");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x;
+    const int q = tid >> 5, lane = tid & 31;
+    const long col = (long)blockIdx.x * (blockDim.x >> 5) + q;
+    const bool ok = col < ncol;
+    float2* slot = reinterpret_cast<float2*>(smem_raw) + q * SS;
+    const float2* src = in + (ok ? col : 0) * nin;
+    float2* dst = out + (ok ? col : 0) * (2 * L);
+    const int ts = twL / (2 * L);
+    {
+        float2 v[A];
+#pragma unroll
+        for (int n1 = 0; n1 < A; n1++) {
+            const int n = B * n1 + lane;
+            v[n1] = (ok && n < nin) ? __ldg(src + n) : make_float2(0.f, 0.f);
+        }
+        fft4<L, -1, false, false>(v, slot, lane, tw4);
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < A; j++) dst[2 * fft4_out_index<L>(lane, j)] = v[j];
+        }
+    }
+    {
+        float2 v[A];
+#pragma unroll
+        for (int n1 = 0; n1 < A; n1++) {
+            const int n = B * n1 + lane;
+            const float2 x = (ok && n < nin) ? __ldg(src + n) : make_float2(0.f, 0.f);
+            const float2 w = __ldg(&tw[n * ts]);
+            v[n1] = make_float2(x.x * w.x - x.y * w.y, x.x * w.y + x.y * w.x);
+        }
+        fft4<L, -1, false, false>(v, slot, lane, tw4);
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < A; j++) dst[2 * fft4_out_index<L>(lane, j) + 1] = v[j];
+        }
+    }
+}
+
+// Inverse of k_ycolf4_2k keeping nout <= 1024 outputs: x[n] = E[n] + W_2048^-n O[n] with E, O
+// the inverse 1024-point transforms of the even and odd spectrum entries.  E waits in a
+// per-lane shared-memory stash (1024 complex per warp after the fft4 slots) while O is formed.
+__global__ void __launch_bounds__(128, 4) k_ycoli4_2k(const float2* __restrict__ in, float2* __restrict__ out, int nout,
+                                                 long ncol, const float2* __restrict__ tw4, const float2* __restrict__ tw,
+                                                 int twL, const int* __restrict__ active) {
+    if (active && !*active) return;
+    constexpr int L = 1024, A = Split<L>::A, B = Split<L>::B, SS = Slot<L>::S;
+    static_assert(B == 32, "one warp per column");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x;
+    const int q = tid >> 5, lane = tid & 31;
+    const long col = (long)blockIdx.x * (blockDim.x >> 5) + q;
+    const bool ok = col < ncol;
+    float2* slot = reinterpret_cast<float2*>(smem_raw) + q * SS;
+    float2* stash = reinterpret_cast<float2*>(smem_raw) + (blockDim.x >> 5) * SS + q * (A * 32);
+    const float2* src = in + (ok ? col : 0) * (2 * L);
+    const int ts = twL / (2 * L);
+    float2 v[A];
+#pragma unroll
+    for (int n1 = 0; n1 < A; n1++) v[n1] = ok ? __ldg(src + 2 * (B * n1 + lane)) : make_float2(0.f, 0.f);
+    fft4<L, +1, false, false>(v, slot, lane, tw4);
+#pragma unroll
+    for (int j = 0; j < A; j++) stash[j * 32 + lane] = v[j];   // read back by the same lane
+#pragma unroll
+    for (int n1 = 0; n1 < A; n1++) v[n1] = ok ? __ldg(src + 2 * (B * n1 + lane) + 1) : make_float2(0.f, 0.f);
+    fft4<L, +1, false, false>(v, slot, lane, tw4);
+    if (ok) {
+        float2* dst = out + col * nout;
+#pragma unroll
+        for (int j = 0; j < A; j++) {
+            const int n = fft4_out_index<L>(lane, j);
+            if (n < nout) {
+                const float2 w = __ldg(&tw[n * ts]);   // conj(w) = W_2048^-n for the inverse
+                const float2 o = v[j], e = stash[j * 32 + lane];
+                dst[n] = make_float2(e.x + w.x * o.x + w.y * o.y, e.y + w.x * o.y - w.y * o.x);
+            }
+        }
+    }
+}
+
+// z transform + symmetric tensor multiply + inverse z for one (kx, k1) per B lanes, all three
+// components in registers (3 x A complex), so the multiply needs no exchange.  Lane l of a
+// warp: sequence l % G (consecutive k1), member l / G (G = 32 / B sequences per warp).
+// kern: [kx][f1][f0][6].  PR: the z axis is zero-padded (N0 = LZ / 2).
+template <int LZ, bool PR>
+__global__ void __launch_bounds__(256) k_zconv4(float2* __restrict__ X2, int N0, int C2, int L1,
+                                              const float* __restrict__ kern, const float2* __restrict__ tw4,
+                                              const int* __restrict__ active) {
+    if (active && !*active) return;
+    constexpr int A = Split<LZ>::A, B = Split<LZ>::B, SS = Slot<LZ>::S, G = 32 / B;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x;
+    const int l = tid & 31, w = tid >> 5;
+    const int q = l % G, lane = l / G;
+    const int kx = blockIdx.y;
+    const int k1 = blockIdx.x * (blockDim.x / B) + w * G + q;
+    const bool ok = k1 < L1;
+    float2* slot = reinterpret_cast<float2*>(smem_raw) + (w * G + q) * SS;
+    const long pst = (long)C2 * L1;   // between a0 rows
+    const long cst = (long)N0 * pst;  // between components
+    float2* base = X2 + (long)kx * L1 + (ok ? k1 : 0);
+    float2 v[3][A];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int n1 = 0; n1 < A; n1++) {
+            const int a0 = B * n1 + lane;
+            v[c][n1] = (ok && !(PR && n1 >= A / 2) && a0 < N0) ? base[c * cst + a0 * pst] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+    for (int c = 0; c < 3; c++) fft4<LZ, -1, PR, false>(v[c], slot, lane, tw4);
+    const int h0 = LZ / 2, h1 = L1 / 2;
+    const int k1c = ok ? k1 : 0;
+    const int f1 = k1c > h1 ? L1 - k1c : k1c;
+    const float s1 = k1c > h1 ? -1.f : 1.f;
+    const float* Kb = kern + ((long)kx * (h1 + 1) + f1) * (h0 + 1) * 6;
+#pragma unroll
+    for (int j = 0; j < A; j++) {
+        const int k0 = fft4_out_index<LZ>(lane, j);
+        const int f0 = k0 > h0 ? LZ - k0 : k0;
+        const float s0 = k0 > h0 ? -1.f : 1.f;
+        const float* K = Kb + f0 * 6;
+        const float kxx = __ldg(K + KXX), kyy = __ldg(K + KYY), kzz = __ldg(K + KZZ);
+        const float kyz = s1 * __ldg(K + KYZ), kxz = s0 * __ldg(K + KXZ), kxy = s0 * s1 * __ldg(K + KXY);
+        const float2 m0 = v[0][j], m1 = v[1][j], m2 = v[2][j];
+        v[0][j] = make_float2(kxx * m0.x + kxy * m1.x + kxz * m2.x, kxx * m0.y + kxy * m1.y + kxz * m2.y);
+        v[1][j] = make_float2(kxy * m0.x + kyy * m1.x + kyz * m2.x, kxy * m0.y + kyy * m1.y + kyz * m2.y);
+        v[2][j] = make_float2(kxz * m0.x + kyz * m1.x + kzz * m2.x, kxz * m0.y + kyz * m1.y + kzz * m2.y);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        // back to the natural input distribution (lane n2 holds entries B n1 + n2)
+#pragma unroll
+        for (int j = 0; j < A; j++) slot[fft4_out_index<LZ>(lane, j)] = v[c][j];
+        __syncwarp();
+#pragma unroll
+        for (int n1 = 0; n1 < A; n1++) v[c][n1] = slot[B * n1 + lane];
+        __syncwarp();
+        fft4<LZ, +1, false, PR>(v[c], slot, lane, tw4);
+    }
+    if (ok) {
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int j = 0; j < A; j++) {
+                const int a0 = fft4_out_index<LZ>(lane, j);
+                if (a0 < N0) base[c * cst + a0 * pst] = v[c][j];
+            }
+    }
+}
+
 // Dispatch tables for the fast kernels.
 typedef void (*xfwd4_fn)(const float*, const float*, const int*, int, const float*, long, int, int, int, int,
                          float2*, const float2*, int, const float2*, int, const int*, const SlotStrides);
@@ -650,6 +888,35 @@ static yz4_fn yz4_for_z(int LZ) {
     }
     return nullptr;
 }
+typedef void (*ycf4_fn)(const float2*, int, float2*, long, const float2*, const int*);
+typedef void (*yci4_fn)(const float2*, float2*, int, long, const float2*, const int*);
+typedef void (*zc4_fn)(float2*, int, int, int, const float*, const float2*, const int*);
+
+static ycf4_fn ycf4_for(int L, bool pr, int* B, int* S) {
+    switch (L) {
+#define YC(l) case l: *B = Split<l>::B; *S = Slot<l>::S; return pr ? k_ycolf4<l, true> : k_ycolf4<l, false>;
+        YC(16) YC(32) YC(64) YC(128) YC(256) YC(512) YC(1024)
+#undef YC
+    }
+    return nullptr;
+}
+static yci4_fn yci4_for(int L, bool pr) {
+    switch (L) {
+#define YC(l) case l: return pr ? k_ycoli4<l, true> : k_ycoli4<l, false>;
+        YC(16) YC(32) YC(64) YC(128) YC(256) YC(512) YC(1024)
+#undef YC
+    }
+    return nullptr;
+}
+static zc4_fn zc4_for(int LZ, bool pr, int* B, int* S) {
+    switch (LZ) {
+#define ZC(l) case l: *B = Split<l>::B; *S = Slot<l>::S; return pr ? k_zconv4<l, true> : k_zconv4<l, false>;
+        ZC(32) ZC(64) ZC(128)
+#undef ZC
+    }
+    return nullptr;
+}
+
 static yz4_fn yz4_for(int L1, int LZ, bool pr, int* B, int* S) {
     switch (L1) {
 #define YZ(l) case l: *B = Split<l>::B; *S = Slot<l>::S; return pr ? yz4_for_z<l, true>(LZ) : yz4_for_z<l, false>(LZ);
@@ -709,6 +976,13 @@ struct hsb_demag_plan_s {
     int x4_rows, x4_threads, x4_smem, yz4_threads, yz4_smem;
     int x4_S;           // slot stride of the x kernels
     int x4i_rows, x4i_threads, x4i_smem;  // inverse x kernel (tuned separately)
+    // four-step multi-pass kernels (L0 > 16): y columns (yc2k = the 2048-point split) and z
+    ycf4_fn ycf4;
+    yci4_fn yci4;
+    zc4_fn zc4;
+    int yc2k, yc_threads, yc_cols, yc_smem, zc_k1, zc_smem;
+    float2* tw4c;       // four-step twiddles of the y columns (length L1, or 1024 for yc2k)
+    float2* tw4z;       // and of the z transform (length L0)
 };
 
 // Largest power-of-two tile (<= cap) whose ping-pong buffers of `per_item` padded complex
@@ -1061,6 +1335,40 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
         P->TKz = pick_tile(L0, 3 * sizeof(float2), SMEM_TILE_BUDGET, 32);
         P->smem_z = 2 * 3 * P->TKz * fpad_len(L0) * (int)sizeof(float2);
         PTRY(cudaFuncSetAttribute(k_fft_z<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_z));
+        // four-step register kernels where the lengths fit; an axis is zero-padded exactly
+        // when its logic size is twice the grid's
+        const bool pry = L1 == 2 * N1, prz = L0 == 2 * N0;
+        int Bc = 0, Sc = 0;
+        P->ycf4 = ycf4_for(L1, pry, &Bc, &Sc);
+        if (P->ycf4) {
+            P->yci4 = yci4_for(L1, pry);
+            P->yc_threads = 256;
+            P->yc_cols = 256 / Bc;
+            P->yc_smem = P->yc_cols * Sc * (int)sizeof(float2);
+            rc = make_tw4(L1, Bc, P->twL, &P->tw4c);
+            if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }
+            PTRY(cudaFuncSetAttribute(P->ycf4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->yc_smem));
+            PTRY(cudaFuncSetAttribute(P->yci4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->yc_smem));
+        } else if (L1 == 2048 && pry) {
+            P->yc2k = 1;
+            P->yc_threads = 128;
+            P->yc_cols = 4;
+            // fft4 slots, then the inverse kernel's per-warp stash of 1024 complex
+            P->yc_smem = P->yc_cols * (Slot<1024>::S + 1024) * (int)sizeof(float2);
+            rc = make_tw4(1024, Split<1024>::B, P->twL, &P->tw4c);
+            if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }
+            PTRY(cudaFuncSetAttribute(k_ycolf4_2k, cudaFuncAttributeMaxDynamicSharedMemorySize, P->yc_smem));
+            PTRY(cudaFuncSetAttribute(k_ycoli4_2k, cudaFuncAttributeMaxDynamicSharedMemorySize, P->yc_smem));
+        }
+        int Bz = 0, Sz = 0;
+        P->zc4 = zc4_for(L0, prz, &Bz, &Sz);
+        if (P->zc4) {
+            P->zc_k1 = 256 / Bz;
+            P->zc_smem = P->zc_k1 * Sz * (int)sizeof(float2);
+            rc = make_tw4(L0, Bz, P->twL, &P->tw4z);
+            if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }
+            PTRY(cudaFuncSetAttribute(P->zc4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->zc_smem));
+        }
     }
     {
         // four-step kernels for the FP32 convolution when the lengths fit
@@ -1117,6 +1425,8 @@ HSB_EXPORT int hsb_demag_plan_destroy(hsb_demag_plan P) {
     cudaFree(P->kern4);
     cudaFree(P->tw4x);
     cudaFree(P->tw4y);
+    cudaFree(P->tw4c);
+    cudaFree(P->tw4z);
     cudaFree(P->X1);
     cudaFree(P->X2);
     cudaFree(P->tw);
@@ -1191,13 +1501,29 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
         }
     } else {
         const long ncol = 3L * N0 * C2;
-        k_fft_cols<float, -1><<<hsb_div_up(ncol, P->TBy), XTHREADS, P->smem_y, st>>>(
-            P->X1, N1, N1, P->X2, L1, L1, L1, ncol, P->tw, P->twL, P->TBy, active);
-        dim3 gz(hsb_div_up(L1, P->TKz), C2);
-        k_fft_z<float><<<gz, XTHREADS, P->smem_z, st>>>(P->X2, 3, N0, L0, C2, L1, P->kern, 1, P->tw, P->twL,
-                                                               P->TKz, active);
-        k_fft_cols<float, +1><<<hsb_div_up(ncol, P->TBy), XTHREADS, P->smem_y, st>>>(
-            P->X2, L1, L1, P->X1, N1, N1, L1, ncol, P->tw, P->twL, P->TBy, active);
+        const long gc = P->yc_cols ? hsb_div_up(ncol, P->yc_cols) : 0;
+        if (P->ycf4)
+            P->ycf4<<<gc, P->yc_threads, P->yc_smem, st>>>(P->X1, N1, P->X2, ncol, P->tw4c, active);
+        else if (P->yc2k)
+            k_ycolf4_2k<<<gc, P->yc_threads, P->yc_smem, st>>>(P->X1, N1, P->X2, ncol, P->tw4c, P->tw, P->twL, active);
+        else
+            k_fft_cols<float, -1><<<hsb_div_up(ncol, P->TBy), XTHREADS, P->smem_y, st>>>(
+                P->X1, N1, N1, P->X2, L1, L1, L1, ncol, P->tw, P->twL, P->TBy, active);
+        if (P->zc4) {
+            dim3 gz(hsb_div_up(L1, P->zc_k1), C2);
+            P->zc4<<<gz, 256, P->zc_smem, st>>>(P->X2, N0, C2, L1, P->kern, P->tw4z, active);
+        } else {
+            dim3 gz(hsb_div_up(L1, P->TKz), C2);
+            k_fft_z<float><<<gz, XTHREADS, P->smem_z, st>>>(P->X2, 3, N0, L0, C2, L1, P->kern, 1, P->tw, P->twL,
+                                                                   P->TKz, active);
+        }
+        if (P->yci4)
+            P->yci4<<<gc, P->yc_threads, P->yc_smem, st>>>(P->X2, P->X1, N1, ncol, P->tw4c, active);
+        else if (P->yc2k)
+            k_ycoli4_2k<<<gc, P->yc_threads, P->yc_smem, st>>>(P->X2, P->X1, N1, ncol, P->tw4c, P->tw, P->twL, active);
+        else
+            k_fft_cols<float, +1><<<hsb_div_up(ncol, P->TBy), XTHREADS, P->smem_y, st>>>(
+                P->X2, L1, L1, P->X1, N1, N1, L1, ncol, P->tw, P->twL, P->TBy, active);
     }
     if (io.ev) cudaEventRecord(io.ev[2], st);
     if (P->xinv4) {

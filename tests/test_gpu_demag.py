@@ -18,6 +18,9 @@ GEOMS = [
     ((4, 32, 64), (4e-9, 4e-9, 4e-9), (0, 0, 0)),                  # fused, L0 = 8
     ((8, 16, 32), (2e-9, 2e-9, 2e-9), (0, 0, 0)),                  # fused, L0 = 16
     ((16, 16, 16), (1e-9, 2.5e-9, 5e-9), (0, 0, 0)),               # multipass (L0 = 32)
+    ((16, 1024, 4), (2e-9, 2e-9, 2e-9), (0, 0, 0)),                # multipass, 2048-point y split
+    ((64, 8, 8), (1e-9, 2e-9, 2e-9), (0, 0, 0)),                   # multipass, z length 128
+    ((32, 8, 16), (2e-9, 3e-9, 2e-9), (1, 0, 0)),                  # multipass, periodic z (L0 = N0 = 32)
     ((4, 8, 16), (1e-9, 2e-9, 3e-9), (2, 0, 3)),                   # periodic axes
     ((1, 1, 64), (2e-9, 2e-9, 2e-9), (0, 0, 0)),                   # a single row
 ]
