@@ -430,8 +430,9 @@ __global__ void __launch_bounds__(256, 3) k_xfwd4(const float* __restrict__ in0,
 #pragma unroll
     for (int j = 0; j < A; j++) slot[fft4_out_index<M>(lane, j)] = v[j];
     __syncwarp();
-    // X[k] = E[k] + W^k O[k], k = lane + B j (and k = M on lane 0)
-    const int ts = twL / L2;
+    // X[k] = E[k] + W^k O[k], k = lane + B j (and k = M on lane 0), with
+    // W_L2^k = W_L2^lane (one table entry) x exp(-2 pi i j / 2A) (a constant per j)
+    const float2 wl = __ldg(&tw[lane * (twL / L2)]);
 #pragma unroll
     for (int j = 0; j < A; j++) {
         const int k = lane + B * j;
@@ -440,7 +441,8 @@ __global__ void __launch_bounds__(256, 3) k_xfwd4(const float* __restrict__ in0,
         const float2 zc = make_float2(zc0.x, -zc0.y);
         const float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
         const float2 od = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
-        const float2 w = __ldg(&tw[k * ts]);
+        const float cr = (float)c64cos(j * (32 / A)), ci = (float)-c64sin(j * (32 / A));
+        const float2 w = make_float2(wl.x * cr - wl.y * ci, wl.x * ci + wl.y * cr);
         v[j] = make_float2(ev.x + w.x * od.x - w.y * od.y, ev.y + w.x * od.y + w.y * od.x);
     }
     float2 xm = make_float2(0.f, 0.f);
@@ -509,7 +511,8 @@ __global__ void __launch_bounds__(256, 3) k_xinv4(const float2* __restrict__ in,
     }
     __syncthreads();
     float2* slot = sm + r * SS;
-    const int ts = twL / L2;
+    // W_L2^k = W_L2^lane x exp(-2 pi i n1 / 2A) for k = lane + B n1
+    const float2 wl = __ldg(&tw[lane * (twL / L2)]);
     float2 v[A];
 #pragma unroll
     for (int n1 = 0; n1 < A; n1++) {
@@ -520,7 +523,8 @@ __global__ void __launch_bounds__(256, 3) k_xinv4(const float2* __restrict__ in,
         const float2 xc = make_float2(xc0.x, -xc0.y);
         const float2 sA = make_float2(xk.x + xc.x, xk.y + xc.y);
         const float2 d = make_float2(xk.x - xc.x, xk.y - xc.y);
-        const float2 w0 = __ldg(&tw[k * ts]);
+        const float cr = (float)c64cos(n1 * (32 / A)), ci = (float)-c64sin(n1 * (32 / A));
+        const float2 w0 = make_float2(wl.x * cr - wl.y * ci, wl.x * ci + wl.y * cr);
         const float2 w = make_float2(w0.x, -w0.y);
         const float2 wd = make_float2(w.x * d.x - w.y * d.y, w.x * d.y + w.y * d.x);
         v[n1] = make_float2(sA.x - wd.y, sA.y + wd.x);
@@ -569,7 +573,6 @@ __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restric
     // lanes that exist in this thread's warp (the block may end with a partial warp)
     const int wbase = tid & ~31;
     const unsigned wmask = (nthr - wbase >= 32) ? 0xffffffffu : ((1u << (nthr - wbase)) - 1u);
-    (void)ncol;
     float2 v[A];
     const float2* src = X1 + ((long)col * C2 + kx) * N1;
 #pragma unroll
@@ -577,7 +580,11 @@ __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restric
         const int n = B * n1 + lane;
         v[n1] = (!(PR && n1 >= A / 2) && n < N1) ? src[n] : make_float2(0.f, 0.f);
     }
-    fft4<L1, -1, PR, false>(v, slot, lane, tw4, wmask);
+    // the block's copy of the four-step twiddle matrix (after the column loads are issued)
+    float2* tws = sm + ncol * SS;
+    for (int i = tid; i < L1; i += nthr) tws[i] = __ldg(&tw4[i]);
+    __syncthreads();
+    fft4<L1, -1, PR, false, true>(v, slot, lane, tws, wmask);
 #pragma unroll
     for (int j = 0; j < A; j++) slot[fft4_out_index<L1>(lane, j)] = v[j];
     __syncthreads();
@@ -622,7 +629,7 @@ __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restric
 #pragma unroll
     for (int n1 = 0; n1 < A; n1++) v[n1] = slot[B * n1 + lane];
     __syncwarp(wmask);
-    fft4<L1, +1, false, PR>(v, slot, lane, tw4, wmask);
+    fft4<L1, +1, false, PR, true>(v, slot, lane, tws, wmask);
     float2* dst = X1 + ((long)col * C2 + kx) * N1;
 #pragma unroll
     for (int j = 0; j < A; j++) {
@@ -696,7 +703,10 @@ __global__ void __launch_bounds__(256) k_ycoli4(const float2* __restrict__ in, f
 
 // L = 2048 with nin <= 1024 (open boundary) as two 1024-point transforms, one warp per
 // column: X[2k] = FFT_1024(x)[k] and X[2k+1] = FFT_1024(x[n] W_2048^n)[k] (the zero upper
-// half removes the second radix-2 input).  tw: the plan's table exp(-2 pi i j / twL).
+// half removes the second radix-2 input).  The column's inputs wait in a per-lane
+// shared-memory stash (1024 complex per warp after the fft4 slots) for the odd pass.
+// tw: the plan's table exp(-2 pi i j / twL).  (Measured: one warp per column at 12 warps
+// per SM beats two warps per column, one per parity, at 24.)
 __global__ void __launch_bounds__(128, 4) k_ycolf4_2k(const float2* __restrict__ in, int nin, float2* __restrict__ out,
                                                  long ncol, const float2* __restrict__ tw4, const float2* __restrict__ tw,
                                                  int twL, const int* __restrict__ active) {
@@ -711,6 +721,7 @@ __global__ void __launch_bounds__(128, 4) k_ycolf4_2k(const float2* __restrict__
     float2* slot = reinterpret_cast<float2*>(smem_raw) + q * SS;
     const float2* src = in + (ok ? col : 0) * nin;
     float2* dst = out + (ok ? col : 0) * (2 * L);
+    float2* stash = reinterpret_cast<float2*>(smem_raw) + (blockDim.x >> 5) * SS + q * (A * 32);
     const int ts = twL / (2 * L);
     {
         float2 v[A];
@@ -718,6 +729,7 @@ __global__ void __launch_bounds__(128, 4) k_ycolf4_2k(const float2* __restrict__
         for (int n1 = 0; n1 < A; n1++) {
             const int n = B * n1 + lane;
             v[n1] = (ok && n < nin) ? __ldg(src + n) : make_float2(0.f, 0.f);
+            stash[n1 * 32 + lane] = v[n1];   // the odd pass re-reads its own lane's inputs
         }
         fft4<L, -1, false, false>(v, slot, lane, tw4);
         if (ok) {
@@ -730,7 +742,7 @@ __global__ void __launch_bounds__(128, 4) k_ycolf4_2k(const float2* __restrict__
 #pragma unroll
         for (int n1 = 0; n1 < A; n1++) {
             const int n = B * n1 + lane;
-            const float2 x = (ok && n < nin) ? __ldg(src + n) : make_float2(0.f, 0.f);
+            const float2 x = stash[n1 * 32 + lane];
             const float2 w = __ldg(&tw[n * ts]);
             v[n1] = make_float2(x.x * w.x - x.y * w.y, x.x * w.y + x.y * w.x);
         }
@@ -786,20 +798,37 @@ __global__ void __launch_bounds__(128, 4) k_ycoli4_2k(const float2* __restrict__
 // z transform + symmetric tensor multiply + inverse z for one (kx, k1) per B lanes, all three
 // components in registers (3 x A complex), so the multiply needs no exchange.  Lane l of a
 // warp: sequence l % G (consecutive k1), member l / G (G = 32 / B sequences per warp).
-// kern: [kx][f1][f0][6].  PR: the z axis is zero-padded (N0 = LZ / 2).
+// 256 threads = K1B consecutive k1 per block.  kern4: [kx][f0][6][f1]; the block's
+// f1 range (always K1B consecutive values) is staged in shared memory with coalesced loads.
+// PR: the z axis is zero-padded (N0 = LZ / 2).
+// Slot stride ZS: a half-warp holds G sequences (G = 32 / B), so their slots must start on
+// distinct 64-bit bank pairs: ZS = 16 / G (mod 16), and ZS holds the B x (A + 1) transpose and
+// the L natural-order entries.
+template <int LZ> struct ZConv {
+    static constexpr int A = Split<LZ>::A, B = Split<LZ>::B, G = 32 / B, K1B = 256 / B, KS = K1B + 1;
+    static constexpr int T = B * (A + 1) > LZ ? B * (A + 1) : LZ;
+    static constexpr int ZS = ((T - 16 / G + 15) / 16) * 16 + 16 / G;
+    static constexpr int smem = K1B * ZS * 8 + (LZ / 2 + 1) * 6 * KS * 4;
+};
 template <int LZ, bool PR>
-__global__ void __launch_bounds__(256) k_zconv4(float2* __restrict__ X2, int N0, int C2, int L1,
-                                              const float* __restrict__ kern, const float2* __restrict__ tw4,
+__global__ void __launch_bounds__(256, LZ <= 64 ? 2 : 1) k_zconv4(float2* __restrict__ X2, int N0, int C2, int L1,
+                                              const float* __restrict__ kern4, const float2* __restrict__ tw4,
                                               const int* __restrict__ active) {
     if (active && !*active) return;
-    constexpr int A = Split<LZ>::A, B = Split<LZ>::B, SS = Slot<LZ>::S, G = 32 / B;
+    constexpr int A = Split<LZ>::A, B = Split<LZ>::B, SS = ZConv<LZ>::ZS, G = 32 / B;
+    constexpr int K1B = ZConv<LZ>::K1B, KS = ZConv<LZ>::KS, h0 = LZ / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* ks = reinterpret_cast<float*>(smem_raw + K1B * SS * sizeof(float2));   // [(h0 + 1) * 6][KS]
     const int tid = threadIdx.x;
     const int l = tid & 31, w = tid >> 5;
     const int q = l % G, lane = l / G;
     const int kx = blockIdx.y;
-    const int k1 = blockIdx.x * (blockDim.x / B) + w * G + q;
+    const int k10 = blockIdx.x * K1B;
+    const int k1 = k10 + w * G + q;
     const bool ok = k1 < L1;
+    const int h1 = L1 / 2;
+    // smallest f1 = min(k1, L1 - k1) over the block's k1 < L1
+    const int flo = min(k10, L1 - (min(k10 + K1B, L1) - 1));
     float2* slot = reinterpret_cast<float2*>(smem_raw) + (w * G + q) * SS;
     const long pst = (long)C2 * L1;   // between a0 rows
     const long cst = (long)N0 * pst;  // between components
@@ -812,21 +841,29 @@ __global__ void __launch_bounds__(256) k_zconv4(float2* __restrict__ X2, int N0,
             const int a0 = B * n1 + lane;
             v[c][n1] = (ok && !(PR && n1 >= A / 2) && a0 < N0) ? base[c * cst + a0 * pst] : make_float2(0.f, 0.f);
         }
+    {
+        const float* kb = kern4 + (long)kx * (h0 + 1) * 6 * (h1 + 1);
+        for (int e = tid; e < (h0 + 1) * 6 * K1B; e += 256) {
+            const int row = e / K1B, i = e - row * K1B;
+            const int f1 = flo + i;
+            if (f1 <= h1) ks[row * KS + i] = __ldg(kb + (long)row * (h1 + 1) + f1);
+        }
+    }
 #pragma unroll
     for (int c = 0; c < 3; c++) fft4<LZ, -1, PR, false>(v[c], slot, lane, tw4);
-    const int h0 = LZ / 2, h1 = L1 / 2;
-    const int k1c = ok ? k1 : 0;
+    __syncthreads();   // the staged spectrum is complete (the slots are per sequence)
+    const int k1c = ok ? k1 : k10;
     const int f1 = k1c > h1 ? L1 - k1c : k1c;
     const float s1 = k1c > h1 ? -1.f : 1.f;
-    const float* Kb = kern + ((long)kx * (h1 + 1) + f1) * (h0 + 1) * 6;
+    const float* Kb = ks + (f1 - flo);
 #pragma unroll
     for (int j = 0; j < A; j++) {
         const int k0 = fft4_out_index<LZ>(lane, j);
         const int f0 = k0 > h0 ? LZ - k0 : k0;
         const float s0 = k0 > h0 ? -1.f : 1.f;
-        const float* K = Kb + f0 * 6;
-        const float kxx = __ldg(K + KXX), kyy = __ldg(K + KYY), kzz = __ldg(K + KZZ);
-        const float kyz = s1 * __ldg(K + KYZ), kxz = s0 * __ldg(K + KXZ), kxy = s0 * s1 * __ldg(K + KXY);
+        const float* K = Kb + f0 * 6 * KS;
+        const float kxx = K[KXX * KS], kyy = K[KYY * KS], kzz = K[KZZ * KS];
+        const float kyz = s1 * K[KYZ * KS], kxz = s0 * K[KXZ * KS], kxy = s0 * s1 * K[KXY * KS];
         const float2 m0 = v[0][j], m1 = v[1][j], m2 = v[2][j];
         v[0][j] = make_float2(kxx * m0.x + kxy * m1.x + kxz * m2.x, kxx * m0.y + kxy * m1.y + kxz * m2.y);
         v[1][j] = make_float2(kxy * m0.x + kyy * m1.x + kyz * m2.x, kxy * m0.y + kyy * m1.y + kyz * m2.y);
@@ -908,9 +945,9 @@ static yci4_fn yci4_for(int L, bool pr) {
     }
     return nullptr;
 }
-static zc4_fn zc4_for(int LZ, bool pr, int* B, int* S) {
+static zc4_fn zc4_for(int LZ, bool pr, int* K1B, int* smem) {
     switch (LZ) {
-#define ZC(l) case l: *B = Split<l>::B; *S = Slot<l>::S; return pr ? k_zconv4<l, true> : k_zconv4<l, false>;
+#define ZC(l) case l: *K1B = ZConv<l>::K1B; *smem = ZConv<l>::smem; return pr ? k_zconv4<l, true> : k_zconv4<l, false>;
         ZC(32) ZC(64) ZC(128)
 #undef ZC
     }
@@ -1353,20 +1390,18 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
             P->yc2k = 1;
             P->yc_threads = 128;
             P->yc_cols = 4;
-            // fft4 slots, then the inverse kernel's per-warp stash of 1024 complex
+            // fft4 slots, then the per-warp stash of 1024 complex
             P->yc_smem = P->yc_cols * (Slot<1024>::S + 1024) * (int)sizeof(float2);
             rc = make_tw4(1024, Split<1024>::B, P->twL, &P->tw4c);
             if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }
             PTRY(cudaFuncSetAttribute(k_ycolf4_2k, cudaFuncAttributeMaxDynamicSharedMemorySize, P->yc_smem));
             PTRY(cudaFuncSetAttribute(k_ycoli4_2k, cudaFuncAttributeMaxDynamicSharedMemorySize, P->yc_smem));
         }
-        int Bz = 0, Sz = 0;
-        P->zc4 = zc4_for(L0, prz, &Bz, &Sz);
+        P->zc4 = zc4_for(L0, prz, &P->zc_k1, &P->zc_smem);
         if (P->zc4) {
-            P->zc_k1 = 256 / Bz;
-            P->zc_smem = P->zc_k1 * Sz * (int)sizeof(float2);
-            rc = make_tw4(L0, Bz, P->twL, &P->tw4z);
+            rc = make_tw4(L0, 256 / P->zc_k1, P->twL, &P->tw4z);
             if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }
+            if (!P->kern4) PTRY(cudaMalloc(&P->kern4, sizeof(float) * kcount));
             PTRY(cudaFuncSetAttribute(P->zc4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->zc_smem));
         }
     }
@@ -1397,13 +1432,13 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
         }
         int By = 0, Sy = 0;
         yz4_fn yf = (L0 <= 16) ? yz4_for(L1, L0, pryz, &By, &Sy) : nullptr;
-        if (yf && 3 * N0 * By <= 384 && 3 * N0 * Sy * (int)sizeof(float2) <= 110 * 1024) {
+        if (yf && 3 * N0 * By <= 384 && (3 * N0 * Sy + L1) * (int)sizeof(float2) <= 110 * 1024) {
             P->yz4 = yf;
-            PTRY(cudaMalloc(&P->kern4, sizeof(float) * kcount));
+            if (!P->kern4) PTRY(cudaMalloc(&P->kern4, sizeof(float) * kcount));
             rc = make_tw4(L1, By, P->twL, &P->tw4y);
             if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }
             P->yz4_threads = 3 * N0 * By;
-            P->yz4_smem = 3 * N0 * Sy * (int)sizeof(float2);
+            P->yz4_smem = (3 * N0 * Sy + L1) * (int)sizeof(float2);   // column slots + twiddle matrix
             PTRY(cudaFuncSetAttribute(P->yz4, cudaFuncAttributeMaxDynamicSharedMemorySize, P->yz4_smem));
             PTRY(cudaFuncSetAttribute(P->yz4, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         }
@@ -1511,7 +1546,7 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
                 P->X1, N1, N1, P->X2, L1, L1, L1, ncol, P->tw, P->twL, P->TBy, active);
         if (P->zc4) {
             dim3 gz(hsb_div_up(L1, P->zc_k1), C2);
-            P->zc4<<<gz, 256, P->zc_smem, st>>>(P->X2, N0, C2, L1, P->kern, P->tw4z, active);
+            P->zc4<<<gz, 256, P->zc_smem, st>>>(P->X2, N0, C2, L1, P->kern4, P->tw4z, active);
         } else {
             dim3 gz(hsb_div_up(L1, P->TKz), C2);
             k_fft_z<float><<<gz, XTHREADS, P->smem_z, st>>>(P->X2, 3, N0, L0, C2, L1, P->kern, 1, P->tw, P->twL,

@@ -112,9 +112,10 @@ template <int L> struct Slot {
 
 // Four-step transform of one sequence (see header).  `lane` in [0, B); all B lanes of
 // the sequence, and every existing lane of the warp (`wmask`), must call it.
-// `tw4`: the A x B twiddle matrix of length L.
+// `tw4`: the A x B twiddle matrix of length L, in global memory, or in shared memory
+// when SMTW (a block-staged copy).
 // ZIN: inputs L/2..L-1 are zero; HOUT: only outputs 0..L/2-1 are wanted.
-template <int L, int DIR, bool ZIN = false, bool HOUT = false>
+template <int L, int DIR, bool ZIN = false, bool HOUT = false, bool SMTW = false>
 __device__ __forceinline__ void fft4(float2 (&v)[Split<L>::A], float2* slot, int lane,
                                      const float2* __restrict__ tw4, unsigned wmask = 0xffffffffu) {
     constexpr int A = Split<L>::A, B = Split<L>::B;
@@ -123,7 +124,7 @@ __device__ __forceinline__ void fft4(float2 (&v)[Split<L>::A], float2* slot, int
     if (B > 1) {
 #pragma unroll
         for (int k1 = 1; k1 < A; k1++) {
-            float2 w = __ldg(&tw4[k1 * B + lane]);
+            float2 w = SMTW ? tw4[k1 * B + lane] : __ldg(&tw4[k1 * B + lane]);
             if (DIR > 0) w.y = -w.y;
             const float2 a = v[k1];
             v[k1] = make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
