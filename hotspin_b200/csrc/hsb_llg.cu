@@ -70,14 +70,16 @@ __device__ __forceinline__ void mfa_w(const HsbPhys& P, float x, float& W, float
 // The longitudinal-field multiplier n kB T (W(am b) - am) / (mu0 Ms0 W'(am b) am), b = lf_b / T.
 // For J = 1/2 above the series range it uses e = expm1(-2x): tanh x = -e / (2 + e) and
 // 1 / cosh^2 x = 4 (1 + e) / (2 + e)^2, the same values as mfa_w's forms with one
-// transcendental instead of two.
+// transcendental instead of two; with d = 2 + e, (W - am) d^2 = -d (e + am d), so the
+// multiplier is -pre T d (e + am d) / (4 (1 + e) am).  Both divisions use the fast reciprocal
+// form: T > 0 is kelvin-sized, and the denominator leaves the normal range only where
+// exp(-2x) underflows (x > 43), where the field is unbounded in any arithmetic.
 __device__ __forceinline__ float mfa_mult(const HsbPhys& P, float am, float Ts) {
-    const float x = am * (P.lf_b / Ts);
+    const float x = am * __fdividef(P.lf_b, Ts);
     if (!P.lf_langevin && P.lf_lpre == 1.0f && P.lf_gpre == 2.0f && fabsf(x) >= P.lf_lim) {
         const float e = expm1f(-2.0f * x);
         const float d = 2.0f + e;
-        const float W = -e / d;
-        return P.lf_pre * Ts * (W - am) * d * d / (4.0f * (1.0f + e) * am);
+        return __fdividef(-P.lf_pre * Ts * d * (e + am * d), 4.0f * (1.0f + e) * am);
     }
     float W, dW;
     mfa_w(P, x, W, dW);
@@ -696,6 +698,7 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
     }
     float emax = 0.f;
     bool bad = false;
+    const float dt_rtol = A.err ? fdt / A.rtol : 0.f;
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < ngroups; g += (long)gridDim.x * blockDim.x) {
         const long i = g * W;
         const unsigned iu = (unsigned)i;
@@ -868,10 +871,11 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
                     }
                     Qe += q2;
                 }
+                // heat capacities are ~1e4..1e7 J/(m^3 K): the fast reciprocal division applies
                 const float Ce = P.gamma_e * Te;
-                k[3 % CH][q] = (Ce == 0.f) ? 0.f : Qe / Ce;
+                k[3 % CH][q] = (Ce == 0.f) ? 0.f : __fdividef(Qe, Ce);
                 const float Ql = lapL[q] + P.g_ep * (Te - Tl);
-                k[4 % CH][q] = (P.c_l == 0.f) ? 0.f : Ql / P.c_l;
+                k[4 % CH][q] = (P.c_l == 0.f) ? 0.f : __fdividef(Ql, P.c_l);
             }
         }
         // ---- stores and the error norm
@@ -923,7 +927,7 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
                 for (int q = 0; q < W; q++) acc[c][q] += A.ceself * k[c][q];
 #pragma unroll
             for (int q = 0; q < W; q++) {
-                float em = fmaxf(fabsf(acc[0][q]), fmaxf(fabsf(acc[1][q]), fabsf(acc[2][q]))) * fdt / A.rtol;
+                float em = fmaxf(fabsf(acc[0][q]), fmaxf(fabsf(acc[1][q]), fabsf(acc[2][q]))) * dt_rtol;
                 if (!(em == em)) bad = true;
                 emax = fmaxf(emax, em);
             }
@@ -936,7 +940,7 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
                     for (int q = 0; q < W; q++) {
                         const float sc = A.rtol * fmaxf(fabsf(ye[q]), fabsf(y[c][q]));
                         const float ec = fabsf(acc[c][q]) * fdt;
-                        const float em = sc > 0.f ? ec / sc : (ec > 0.f ? INFINITY : 0.f);
+                        const float em = sc > 0.f ? __fdividef(ec, sc) : (ec > 0.f ? INFINITY : 0.f);
                         if (!(em == em)) bad = true;
                         emax = fmaxf(emax, em);
                     }
