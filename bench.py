@@ -82,6 +82,38 @@ def algorithmic_bytes(kw, fused=True):
             "stage_attempt": stage, "stage_launches": 7, "demag_per_attempt": 6}
 
 
+def family_roofline(kw, solver, prof_ms):
+    """Algorithmic bytes and HBM fraction of each kernel family for one attempt of `solver`
+    (`prof_ms`: the attempt's device time per family, summed over its launches)."""
+    n0, n1, n2 = kw["size"]
+    ncell = n0 * n1 * n2
+    L0, L1, L2 = [2 * s if s > 1 else s for s in kw["size"]]
+    c2 = L2 // 2 + 1
+    spec = 3 * n0 * c2 * n1 * 8
+    x2 = 3 * n0 * c2 * L1 * 8                     # multi-pass y-transformed spectrum
+    kern = c2 * (L1 // 2 + 1) * (L0 // 2 + 1) * 6 * 4
+    nch = 5 if kw.get("ttm") else 3
+    fused = L0 <= 16
+    yz = 2 * spec + kern if fused else 2 * spec + 4 * x2 + kern
+    if solver == "rk4":
+        ndemag = 4
+        # s1: y0, H_d, write k-sum, y2; s2, s3: y_s, H_d, y0, k-sum, write k-sum, y_(s+1);
+        # s4: y4, H_d, y0, k-sum, write y_new
+        stage = ncell * (nch * 4 * (3 + 5 + 5 + 4) + 4 * 12)
+    else:
+        ndemag = 6
+        stage = algorithmic_bytes(kw)["stage_attempt"]
+    peak, _ = peaks()
+    byt = {"stage": stage, "xfwd": ndemag * (ncell * 12 + spec), "yz": ndemag * yz,
+           "xinv": ndemag * (spec + ncell * 12)}
+    out = {}
+    for k, b in byt.items():
+        gbs = b / (prof_ms[k] / 1e3) / 1e9
+        out[k] = {"algorithmic_bytes_per_attempt": int(b), "ms_per_attempt": round(prof_ms[k], 4),
+                  "achieved_gbs": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 3)}
+    return out
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -364,11 +396,11 @@ def other_configs():
             prof = (ctypes.c_double * 7)()
             _lib.check(lib.hsb_sim_profile(sim._h, 2, prof), "profile")
         n = int(np.prod(size))
+        fam = {"stage": prof[0], "xfwd": prof[1], "yz": prof[2], "xinv": prof[3]}
         out[name] = {"value": round(n * nsteps / (ms / 1e3) / 1e6, 1), "unit": UNIT, "cells": n,
                      "ms_per_step": round(ms / nsteps, 4), "steps": nsteps,
                      "attempts": int(s1["attempts"] - s0["attempts"]),
-                     "attempt_ms_by_family": {"stage": round(prof[0], 4), "xfwd": round(prof[1], 4),
-                                              "yz": round(prof[2], 4), "xinv": round(prof[3], 4)}}
+                     "kernel_roofline": family_roofline(kw, kw["solver"], fam)}
     return out
 
 
