@@ -34,7 +34,7 @@ MUB = 9.27400968202020202e-24
 # DRAM bytes (read + write) per launch of each kernel family on this workload, from one ncu
 # capture each (dram__bytes_read.sum + dram__bytes_write.sum; stage: the 7 launches of one
 # DP45 attempt averaged; profiles/stage_kernel_512x512x4.md, profiles/demag_fft_kernels_512x512x4.md).
-TRAFFIC_PER_LAUNCH = {"stage": 133_478_000, "yz": 56_891_000, "xfwd": 12_633_000, "xinv": 25_285_000}
+TRAFFIC_PER_LAUNCH = {"stage": 133_196_000, "yz": 56_891_000, "xfwd": 12_633_000, "xinv": 25_285_000}
 
 
 def workload():
