@@ -64,7 +64,6 @@ _SIGS = {
     "hsb_sim_launches_per_attempt": (c_int, [c_vp, c_ip]),
     "hsb_average_m_noalloc": (c_int, [c_vp, c_i64, c_vp, c_vp]),
     "hsb_set_stage_variant": (c_int, [c_int]),
-    "hsb_set_pdl": (c_int, [c_int]),
     "hsb_stage_variant_of": (c_int, [c_vp]),
     "hsb_batch_footprint": (c_int, [ctypes.POINTER(SimDesc), c_i32, ctypes.POINTER(c_i64)]),
     "hsb_batch_create": (c_int, [ctypes.POINTER(SimDesc), c_i32, ctypes.POINTER(c_vp)]),

@@ -43,35 +43,6 @@ static inline int hsb_grid_1d(long n, int threads, int blocks_per_sm = 8) {
     return (int)(need < cap ? need : cap);
 }
 
-// ------------------------------------------------------------------ programmatic dependent launch
-// Kernels on the step path begin with hsb_pdl_enter(): it waits until the preceding kernel in
-// the stream has completed and its writes are visible (a no-op when this launch was not
-// programmatic), then lets the next kernel start launching, so that its blocks are resident
-// and waiting when this grid finishes instead of being launched after it.  Every access to
-// global memory comes after the wait.  hsb_launch sets the programmatic-serialization
-// attribute while hsb_pdl_enabled() (hsb_set_pdl; off by default: measured slower in the
-// step graphs).
-__device__ __forceinline__ void hsb_pdl_enter() {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-int hsb_pdl_enabled();
-template <typename... KArgs, typename... Args>
-static inline cudaError_t hsb_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                                     Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = hsb_pdl_enabled() ? 1 : 0;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, args...);
-}
-
 // ------------------------------------------------------------------ device helpers
 __device__ __forceinline__ float warp_sum_f(float v) {
 #pragma unroll

@@ -375,7 +375,6 @@ __global__ void __launch_bounds__(256, 3) k_xfwd4(const float* __restrict__ in0,
                                                float2* __restrict__ out, const float2* __restrict__ tw, int twL,
                                                const float2* __restrict__ tw4, int TY,
                                                const int* __restrict__ active, const SlotStrides ss) {
-    hsb_pdl_enter();
     const int sl = blockIdx.z;
     if (active && !active[sl * ss.sel]) return;
     in0 += sl * ss.in;
@@ -475,7 +474,6 @@ __global__ void __launch_bounds__(256, 3) k_xinv4(const float2* __restrict__ in,
                                                float scale, const float2* __restrict__ tw, int twL,
                                                const float2* __restrict__ tw4, int TY,
                                                const int* __restrict__ active, const SlotStrides ss) {
-    hsb_pdl_enter();
     const int sl = blockIdx.z;
     if (active && !active[sl * ss.sel]) return;
     in += sl * ss.x1;
@@ -560,7 +558,6 @@ template <int L1, int LZ, bool PR>
 __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restrict__ X1, int N0, int N1, int C2,
                                              const float* __restrict__ kern4, const float2* __restrict__ tw4,
                                              const int* __restrict__ active, const SlotStrides ss) {
-    hsb_pdl_enter();
     const int sl = blockIdx.z;
     if (active && !active[sl * ss.sel]) return;
     X1 += sl * ss.x1;
@@ -653,7 +650,6 @@ template <int L, bool PR>
 __global__ void __launch_bounds__(256) k_ycolf4(const float2* __restrict__ in, int nin, float2* __restrict__ out,
                                               long ncol, const float2* __restrict__ tw4,
                                               const int* __restrict__ active) {
-    hsb_pdl_enter();
     if (active && !*active) return;
     constexpr int A = Split<L>::A, B = Split<L>::B, SS = Slot<L>::S;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -682,7 +678,6 @@ template <int L, bool PR>
 __global__ void __launch_bounds__(256) k_ycoli4(const float2* __restrict__ in, float2* __restrict__ out, int nout,
                                               long ncol, const float2* __restrict__ tw4,
                                               const int* __restrict__ active) {
-    hsb_pdl_enter();
     if (active && !*active) return;
     constexpr int A = Split<L>::A, B = Split<L>::B, SS = Slot<L>::S;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -715,7 +710,6 @@ __global__ void __launch_bounds__(256) k_ycoli4(const float2* __restrict__ in, f
 __global__ void __launch_bounds__(128, 4) k_ycolf4_2k(const float2* __restrict__ in, int nin, float2* __restrict__ out,
                                                  long ncol, const float2* __restrict__ tw4, const float2* __restrict__ tw,
                                                  int twL, const int* __restrict__ active) {
-    hsb_pdl_enter();
     if (active && !*active) return;
     constexpr int L = 1024, A = Split<L>::A, B = Split<L>::B, SS = Slot<L>::S;
     static_assert(B == 32, "one warp per column");
@@ -766,7 +760,6 @@ __global__ void __launch_bounds__(128, 4) k_ycolf4_2k(const float2* __restrict__
 __global__ void __launch_bounds__(128, 4) k_ycoli4_2k(const float2* __restrict__ in, float2* __restrict__ out, int nout,
                                                  long ncol, const float2* __restrict__ tw4, const float2* __restrict__ tw,
                                                  int twL, const int* __restrict__ active) {
-    hsb_pdl_enter();
     if (active && !*active) return;
     constexpr int L = 1024, A = Split<L>::A, B = Split<L>::B, SS = Slot<L>::S;
     static_assert(B == 32, "one warp per column");
@@ -821,7 +814,6 @@ template <int LZ, bool PR>
 __global__ void __launch_bounds__(256, LZ <= 64 ? 2 : 1) k_zconv4(float2* __restrict__ X2, int N0, int C2, int L1,
                                               const float* __restrict__ kern4, const float2* __restrict__ tw4,
                                               const int* __restrict__ active) {
-    hsb_pdl_enter();
     if (active && !*active) return;
     constexpr int A = Split<LZ>::A, B = Split<LZ>::B, SS = ZConv<LZ>::ZS, G = 32 / B;
     constexpr int K1B = ZConv<LZ>::K1B, KS = ZConv<LZ>::KS, h0 = LZ / 2;
@@ -1258,10 +1250,10 @@ static int tune_x(hsb_demag_plan_s* P, cudaStream_t st) {
                 for (int rep = 0; rep < 4; rep++) {
                     cudaEventRecord(e0, st);
                     if (which == 0)
-                        hsb_launch(P->xfwd4, g, th, smem, st, m, m, nullptr, 0, nullptr, ncell, N0, N1, N2, N1, P->X1, P->tw,
+                        P->xfwd4<<<g, th, smem, st>>>(m, m, nullptr, 0, nullptr, ncell, N0, N1, N2, N1, P->X1, P->tw,
                                                       P->twL, P->tw4x, rows, nullptr, ss);
                     else
-                        hsb_launch(P->xinv4, g, th, smem, st, P->X1, N1, N0, N1, N2, H, H, nullptr, 0, ncell, 1.0f, P->tw,
+                        P->xinv4<<<g, th, smem, st>>>(P->X1, N1, N0, N1, N2, H, H, nullptr, 0, ncell, 1.0f, P->tw,
                                                       P->twL, P->tw4x, rows, nullptr, ss);
                     cudaEventRecord(e1, st);
                     if (cudaEventSynchronize(e1) != cudaSuccess) {
@@ -1525,7 +1517,7 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     if (io.ev) cudaEventRecord(io.ev[0], st);
     if (P->xfwd4) {
         dim3 gx(hsb_div_up(N1, P->x4_rows), 3 * N0, nz);
-        hsb_launch(P->xfwd4, gx, P->x4_threads, P->x4_smem, st, io.m[0], io.m[1], io.msel, io.minv, mask, ncell, N0, N1, N2,
+        P->xfwd4<<<gx, P->x4_threads, P->x4_smem, st>>>(io.m[0], io.m[1], io.msel, io.minv, mask, ncell, N0, N1, N2,
                                                         N1, X1, P->tw, P->twL, P->tw4x, P->x4_rows, active, ss);
     } else {
         dim3 gx(hsb_div_up(N1, P->TYx), 3 * N0);
@@ -1535,7 +1527,7 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     if (io.ev) cudaEventRecord(io.ev[1], st);
     if (P->yz4) {
         dim3 gyz(C2, 1, nz);
-        hsb_launch(P->yz4, gyz, P->yz4_threads, P->yz4_smem, st, X1, N0, N1, C2, kern, P->tw4y, active, ss);
+        P->yz4<<<gyz, P->yz4_threads, P->yz4_smem, st>>>(X1, N0, N1, C2, kern, P->tw4y, active, ss);
     } else if (P->fused) {
         switch (P->lz) {
 #define RUNYZ(LZ) case LZ: k_fft_yz_conv<LZ><<<C2, yz_threads<LZ>::value, P->smem_yz, st>>>(P->X1, N0, N1, L1, C2, P->kern, P->tw, P->twL, active); break;
@@ -1546,24 +1538,24 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
         const long ncol = 3L * N0 * C2;
         const long gc = P->yc_cols ? hsb_div_up(ncol, P->yc_cols) : 0;
         if (P->ycf4)
-            hsb_launch(P->ycf4, gc, P->yc_threads, P->yc_smem, st, P->X1, N1, P->X2, ncol, P->tw4c, active);
+            P->ycf4<<<gc, P->yc_threads, P->yc_smem, st>>>(P->X1, N1, P->X2, ncol, P->tw4c, active);
         else if (P->yc2k)
-            hsb_launch(k_ycolf4_2k, gc, P->yc_threads, P->yc_smem, st, P->X1, N1, P->X2, ncol, P->tw4c, P->tw, P->twL, active);
+            k_ycolf4_2k<<<gc, P->yc_threads, P->yc_smem, st>>>(P->X1, N1, P->X2, ncol, P->tw4c, P->tw, P->twL, active);
         else
             k_fft_cols<float, -1><<<hsb_div_up(ncol, P->TBy), XTHREADS, P->smem_y, st>>>(
                 P->X1, N1, N1, P->X2, L1, L1, L1, ncol, P->tw, P->twL, P->TBy, active);
         if (P->zc4) {
             dim3 gz(hsb_div_up(L1, P->zc_k1), C2);
-            hsb_launch(P->zc4, gz, 256, P->zc_smem, st, P->X2, N0, C2, L1, P->kern4, P->tw4z, active);
+            P->zc4<<<gz, 256, P->zc_smem, st>>>(P->X2, N0, C2, L1, P->kern4, P->tw4z, active);
         } else {
             dim3 gz(hsb_div_up(L1, P->TKz), C2);
             k_fft_z<float><<<gz, XTHREADS, P->smem_z, st>>>(P->X2, 3, N0, L0, C2, L1, P->kern, 1, P->tw, P->twL,
                                                                    P->TKz, active);
         }
         if (P->yci4)
-            hsb_launch(P->yci4, gc, P->yc_threads, P->yc_smem, st, P->X2, P->X1, N1, ncol, P->tw4c, active);
+            P->yci4<<<gc, P->yc_threads, P->yc_smem, st>>>(P->X2, P->X1, N1, ncol, P->tw4c, active);
         else if (P->yc2k)
-            hsb_launch(k_ycoli4_2k, gc, P->yc_threads, P->yc_smem, st, P->X2, P->X1, N1, ncol, P->tw4c, P->tw, P->twL, active);
+            k_ycoli4_2k<<<gc, P->yc_threads, P->yc_smem, st>>>(P->X2, P->X1, N1, ncol, P->tw4c, P->tw, P->twL, active);
         else
             k_fft_cols<float, +1><<<hsb_div_up(ncol, P->TBy), XTHREADS, P->smem_y, st>>>(
                 P->X2, L1, L1, P->X1, N1, N1, L1, ncol, P->tw, P->twL, P->TBy, active);
@@ -1571,7 +1563,7 @@ int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, 
     if (io.ev) cudaEventRecord(io.ev[2], st);
     if (P->xinv4) {
         dim3 gi(hsb_div_up(N1, P->x4i_rows), 3 * N0, nz);
-        hsb_launch(P->xinv4, gi, P->x4i_threads, P->x4i_smem, st, X1, N1, N0, N1, N2, io.h[0], io.h[1], io.hsel, io.hinv,
+        P->xinv4<<<gi, P->x4i_threads, P->x4i_smem, st>>>(X1, N1, N0, N1, N2, io.h[0], io.h[1], io.hsel, io.hinv,
                                                           ncell, ms0, P->tw, P->twL, P->tw4x, P->x4i_rows, active, ss);
     } else {
         dim3 gi(hsb_div_up(N1, P->TYxi), 3 * N0);

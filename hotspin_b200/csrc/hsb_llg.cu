@@ -334,7 +334,6 @@ __device__ __forceinline__ float* resolve_off(const PtrSel& s, const HsbSolverDe
 template <int CH, bool BATCH>
 __global__ void __launch_bounds__(256, 2) k_stage4(const __grid_constant__ HsbPhys P0, const StageArgs A,
                                                    HsbSolverDev* sd0, const BatchArgs Bt) {
-    hsb_pdl_enter();
     const int slot = BATCH ? (int)blockIdx.z : 0;
     HsbSolverDev* sd = sd0 + slot;
     if (!A.ungated && !(A.prep_gated ? sd->prep : sd->active)) return;
@@ -653,7 +652,6 @@ template <int CH, bool BATCH, int W, int NK>
 __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
     k_stagec(const __grid_constant__ HsbPhys P0, const StageArgs A, const KList KL, HsbSolverDev* sd0,
              const BatchArgs Bt) {
-    hsb_pdl_enter();
     const int slot = BATCH ? (int)blockIdx.z : 0;
     HsbSolverDev* sd = sd0 + slot;
     if (!A.ungated && !(A.prep_gated ? sd->prep : sd->active)) return;
@@ -962,7 +960,6 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
 template <int CH, bool BATCH>
 __global__ void __launch_bounds__(256) k_combine(const __grid_constant__ HsbPhys P0, const StageArgs A,
                                                  HsbSolverDev* sd0, const BatchArgs Bt) {
-    hsb_pdl_enter();
     const int slot = BATCH ? (int)blockIdx.z : 0;
     HsbSolverDev* sd = sd0 + slot;
     if (!sd->active) return;
@@ -1000,7 +997,6 @@ __global__ void __launch_bounds__(256) k_combine(const __grid_constant__ HsbPhys
 // Dormand-Prince step-size control, one thread (see the controller rule in the header of
 // include/hotspin_b200.h).  Consumes the attempt's error maximum.
 __global__ void k_dp45_control(HsbSolverDev* sd0, int nslot) {
-    hsb_pdl_enter();
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= nslot) return;
     HsbSolverDev* sd = sd0 + slot;
@@ -1043,7 +1039,6 @@ __global__ void k_dp45_control(HsbSolverDev* sd0, int nslot) {
 
 // Fixed-step bookkeeping: t += dt, step++, swap state buffers, stop at the target.
 __global__ void k_fixed_advance(HsbSolverDev* sd0, int nslot) {
-    hsb_pdl_enter();
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= nslot) return;
     HsbSolverDev* sd = sd0 + slot;
@@ -1101,7 +1096,7 @@ static void launch_c(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, con
     const long cap = (long)hsb_sm_count() * per_sm;
     dim3 grid((unsigned)(g < cap ? g : cap), 1, (unsigned)nslot);
     switch (nk) {
-#define KC(m) case m: hsb_launch(k_stagec<CH, BATCH, W, m>, grid, threads, 0, st, P, A, KL, sd, Bt); break;
+#define KC(m) case m: k_stagec<CH, BATCH, W, m><<<grid, threads, 0, st>>>(P, A, KL, sd, Bt); break;
         KC(0) KC(1) KC(2) KC(3) KC(4) KC(5) KC(6) KC(7)
 #undef KC
     }
@@ -1116,7 +1111,7 @@ static void launch_vec(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, c
         long g = (P.ncell / 4 + threads - 1) / threads;
         const long cap = (long)hsb_sm_count() * 2;
         dim3 grid((unsigned)(g < cap ? g : cap), 1, (unsigned)nslot);
-        hsb_launch(k_stage4<CH, BATCH>, grid, threads, 0, st, P, A, sd, Bt);
+        k_stage4<CH, BATCH><<<grid, threads, 0, st>>>(P, A, sd, Bt);
     } else if (v == 1) {
         launch_c<CH, BATCH, 1>(P, A, sd, Bt, nslot, st);
     } else if (v == 2) {
@@ -1153,13 +1148,13 @@ int hsb_launch_combine(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, c
     const int threads = 256;
     const int grid = hsb_grid_1d(P.ncell, threads, 8);
     BatchArgs nb = {0, nullptr, 1};
-    if (P.nch == 5) hsb_launch(k_combine<5, false>, grid, threads, 0, st, P, A, sd, nb);
-    else hsb_launch(k_combine<3, false>, grid, threads, 0, st, P, A, sd, nb);
+    if (P.nch == 5) k_combine<5, false><<<grid, threads, 0, st>>>(P, A, sd, nb);
+    else k_combine<3, false><<<grid, threads, 0, st>>>(P, A, sd, nb);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }
 
 int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st) {
-    hsb_launch(k_dp45_control, 1, 1, 0, st, sd, 1);
+    k_dp45_control<<<1, 1, 0, st>>>(sd, 1);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }
 
@@ -1179,13 +1174,13 @@ int hsb_launch_combine_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDe
     long g = (P.ncell + threads - 1) / threads;
     const long cap = (long)hsb_sm_count() * 4;
     dim3 grid((unsigned)(g < cap ? g : cap), 1, (unsigned)Bt.nslot);
-    if (P.nch == 5) hsb_launch(k_combine<5, true>, grid, threads, 0, st, P, A, sd, Bt);
-    else hsb_launch(k_combine<3, true>, grid, threads, 0, st, P, A, sd, Bt);
+    if (P.nch == 5) k_combine<5, true><<<grid, threads, 0, st>>>(P, A, sd, Bt);
+    else k_combine<3, true><<<grid, threads, 0, st>>>(P, A, sd, Bt);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }
 
 int hsb_launch_dp45_control_batched(HsbSolverDev* sd, int nslot, cudaStream_t st) {
-    hsb_launch(k_dp45_control, (nslot + 31) / 32, 32, 0, st, sd, nslot);
+    k_dp45_control<<<(nslot + 31) / 32, 32, 0, st>>>(sd, nslot);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }
 
@@ -1201,7 +1196,7 @@ __global__ void k_activate_prepped(HsbSolverDev* sd0, int nslot) {
 }
 
 int hsb_launch_fixed_advance_batched(HsbSolverDev* sd, int nslot, cudaStream_t st) {
-    hsb_launch(k_fixed_advance, (nslot + 31) / 32, 32, 0, st, sd, nslot);
+    k_fixed_advance<<<(nslot + 31) / 32, 32, 0, st>>>(sd, nslot);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }
 
@@ -1211,6 +1206,6 @@ int hsb_launch_activate_prepped(HsbSolverDev* sd, int nslot, cudaStream_t st) {
 }
 
 int hsb_launch_fixed_advance(HsbSolverDev* sd, cudaStream_t st) {
-    hsb_launch(k_fixed_advance, 1, 1, 0, st, sd, 1);
+    k_fixed_advance<<<1, 1, 0, st>>>(sd, 1);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
 }

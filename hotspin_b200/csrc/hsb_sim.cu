@@ -115,6 +115,7 @@ struct hsb_sim_s {
     double* stage_d;
     void* stage_pin;    // batched: pinned per-slot staging of admissions
     cudaGraphExec_t graph;
+    cudaGraphExec_t graph1;  // one attempt: short runs (a few steps) launch no gated attempts
     int graph_steps;    // attempts captured in one graph launch
     bool initialized;   // k1 / hd01 of the current state computed (DP45)
     // eager profiling: events around every launch group of one attempt
@@ -602,27 +603,48 @@ static int prepare(hsb_sim_s* S) {
     return HSB_OK;
 }
 
-static int build_graph(hsb_sim_s* S) {
-    if (S->graph) return HSB_OK;
+// Capture `attempts` attempts into *out.  S->launches counts the kernels of the capture.
+static int capture_attempts(hsb_sim_s* S, int attempts, cudaGraphExec_t* out) {
     cudaGraph_t g;
     HSB_CUDA_TRY(cudaStreamBeginCapture(S->st, cudaStreamCaptureModeThreadLocal));
     int rc = HSB_OK;
     S->launches = 0;
-    for (int a = 0; a < S->graph_steps && rc == HSB_OK; a++) rc = enqueue_attempt(S);
+    for (int a = 0; a < attempts && rc == HSB_OK; a++) rc = enqueue_attempt(S);
     cudaError_t e = cudaStreamEndCapture(S->st, &g);
     if (rc != HSB_OK) return rc;
     if (e != cudaSuccess) {
         hsb_set_error("graph capture: %s", cudaGetErrorString(e));
         return HSB_ERR_CUDA;
     }
-    e = cudaGraphInstantiate(&S->graph, g, 0);
+    e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         hsb_set_error("graph instantiate: %s", cudaGetErrorString(e));
-        S->graph = nullptr;
+        *out = nullptr;
         return HSB_ERR_CUDA;
     }
     return HSB_OK;
+}
+
+static int build_graph(hsb_sim_s* S) {
+    if (S->graph) return HSB_OK;
+    return capture_attempts(S, S->graph_steps, &S->graph);
+}
+
+// The one-attempt graph (S->launches keeps the count of the full graph).
+static int build_graph1(hsb_sim_s* S) {
+    if (S->graph1) return HSB_OK;
+    const long keep = S->launches;
+    const int rc = capture_attempts(S, 1, &S->graph1);
+    S->launches = keep;
+    return rc;
+}
+
+static void drop_graphs(hsb_sim_s* S) {
+    if (S->graph) cudaGraphExecDestroy(S->graph);
+    if (S->graph1) cudaGraphExecDestroy(S->graph1);
+    S->graph = nullptr;
+    S->graph1 = nullptr;
 }
 
 static int plain_only(hsb_sim_s* S, const char* who) {
@@ -654,15 +676,27 @@ static int advance(hsb_sim_s* S, int64_t nsteps, double t_stop) {
     RC(prepare(S));
     RC(build_graph(S));
     const bool fixed_step = S->d.solver != SOLVER_DP45;
+    const int G = S->graph_steps;
+    // fewer steps than a graph holds (e.g. one step per call): one-attempt graphs, so no
+    // launch carries attempts that the device would gate off
+    const bool short_run = nsteps >= 0 && nsteps < G;
+    if (short_run || (fixed_step && nsteps >= 0 && nsteps % G != 0)) RC(build_graph1(S));
     int64_t launched = 0;
-    const int64_t max_attempts = fixed_step ? (nsteps >= 0 ? nsteps : INT64_MAX) : INT64_MAX;
     while (true) {
-        HSB_CUDA_TRY(cudaGraphLaunch(S->graph, S->st));
-        launched += S->graph_steps;
         if (fixed_step && nsteps >= 0) {
-            if (launched >= max_attempts) break;
+            // whole graphs, then single attempts for the remainder
+            if (nsteps - launched >= G) {
+                HSB_CUDA_TRY(cudaGraphLaunch(S->graph, S->st));
+                launched += G;
+            } else {
+                HSB_CUDA_TRY(cudaGraphLaunch(S->graph1, S->st));
+                launched += 1;
+            }
+            if (launched >= nsteps) break;
             continue;
         }
+        HSB_CUDA_TRY(cudaGraphLaunch(short_run ? S->graph1 : S->graph, S->st));
+        launched += short_run ? 1 : G;
         HSB_CUDA_TRY(cudaMemcpyAsync(&S->sd_host->active, &S->sd->active, sizeof(int), cudaMemcpyDeviceToHost, S->st));
         HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
         if (!S->sd_host->active) break;
@@ -797,7 +831,7 @@ static void point_slot0(hsb_sim_s* S, const SlotLayout& L) {
 
 static void free_sim(hsb_sim_s* S) {
     if (!S) return;
-    if (S->graph) cudaGraphExecDestroy(S->graph);
+    drop_graphs(S);
     for (auto e : S->ev_pool) cudaEventDestroy(e);
     if (S->demag) hsb_demag_plan_destroy(S->demag);
     cudaFree(S->arena);
@@ -1051,10 +1085,7 @@ HSB_EXPORT int hsb_sim_set(hsb_sim_s* S, const char* name, const double* host, i
             k_d2f<<<hsb_grid_1d(S->n, 256), 256, 0, S->st>>>(S->stage_d, *dst, S->n);
         }
         fill_phys(S);
-        if (S->graph) {
-            cudaGraphExecDestroy(S->graph);
-            S->graph = nullptr;
-        }
+        drop_graphs(S);
         S->initialized = false;
         HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
         return HSB_OK;

@@ -29,12 +29,4 @@ int hsb_sm_count() {
     return cached[dev];
 }
 
-// Off by default: on the 512x512x4 DP45 bench the step graph with programmatic edges ran at
-// 1307 Mcell-steps/s against 1451 without them (one B200).
-static int g_pdl = 0;
-
-int hsb_pdl_enabled() { return __atomic_load_n(&g_pdl, __ATOMIC_RELAXED); }
-
-HSB_EXPORT int hsb_set_pdl(int on) { return __atomic_exchange_n(&g_pdl, on ? 1 : 0, __ATOMIC_RELAXED); }
-
 HSB_EXPORT int hsb_version(void) { return 1; }

@@ -161,14 +161,6 @@ int hsb_set_stage_variant(int v);
 /* The variant a handle (simulation or batch) runs. */
 int hsb_stage_variant_of(hsb_sim sim);
 
-/* Programmatic dependent launch of the step kernels (no reference counterpart): when on, each
- * stage, FFT and controller kernel is launched so that its blocks become resident while the
- * previous kernel finishes, and waits on the device for that kernel's completion before
- * touching memory.  Off by default (measured slower in the step graphs on B200).  Results are
- * identical either way.  Applies to launches issued (and step graphs captured) afterwards.
- * Returns the previous setting. */
-int hsb_set_pdl(int on);
-
 /* The handle's CUDA stream (cudaStream_t) for callers that interleave their own work. */
 void* hsb_sim_stream(hsb_sim sim);
 

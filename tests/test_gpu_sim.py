@@ -270,44 +270,3 @@ def test_thermal_dp45_equilibrium_is_boltzmann(cuda):
     # 4096 spins x ~10 decorrelated samples: standard error ~0.002
     assert abs(got - want) < 0.015
 
-
-def test_programmatic_launch_changes_nothing(cuda):
-    """Step graphs with programmatic dependent launch and without it (the default) produce
-    bit-identical trajectories: DP45 on TTM + LLB + demag + laser, and RK4 with the thermal
-    field on the multi-pass FFT path."""
-    from hotspin_b200 import _lib
-    lib = _lib.load()
-    size = (2, 16, 32)
-    kw = dict(TTM, size=size, seed=5, laser_t0=5e-14)
-    rng = np.random.default_rng(12)
-    th, ph = np.deg2rad(5.0) * rng.random(size), 2 * np.pi * rng.random(size)
-    me = F.equilibrium_m(300.0, kw["tc"], 0.5)
-    y = {"m": me * np.stack([np.cos(th), np.sin(th) * np.sin(ph), np.sin(th) * np.cos(ph)]),
-         "Te": np.full(size, 300.0), "Tl": np.full(size, 300.0)}
-    size5 = (32, 16, 16)
-    m5 = rng.normal(size=(3,) + size5)
-    m5 /= np.sqrt((m5 * m5).sum(0))
-    kw5 = dict(size=size5, cellsize=(2e-9,) * 3, msat0T0=8e5, lex=float(np.sqrt(2 * 1.3e-11 / (4e-7 * np.pi * 8e5 ** 2))),
-               alpha=(0.5,) * 3, demag=True, normalize=True, thermal=True, seed=3, temperature=100.0)
-    out = {}
-    old = lib.hsb_set_pdl(1)
-    assert old == 0           # off by default
-    try:
-        for pdl in (1, 0):
-            lib.hsb_set_pdl(pdl)
-            with Simulation(**kw, solver="dp45", dt=1e-16, rtol=1e-5, mindt=1e-20, maxdt=1e-13) as sim:
-                for name, val in y.items():
-                    sim.set(name, val)
-                sim.run_until(2e-13)
-                a = (sim.get("m"), sim.get("Te"), sim.status()["steps"])
-            with Simulation(**kw5, solver="rk4", dt=2e-14) as sim:
-                sim.set("m", m5)
-                sim.step(30)
-                b = sim.get("m")
-            out[pdl] = (a, b)
-    finally:
-        lib.hsb_set_pdl(old)
-    (a1, b1), (a0, b0) = out[1], out[0]
-    assert a1[2] == a0[2]
-    assert np.array_equal(a1[0], a0[0]) and np.array_equal(a1[1], a0[1])
-    assert np.array_equal(b1, b0)
