@@ -697,15 +697,15 @@ static int advance(hsb_sim_s* S, int64_t nsteps, double t_stop) {
         }
         HSB_CUDA_TRY(cudaGraphLaunch(short_run ? S->graph1 : S->graph, S->st));
         launched += short_run ? 1 : G;
-        HSB_CUDA_TRY(cudaMemcpyAsync(&S->sd_host->active, &S->sd->active, sizeof(int), cudaMemcpyDeviceToHost, S->st));
-        HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
+        // the whole solver word block (one round trip either way): current when the loop ends
+        RC(get_sd(S));
         if (!S->sd_host->active) break;
         if (launched > 100000000LL) {
             hsb_set_error("solver did not reach its target");
             return HSB_ERR_SOLVER;
         }
     }
-    RC(get_sd(S));
+    if (fixed_step && nsteps >= 0) RC(get_sd(S));
     if (S->sd_host->status & 1) {
         hsb_set_error("state became non-finite at t = %g", S->sd_host->t);
         return HSB_ERR_NONFINITE;
