@@ -586,12 +586,15 @@ static int prepare(hsb_sim_s* S) {
     float* y0 = S->y[0];
     float* y1 = S->y[1];
     const PtrSel YC = pair(y0, y1, SEL_CUR);
+    // ungated: the state's first-stage data are computed even when the run about to start is
+    // already inactive (target reached), so `initialized` always describes the buffers
     if (S->d.thermal) {
-        if (S->demag) RC(run_demag(S, nullptr, 0, nullptr, 0));
+        if (S->demag) RC(run_demag(S, nullptr, 0, nullptr, 0, false));
     } else {
         float* hd = S->demag ? S->hd : nullptr;
-        RC(run_demag(S, nullptr, 0, hd, -1));
+        RC(run_demag(S, nullptr, 0, hd, -1, false));
         StageArgs A = empty_args();
+        A.ungated = 1;
         A.ys = YC;
         A.hd = fixed(hd);
         A.ytherm = YC;
@@ -655,24 +658,36 @@ static int plain_only(hsb_sim_s* S, const char* who) {
     return HSB_OK;
 }
 
+// Arms the solver words for a run on the device, so the host needs no read of them first:
+// a non-finite state stays inactive (reported after the run); a time target already
+// reached leaves it inactive; dt is clipped to land on the target.
+__global__ void k_arm(HsbSolverDev* sd, long long nsteps, double t_stop) {
+    if (sd->status & 1) {
+        sd->active = 0;
+        return;
+    }
+    sd->active = 1;
+    sd->step_stop = nsteps >= 0 ? sd->step + nsteps : -1;
+    sd->t_stop = t_stop;
+    if (t_stop > 0.0) {
+        if (t_stop - sd->t <= 1e-6 * sd->dt) sd->active = 0;
+        else if (sd->dt > t_stop - sd->t) sd->dt = t_stop - sd->t;
+    }
+}
+
 // Advance until the device clears `active` (step or time target reached).
 static int advance(hsb_sim_s* S, int64_t nsteps, double t_stop) {
     RC(plain_only(S, "hsb_sim_step/run_until"));
-    RC(get_sd(S));
-    HsbSolverDev* h = S->sd_host;
-    if (h->status & 1) {
-        hsb_set_error("state is not finite (status %d)", h->status);
-        return HSB_ERR_NONFINITE;
+    if (nsteps == 0) {
+        RC(get_sd(S));
+        if (S->sd_host->status & 1) {
+            hsb_set_error("state is not finite (status %d)", S->sd_host->status);
+            return HSB_ERR_NONFINITE;
+        }
+        return HSB_OK;
     }
-    h->active = 1;
-    h->step_stop = nsteps >= 0 ? h->step + nsteps : -1;
-    h->t_stop = t_stop;
-    if (t_stop > 0.0) {
-        if (t_stop - h->t <= 1e-6 * h->dt) return HSB_OK;
-        if (h->dt > t_stop - h->t) h->dt = t_stop - h->t;
-    }
-    if (nsteps == 0) return HSB_OK;
-    RC(set_sd_fields(S));
+    k_arm<<<1, 1, 0, S->st>>>(S->sd, (long long)nsteps, t_stop);
+    HSB_CUDA_TRY(cudaGetLastError());
     RC(prepare(S));
     RC(build_graph(S));
     const bool fixed_step = S->d.solver != SOLVER_DP45;
