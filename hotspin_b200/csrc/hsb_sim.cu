@@ -116,6 +116,7 @@ struct hsb_sim_s {
     void* stage_pin;    // batched: pinned per-slot staging of admissions
     cudaGraphExec_t graph;
     cudaGraphExec_t graph1;  // one attempt: short runs (a few steps) launch no gated attempts
+    bool sd_fresh;      // sd_host equals the device words: read back, nothing enqueued since
     int graph_steps;    // attempts captured in one graph launch
     bool initialized;   // k1 / hd01 of the current state computed (DP45)
     // eager profiling: events around every launch group of one attempt
@@ -273,18 +274,21 @@ __global__ void k_energy(const HsbPhys P, const float* __restrict__ y, const flo
 
 // ------------------------------------------------------------------ helpers
 static int set_sd_fields(hsb_sim_s* S) {
+    S->sd_fresh = false;
     HSB_CUDA_TRY(cudaMemcpyAsync(S->sd, S->sd_host, sizeof(HsbSolverDev), cudaMemcpyHostToDevice, S->st));
     return HSB_OK;
 }
 static int get_sd(hsb_sim_s* S) {
     HSB_CUDA_TRY(cudaMemcpyAsync(S->sd_host, S->sd, sizeof(HsbSolverDev), cudaMemcpyDeviceToHost, S->st));
     HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
+    S->sd_fresh = true;
     return HSB_OK;
 }
 
 // Demag of one of the two state buffers (sel: -1 fixed pointer `m`, 0 = y[cur], 1 = y[next])
 // into `h` (or into hd01[cur / next] when hsel >= 0).
 static int run_demag(hsb_sim_s* S, const float* m, int msel, float* h, int hsel, bool gated = true) {
+    S->sd_fresh = false;
     if (!S->demag) return HSB_OK;
     HsbDemagIO io;
     if (msel < 0) {
@@ -361,15 +365,18 @@ static int timed(hsb_sim_s* S, int cat, F&& f) {
 
 // Launches of one simulation or of a batch of slots.
 static int L_stage(hsb_sim_s* S, StageArgs A) {
+    S->sd_fresh = false;
     if (S->prep_mode) A.prep_gated = 1;
     if (S->batched) return hsb_launch_stage_batched(S->P, A, S->sd, S->bt, S->st, S->stage_variant);
     return hsb_launch_stage(S->P, A, S->sd, S->st, S->stage_variant);
 }
 static int L_combine(hsb_sim_s* S, const StageArgs& A) {
+    S->sd_fresh = false;
     if (S->batched) return hsb_launch_combine_batched(S->P, A, S->sd, S->bt, S->st);
     return hsb_launch_combine(S->P, A, S->sd, S->st);
 }
 static int L_control(hsb_sim_s* S) {
+    S->sd_fresh = false;
     if (S->batched) return hsb_launch_dp45_control_batched(S->sd, S->nslot, S->st);
     return hsb_launch_dp45_control(S->sd, S->st);
 }
@@ -382,6 +389,7 @@ static void thermal_keep(hsb_sim_s* S, StageArgs& A, bool first) {
 }
 
 static int L_advance(hsb_sim_s* S) {
+    S->sd_fresh = false;
     if (S->batched) return hsb_launch_fixed_advance_batched(S->sd, S->nslot, S->st);
     return hsb_launch_fixed_advance(S->sd, S->st);
 }
@@ -686,6 +694,7 @@ static int advance(hsb_sim_s* S, int64_t nsteps, double t_stop) {
         }
         return HSB_OK;
     }
+    S->sd_fresh = false;
     k_arm<<<1, 1, 0, S->st>>>(S->sd, (long long)nsteps, t_stop);
     HSB_CUDA_TRY(cudaGetLastError());
     RC(prepare(S));
@@ -1204,7 +1213,7 @@ HSB_EXPORT int hsb_sim_status(hsb_sim_s* S, double* t, double* dt, int64_t* step
                               int64_t* rejects, double* err, int32_t* status) {
     RC(plain_only(S, "hsb_sim_status"));
     if (!S) return HSB_ERR_INVALID;
-    RC(get_sd(S));
+    if (!S->sd_fresh) RC(get_sd(S));   // after a step call the words were just read back
     const HsbSolverDev* h = S->sd_host;
     if (t) *t = h->t;
     if (dt) *dt = h->dt;
@@ -1584,6 +1593,7 @@ HSB_EXPORT int hsb_batch_launch(hsb_sim_s* B, int32_t graphs) {
     }
     RC(prepare_slots(B));
     RC(build_graph(B));
+    B->sd_fresh = false;
     for (int g = 0; g < graphs; g++) HSB_CUDA_TRY(cudaGraphLaunch(B->graph, B->st));
     HSB_CUDA_TRY(cudaMemcpyAsync(B->sd_host, B->sd, sizeof(HsbSolverDev) * B->nslot, cudaMemcpyDeviceToHost,
                                  B->st));
