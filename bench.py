@@ -348,10 +348,10 @@ def run_ours(args):
 
 
 def other_configs():
-    """Device throughput of the other single-simulation configurations (synthetic states):
-    config 2 (LLB at 300 K, 256x256x8 of 2 nm, FePt-like, Ku 7e6 along z, lambda 0.1,
-    thermal field, DP45 rtol 1e-5) and config 5 (plain LLG, 1024x1024x32 of 2 nm, alpha 0.5,
-    RK4 20 fs; demag padded to 2048x2048x64 on the multi-pass FFT path)."""
+    """Device throughput of the other single-simulation workloads (synthetic states): LLB at
+    300 K on 256x256x8 cells of 2 nm (FePt-like, Ku 7e6 along z, lambda 0.1, thermal field,
+    DP45 rtol 1e-5) and plain LLG on 1024x1024x32 cells of 2 nm (alpha 0.5, RK4 20 fs; demag
+    padded to 2048x2048x64 on the multi-pass FFT path)."""
     import ctypes
     import torch
     from hotspin_b200 import _lib
@@ -359,13 +359,13 @@ def other_configs():
     lib = _lib.load()
     out = {}
     cases = {
-        "c2_llb_256x256x8_dp45": (dict(size=(8, 256, 256), cellsize=(2e-9,) * 3, msat0T0=1.1e6,
+        "llb_256x256x8_dp45": (dict(size=(8, 256, 256), cellsize=(2e-9,) * 3, msat0T0=1.1e6,
                                         lex=math.sqrt(2 * 1e-11 / (MU0 * 1.1e6 ** 2)), gamma_ll=2.211e5,
                                         alpha=(0.1,) * 3, ku=7e6, anis_u=(1.0, 0.0, 0.0), demag=True, llb=True,
                                         tc=700.0, spin_j=0.5, n_spins=1.1e6 / (2 * MUB * 0.5), temperature=300.0,
                                         thermal=True, seed=2, solver="dp45", dt=1e-16, rtol=1e-5, mindt=1e-20,
                                         maxdt=1e-12), 100),
-        "c5_llg_1024x1024x32_rk4": (dict(size=(32, 1024, 1024), cellsize=(2e-9,) * 3, msat0T0=8e5,
+        "llg_1024x1024x32_rk4": (dict(size=(32, 1024, 1024), cellsize=(2e-9,) * 3, msat0T0=8e5,
                                           lex=math.sqrt(2 * 1.3e-11 / (MU0 * 8e5 ** 2)),
                                           gamma_ll=2.211e5 / (1 + 0.25), alpha=(0.5,) * 3, demag=True,
                                           normalize=True, solver="rk4", dt=20e-15), 20),
@@ -458,7 +458,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched-serving comparison")
-    ap.add_argument("--no-configs", action="store_true", help="skip the config 2 / config 5 throughput lines")
+    ap.add_argument("--no-configs", action="store_true", help="skip the LLB 256x256x8 and LLG 1024x1024x32 throughput lines")
     ap.add_argument("--serving-requests", type=int, default=256)
     ap.add_argument("--serving-tend", type=float, default=50e-12)
     args = ap.parse_args()

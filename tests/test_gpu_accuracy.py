@@ -1,12 +1,12 @@
-"""Accuracy of the FP32 device path against the FP64 oracle on reduced versions of the five
-benchmark configurations: max |dm| (and |dT| for the two-temperature model) and the relative
+"""Accuracy of the FP32 device path against the FP64 oracle on reduced versions of the
+benchmark workloads: max |dm| (and |dT| for the two-temperature model) and the relative
 energy error after the stated integration.
 
-The full-size configurations are too large for the FP64 host oracle; each case keeps the
-configuration's physics, integrator and tolerance on a grid the oracle integrates in seconds.
+The full-size workloads are too large for the FP64 host oracle; each case keeps the
+workload's physics, integrator and tolerance on a grid the oracle integrates in seconds.
 Thermal fields are off (their parity is trajectory-level and is covered by test_gpu_sim.py);
-config 1's random start is replaced by the reference's smooth standard-problem start (the
-random start is chaotic, so no implementation stays within 1e-5 of another on it).
+the thin-film LLG case's random start is replaced by the reference's smooth standard-problem
+start (the random start is chaotic, so no implementation stays within 1e-5 of another on it).
 The LLB cases' energy tolerance is looser than their |dm| one: the longitudinal-field energy
 is as stiff in |m| as the longitudinal relaxation (the reason those solves need femtosecond
 steps), so a |m| difference at FP32 rounding moves it by ~1e-4 of the total.
@@ -42,22 +42,22 @@ def _random_unit(size, seed):
 
 
 CASES = {
-    # config 1: plain LLG, RK4 50 fs (smooth start, 1000 steps)
-    "c1_llg_rk4": dict(
+    # thin-film plain LLG (128x32x1), RK4 50 fs (smooth start, 1000 steps)
+    "llg_film_rk4": dict(
         kw=dict(size=(1, 32, 128), cellsize=(3e-9, 3.90625e-9, 3.90625e-9), msat0T0=8e5, lex=_lex(8e5, 1.3e-11),
                 gamma_ll=F.GAMMA0 / (1 + 0.02 ** 2), alpha=(0.02,) * 3, b_ext=(0.0, 0.012, 0.016), demag=True,
                 normalize=True),
         init=lambda size: {"m": np.stack([np.zeros(size), np.full(size, 2 ** -0.5), np.full(size, 2 ** -0.5)])},
         solver="rk4", dt=50e-15, steps=1000, tol_m=1e-5, tol_e=1e-5),
-    # config 2: LLB at 300 K, FePt-like, uniaxial Ku along z (program X), DP45 1e-5
-    "c2_llb_dp45": dict(
+    # LLB at 300 K, FePt-like, uniaxial Ku along z (program X), DP45 1e-5
+    "llb_fept_dp45": dict(
         kw=dict(size=(8, 16, 16), cellsize=(2e-9,) * 3, msat0T0=1.1e6, lex=_lex(1.1e6, 1e-11), gamma_ll=F.GAMMA0,
                 alpha=(0.1,) * 3, ku=7e6, anis_u=(1.0, 0.0, 0.0), demag=True, llb=True, tc=700.0, spin_j=0.5,
                 n_spins=1.1e6 / (2 * MUB * 0.5), temperature=300.0),
         init=lambda size: {"m": _tilted(size, 5.0, 2, F.equilibrium_m(300.0, 700.0, 0.5))},
         solver="dp45", dt=1e-16, t_end=1e-12, tol_m=1e-4, tol_e=1e-3),
-    # config 3: two-temperature model + LLB with the laser pulse, DP45 1e-5
-    "c3_ttm_llb_dp45": dict(
+    # two-temperature model + LLB with the laser pulse, DP45 1e-5
+    "ttm_llb_laser_dp45": dict(
         kw=dict(size=(4, 32, 32), cellsize=(4e-9,) * 3, msat0T0=8e5, lex=_lex(8e5, 1.3e-11),
                 gamma_ll=F.GAMMA0 / (1 + 0.02 ** 2), alpha=(0.02,) * 3, b_ext=(0.02, 0.0, 0.0), demag=True, llb=True,
                 tc=630.0, spin_j=0.5, n_spins=8e5 / (2 * MUB * 0.5), temperature=300.0, ttm=True, gamma_e=700.0,
@@ -66,8 +66,8 @@ CASES = {
         init=lambda size: dict(m=_tilted(size, 5.0, 3, F.equilibrium_m(300.0, 630.0, 0.5)),
                                Te=np.full(size, 300.0), Tl=np.full(size, 300.0)),
         solver="dp45", dt=2e-16, t_end=5e-13, tol_m=1e-4, tol_e=1e-3),
-    # config 5: large-instance physics on the multi-pass FFT path (L0 = 64), RK4 20 fs, alpha 0.5
-    "c5_llg_rk4_multipass": dict(
+    # large-instance LLG physics on the multi-pass FFT path (L0 = 64), RK4 20 fs, alpha 0.5
+    "llg_multipass_rk4": dict(
         kw=dict(size=(32, 16, 16), cellsize=(2e-9,) * 3, msat0T0=8e5, lex=_lex(8e5, 1.3e-11),
                 gamma_ll=F.GAMMA0 / (1 + 0.5 ** 2), alpha=(0.5,) * 3, demag=True, normalize=True),
         init=lambda size: {"m": _random_unit(size, 5)},
