@@ -554,7 +554,13 @@ __global__ void __launch_bounds__(256, 3) k_xinv4(const float2* __restrict__ in,
 // 3*N0 sequences of length L1 (B lanes each), z in registers (LZ = L0 <= 16).
 // PR: y and z are zero-padded to twice their lengths (open boundaries): the upper halves of
 // the forward inputs are zero and only the lower halves of the inverse outputs are kept.
-template <int L1, int LZ, bool PR>
+// Symmetric-tensor component of the pair (c, c2) of program components.
+__host__ __device__ constexpr int kcomp(int c, int c2) {
+    return c == c2 ? c : ((c + c2 == 3) ? KYZ : ((c + c2 == 2) ? KXZ : KXY));
+}
+
+// DZ: a zero-padded z axis of 2 or 4 cells is convolved directly (see k_zdirect).
+template <int L1, int LZ, bool PR, bool DZ = PR && (LZ == 4 || LZ == 8)>
 __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restrict__ X1, int N0, int N1, int C2,
                                              const float* __restrict__ kern4, const float2* __restrict__ tw4,
                                              const int* __restrict__ active, const SlotStrides ss) {
@@ -590,6 +596,54 @@ __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restric
     __syncthreads();
     const int h0 = LZ / 2, h1 = L1 / 2;
     for (int k1 = tid; k1 < L1; k1 += nthr) {
+        if constexpr (DZ) {
+            // direct convolution along z with the kernel's z-space rows (k_zdirect):
+            // H_c(a0) = sum_b0,c2 G_c,c2(a0 - b0) m_c2(b0), G real for the components even
+            // in z, i x (the stored value) for KXZ, KXY, and G(-d) = conj G(d)
+            constexpr int NZ = LZ / 2;
+            float2 mz[3][NZ];
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int z = 0; z < NZ; z++) mz[c][z] = sm[(c * N0 + z) * SS + k1];
+            const float s1 = k1 > h1 ? -1.f : 1.f;
+            const long cs = h1 + 1;
+            const float* Gb = kern4 + (long)kx * (h0 + 1) * 6 * cs + (k1 > h1 ? L1 - k1 : k1);
+            float g[6][NZ];
+#pragma unroll
+            for (int d = 0; d < NZ; d++)
+#pragma unroll
+                for (int q = 0; q < 6; q++) g[q][d] = __ldg(Gb + ((long)d * 6 + q) * cs);
+#pragma unroll
+            for (int d = 0; d < NZ; d++) {
+                g[KYZ][d] *= s1;
+                g[KXY][d] *= s1;
+            }
+#pragma unroll
+            for (int a0 = 0; a0 < NZ; a0++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    float ax = 0.f, ay = 0.f;
+#pragma unroll
+                    for (int b0 = 0; b0 < NZ; b0++)
+#pragma unroll
+                        for (int c2 = 0; c2 < 3; c2++) {
+                            const int q = kcomp(c, c2);
+                            const int d = a0 - b0;
+                            const float2 m = mz[c2][b0];
+                            if (q == KXZ || q == KXY) {
+                                const float hv = d < 0 ? -g[q][-d] : g[q][d];
+                                ax = fmaf(-hv, m.y, ax);
+                                ay = fmaf(hv, m.x, ay);
+                            } else {
+                                const float gv = g[q][d < 0 ? -d : d];
+                                ax = fmaf(gv, m.x, ax);
+                                ay = fmaf(gv, m.y, ay);
+                            }
+                        }
+                    sm[(c * N0 + a0) * SS + k1] = make_float2(ax, ay);
+                }
+        } else {
         float2 w[3][LZ];
 #pragma unroll
         for (int c = 0; c < 3; c++)
@@ -624,6 +678,7 @@ __global__ void __launch_bounds__(384, LZ >= 16 ? 1 : 2) k_yz4(float2* __restric
 #pragma unroll
             for (int z = 0; z < LZ; z++)
                 if (z < N0) sm[(c * N0 + z) * SS + k1] = w[c][z];
+        }
     }
     __syncthreads();
 #pragma unroll
@@ -988,6 +1043,35 @@ __global__ void k_extract(const double2* __restrict__ X, int L0, int C2, int L1,
     }
 }
 
+// Direct-z rows of the kernel for a zero-padded z axis of N0 = L0 / 2 <= 4 cells (the y/z
+// kernel's DZ form): the inverse z transform of the folded spectrum of one component,
+// G(d) = sum_k0 K(k0) exp(+2 pi i k0 d / L0), d < N0, in FP64 from the FP64 spectrum.  It is
+// real for the components even in z and imaginary for KXZ and KXY (odd in z; stored: the
+// imaginary part); its real or imaginary part replaces rows d of kern4 (row N0 = h0 keeps
+// the spectrum's value, unused).  Run after k_extract of the same component.
+__global__ void k_zdirect(const double2* __restrict__ X, int L0, int C2, int L1, int comp, double scale,
+                          float* __restrict__ kern4) {
+    const int h0 = L0 / 2, h1 = L1 / 2, N0 = L0 / 2;
+    const bool odd = comp == KXZ || comp == KXY;
+    const long tot = (long)C2 * (h1 + 1);
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < tot; q += (long)gridDim.x * blockDim.x) {
+        const int f1 = (int)(q % (h1 + 1));
+        const int kx = (int)(q / (h1 + 1));
+        double V[5];
+        for (int f0 = 0; f0 <= h0 && f0 < 5; f0++) V[f0] = X[((long)f0 * C2 + kx) * L1 + f1].x * scale;
+        for (int d = 0; d < N0; d++) {
+            double g = 0.0;
+            for (int k0 = 0; k0 < L0; k0++) {
+                const int f0 = k0 > h0 ? L0 - k0 : k0;
+                const double a = 2.0 * (double)k0 * (double)d / (double)L0;   // angle / pi
+                if (odd) g += (k0 > h0 ? -V[f0] : V[f0]) * sinpi(a);
+                else g += V[f0] * cospi(a);
+            }
+            kern4[(((long)kx * (h0 + 1) + d) * 6 + comp) * (h1 + 1) + f1] = (float)g;
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------ host plan
 struct hsb_demag_plan_s {
     int N[3], L[3], pbc[3];
@@ -1019,6 +1103,7 @@ struct hsb_demag_plan_s {
     zc4_fn zc4;
     int yc2k, yc_threads, yc_cols, yc_smem, zc_k1, zc_smem;
     float2* tw4c;       // four-step twiddles of the y columns (length L1, or 1024 for yc2k)
+    int zdirect;        // the y/z kernel convolves z directly: kern4 rows d < N0 hold k_zdirect
     float2* tw4z;       // and of the z transform (length L0)
 };
 
@@ -1178,6 +1263,8 @@ int hsb_demag_spectrum_enqueue(hsb_demag_plan P, const double* cs, int accuracy,
         k_fft_z<double><<<gz, XTHREADS, smz, st>>>(s->X, 1, L0, L0, C2, L1, nullptr, 0, s->tw64, P->twL, TK, nullptr);
         k_extract<<<hsb_grid_1d((long)C2 * (h1 + 1) * (h0 + 1), 256), 256, 0, st>>>(s->X, L0, C2, L1, comp, scale,
                                                                                      kern, kern4, s->dmax);
+        if (kern4 && P->zdirect)
+            k_zdirect<<<hsb_grid_1d((long)C2 * (h1 + 1), 256), 256, 0, st>>>(s->X, L0, C2, L1, comp, scale, kern4);
         HSB_CUDA_TRY(cudaGetLastError());
     }
     return HSB_OK;
@@ -1434,6 +1521,7 @@ HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, co
         yz4_fn yf = (L0 <= 16) ? yz4_for(L1, L0, pryz, &By, &Sy) : nullptr;
         if (yf && 3 * N0 * By <= 384 && (3 * N0 * Sy + L1) * (int)sizeof(float2) <= 110 * 1024) {
             P->yz4 = yf;
+            P->zdirect = pryz && (L0 == 4 || L0 == 8);   // the DZ instantiations of k_yz4
             if (!P->kern4) PTRY(cudaMalloc(&P->kern4, sizeof(float) * kcount));
             rc = make_tw4(L1, By, P->twL, &P->tw4y);
             if (rc != HSB_OK) { hsb_demag_plan_destroy(P); return rc; }

@@ -15,7 +15,8 @@ pytestmark = pytest.mark.gpu
 GEOMS = [
     # (size program order, cellsize, pbc)
     ((1, 32, 128), (3e-9, 3.90625e-9, 3.90625e-9), (0, 0, 0)),    # thin film, fused yz (L0 = 1)
-    ((4, 32, 64), (4e-9, 4e-9, 4e-9), (0, 0, 0)),                  # fused, L0 = 8
+    ((4, 32, 64), (4e-9, 4e-9, 4e-9), (0, 0, 0)),                  # fused, L0 = 8 (direct z)
+    ((2, 16, 32), (2e-9, 3e-9, 4e-9), (0, 0, 0)),                  # fused, L0 = 4 (direct z)
     ((8, 16, 32), (2e-9, 2e-9, 2e-9), (0, 0, 0)),                  # fused, L0 = 16
     ((16, 16, 16), (1e-9, 2.5e-9, 5e-9), (0, 0, 0)),               # multipass (L0 = 32)
     ((16, 1024, 4), (2e-9, 2e-9, 2e-9), (0, 0, 0)),                # multipass, 2048-point y split
