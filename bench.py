@@ -258,6 +258,8 @@ def run_ours(args):
     kw = workload()
     ncell = int(np.prod(kw["size"]))
     st0 = initial_state(kw)
+    if args.stage_variant is not None:      # fixed stage-kernel variant (e.g. under a profiler)
+        _lib.load().hsb_set_stage_variant(args.stage_variant)
     sim = Simulation(**kw, solver="dp45", dt=2e-16, rtol=1e-5, mindt=1e-20, maxdt=1e-13)
     for k, v in st0.items():
         sim.set(k, v)
@@ -459,6 +461,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched-serving comparison")
     ap.add_argument("--no-configs", action="store_true", help="skip the LLB 256x256x8 and LLG 1024x1024x32 throughput lines")
+    ap.add_argument("--stage-variant", type=int, default=None, choices=[0, 1, 2, 4],
+                    help="run this stage-kernel variant instead of the one timed at creation")
     ap.add_argument("--serving-requests", type=int, default=256)
     ap.add_argument("--serving-tend", type=float, default=50e-12)
     args = ap.parse_args()
