@@ -70,7 +70,10 @@ def algorithmic_bytes(kw, fused=True):
     L0, L1, L2 = [2 * s if s > 1 else s for s in kw["size"]]
     c2 = L2 // 2 + 1
     spec = 3 * n0 * c2 * n1 * 8                  # X1: complex FP32 after the x pass
-    kern = c2 * (L1 // 2 + 1) * (L0 // 2 + 1) * 6 * 4
+    # kernel rows read per kx column: L0/2 + 1 folded z frequencies, or the N0 z-space rows of
+    # the direct z convolution (zero-padded z axis of 2 or 4 cells)
+    zrows = n0 if L0 in (4, 8) else L0 // 2 + 1
+    kern = c2 * (L1 // 2 + 1) * zrows * 6 * 4
     nch = 5 if kw.get("ttm") else 3
     # DP45 attempt with a thermal field: stage 1 + stages 2..6 + stage 7
     stage = 0
@@ -91,7 +94,8 @@ def family_roofline(kw, solver, prof_ms):
     c2 = L2 // 2 + 1
     spec = 3 * n0 * c2 * n1 * 8
     x2 = 3 * n0 * c2 * L1 * 8                     # multi-pass y-transformed spectrum
-    kern = c2 * (L1 // 2 + 1) * (L0 // 2 + 1) * 6 * 4
+    zrows = n0 if L0 in (4, 8) else L0 // 2 + 1   # direct z convolution reads N0 rows
+    kern = c2 * (L1 // 2 + 1) * zrows * 6 * 4
     nch = 5 if kw.get("ttm") else 3
     fused = L0 <= 16
     yz = 2 * spec + kern if fused else 2 * spec + 4 * x2 + kern
