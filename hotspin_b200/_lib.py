@@ -59,6 +59,7 @@ _SIGS = {
     "hsb_sim_energy": (c_int, [c_vp, c_dp]),
     "hsb_sim_average_m": (c_int, [c_vp, c_dp]),
     "hsb_sim_energy_terms": (c_int, [c_vp, c_dp]),
+    "hsb_sim_max_torque": (c_int, [c_vp, c_dp]),
     "hsb_sim_stream": (c_vp, [c_vp]),
     "hsb_sim_profile": (c_int, [c_vp, c_int, c_dp]),
     "hsb_sim_launches_per_attempt": (c_int, [c_vp, c_ip]),

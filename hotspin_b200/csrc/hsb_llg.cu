@@ -97,7 +97,7 @@ template <int CH>
 __device__ __forceinline__ void rhs_cell(const HsbPhys& P, const float* __restrict__ ys,
                                          const float* __restrict__ hd, const float* __restrict__ yth,
                                          double t, double dt, long long step, int a0, int a1, int a2,
-                                         long i, float* y, float* k) {
+                                         long i, float* y, float* k, bool torque_only = false) {
     const long n = P.ncell;
     const long s1 = P.N2, s0 = (long)P.N1 * P.N2;
     load_ch<CH>(ys, n, i, y);
@@ -177,9 +177,10 @@ __device__ __forceinline__ void rhs_cell(const HsbPhys& P, const float* __restri
         k[0] = k[1] = k[2] = 0.f;
     } else {
         const float g = P.gamma;
-        k[0] = g * (-H[1] * y[2] + H[2] * y[1]) + g * P.lam[0] * H[0];
-        k[1] = g * (-H[2] * y[0] + H[0] * y[2]) + g * P.lam[1] * H[1];
-        k[2] = g * (-H[0] * y[1] + H[1] * y[0]) + g * P.lam[2] * H[2];
+        const float r = torque_only ? 0.f : 1.f;
+        k[0] = g * (-H[1] * y[2] + H[2] * y[1]) + r * g * P.lam[0] * H[0];
+        k[1] = g * (-H[2] * y[0] + H[0] * y[2]) + r * g * P.lam[1] * H[1];
+        k[2] = g * (-H[0] * y[1] + H[1] * y[0]) + r * g * P.lam[2] * H[2];
     }
     // ---- two-temperature model
     if (CH >= 5) {
@@ -246,7 +247,7 @@ __global__ void __launch_bounds__(256) k_stage(const HsbPhys P, const StageArgs 
         const int a1 = (int)(r % P.N1);
         const int a0 = (int)(r / P.N1);
         float y[CH], k[CH];
-        rhs_cell<CH>(P, ys, hd, yth, ts, dt, step, a0, a1, a2, i, y, k);
+        rhs_cell<CH>(P, ys, hd, yth, ts, dt, step, a0, a1, a2, i, y, k, A.torque_only != 0);
         if (kout) {
 #pragma unroll
             for (int c = 0; c < CH; c++) {
@@ -1138,6 +1139,15 @@ int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cud
         else launch_vec<3, false>(P, A, sd, nb, 1, st, variant);
         return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
     }
+    const int grid = hsb_grid_1d(P.ncell, threads, 8);
+    if (P.nch == 5) k_stage<5><<<grid, threads, 0, st>>>(P, A, sd);
+    else k_stage<3><<<grid, threads, 0, st>>>(P, A, sd);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}
+
+// The generic per-cell kernel whatever the geometry (state queries such as the torque).
+int hsb_launch_stage_generic(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st) {
+    const int threads = 256;
     const int grid = hsb_grid_1d(P.ncell, threads, 8);
     if (P.nch == 5) k_stage<5><<<grid, threads, 0, st>>>(P, A, sd);
     else k_stage<3><<<grid, threads, 0, st>>>(P, A, sd);

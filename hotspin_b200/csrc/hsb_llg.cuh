@@ -137,4 +137,5 @@ struct StageArgs {
     // 1 = generate it and store it to hth, 2 = read it from hth (load-first kernel only)
     int hth_mode;
     PtrSel hth;              // [3][ncell]
+    int torque_only;         // generic kernel only: k = gamma (m x H), without the relaxation term
 };

@@ -24,6 +24,7 @@ bool hsb_stage_keeps_thermal(const HsbPhys& P, int variant);
 bool hsb_stage_tunable(const HsbPhys& P);
 extern "C" int hsb_set_stage_variant(int v);
 int hsb_launch_combine(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st);
+int hsb_launch_stage_generic(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st);
 int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st);
 int hsb_launch_fixed_advance(HsbSolverDev* sd, cudaStream_t st);
 int hsb_launch_stage_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
@@ -1337,6 +1338,52 @@ HSB_EXPORT int hsb_sim_energy_terms(hsb_sim_s* S, double* out5) {
     const double V = S->d.cellsize[0] * S->d.cellsize[1] * S->d.cellsize[2];
     const double pre = V * MU0 * S->d.msat0T0;
     for (int q = 0; q < 5; q++) out5[q] = pre * r[q];
+    return HSB_OK;
+}
+
+// max over cells of |v| for a [3][n] FP32 field, into the FP64 word at `out` (non-negative
+// doubles order like their bit patterns)
+__global__ void k_maxnorm3(const float* __restrict__ v, long n, unsigned long long* out) {
+    double m = 0.0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double x = v[i], y = v[n + i], z = v[2 * n + i];
+        m = fmax(m, sqrt(x * x + y * y + z * z));
+    }
+    m = warp_max_d(m);
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// Maximum over cells of |gamma (m x H_eff)| (1/s) of the current state, H_eff with every field
+// term of the right-hand side (thermal field of the current step included).  hotspin's
+// maxtorque module: max |torque| (mod_maxtorque.go, MaxNormUpdater update_reduce.go:132-142).
+HSB_EXPORT int hsb_sim_max_torque(hsb_sim_s* S, double* out) {
+    RC(plain_only(S, "hsb_sim_max_torque"));
+    if (!S || !out) return HSB_ERR_INVALID;
+    RC(get_sd(S));
+    float* y = S->y[S->sd_host->cur];
+    float* hd = nullptr;
+    if (S->demag) {
+        RC(run_demag(S, y, -1, S->hd, -1, false));
+        hd = S->hd;
+    }
+    StageArgs A = empty_args();
+    A.ungated = 1;
+    A.torque_only = 1;
+    A.ys = fixed(y);
+    A.hd = fixed(hd);
+    A.ytherm = fixed(y);
+    A.kout = fixed(S->ystage[1]);
+    A.kself_w = 1.0f;
+    S->sd_fresh = false;
+    RC(hsb_launch_stage_generic(S->P, A, S->sd, S->st));
+    double* word = S->red + RED_BLOCKS * 8 + 10;
+    HSB_CUDA_TRY(cudaMemsetAsync(word, 0, sizeof(double), S->st));
+    k_maxnorm3<<<hsb_grid_1d(S->n, 256), 256, 0, S->st>>>(S->ystage[1], S->n, (unsigned long long*)word);
+    HSB_CUDA_TRY(cudaGetLastError());
+    HSB_CUDA_TRY(cudaMemcpyAsync(S->red_host, word, sizeof(double), cudaMemcpyDeviceToHost, S->st));
+    HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
+    *out = S->red_host[0];
+    S->initialized = false;    // the stage buffer used here may hold first-stage data
     return HSB_OK;
 }
 

@@ -126,6 +126,12 @@ class Simulation:
         _lib.check(self._lib.hsb_sim_average_m(self._h, a), "hsb_sim_average_m")
         return np.array(list(a))
 
+    def max_torque(self):
+        """max over cells of |gamma (m x H_eff)| (1/s), reduced on the device."""
+        v = ctypes.c_double()
+        _lib.check(self._lib.hsb_sim_max_torque(self._h, ctypes.byref(v)), "hsb_sim_max_torque")
+        return v.value
+
 
 class Batch:
     """A size class of simulations advanced together (hsb_batch_* in include/hotspin_b200.h).

@@ -124,6 +124,10 @@ int hsb_sim_average_m(hsb_sim sim, double* avg3);
 /* The energy's terms (J): Zeeman, exchange, demag, uniaxial anisotropy, MFA longitudinal
  * field (mod_energy.go:20-66 per term; their sum is hsb_sim_energy). */
 int hsb_sim_energy_terms(hsb_sim sim, double* out5);
+/* Maximum over cells of |gamma_LL (m x H_eff)| (1/s) of the current state, reduced on the device:
+ * hotspin's maxtorque module (modules/mod_maxtorque.go, MaxNormUpdater
+ * engine/update_reduce.go:132-142) applied to the LLBar torque (llbar-torque.cu:11-45). */
+int hsb_sim_max_torque(hsb_sim sim, double* out);
 
 /* Device time of one attempt by kernel family (eager launches between CUDA events on the
  * handle's stream; each profiled attempt is a real step): out[0] fused RHS+stage kernels,

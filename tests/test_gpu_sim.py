@@ -74,6 +74,28 @@ def test_rhs_matches_oracle(cuda, kw, thermal):
         assert rel_err(k[4], want["Tl"]) < 3e-5
 
 
+@pytest.mark.parametrize("kw", [LLG, LLB, TTM], ids=["llg", "llb", "ttm"])
+def test_max_torque_matches_oracle(cuda, kw):
+    """hsb_sim_max_torque = max over cells of |gamma (m x H_eff)| of the oracle's field; twice in
+    a row (the reduction word is cleared per call), and the state is untouched."""
+    kw = dict(kw, thermal=False, dt=1e-14, solver="rk4")
+    spec, desc = pair(**{k: v for k, v in kw.items() if k not in ("solver", "dt")})
+    y = state(kw)
+    model = Model(spec)
+    m = F.normalize(y["m"]) if spec.normalize else y["m"]
+    H = model.heff(dict(y, m=m))
+    tau = F.llbar_torque(m, H, None, spec.gamma_ll)
+    want = float(np.sqrt((tau * tau).sum(0)).max())
+    with Simulation(**desc, solver="rk4", dt=kw["dt"]) as sim:
+        for name, v in y.items():
+            sim.set(name, v)
+        got = [sim.max_torque(), sim.max_torque()]
+        m_after = sim.get("m")
+    assert got[0] == got[1]
+    assert abs(got[0] - want) < 3e-5 * want
+    assert np.abs(m_after - m).max() < 1e-6
+
+
 def test_masks_rhs(cuda):
     size = (2, 8, 16)
     rng = np.random.default_rng(4)
