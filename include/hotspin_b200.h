@@ -92,6 +92,9 @@ typedef struct hsb_sim_s* hsb_sim;
 const char* hsb_last_error(void);
 void hsb_clear_error(void);
 int hsb_version(void);
+/* CRC-64 (ISO polynomial, Go hash/crc64 convention) that seals a #dump002 frame
+ * (dump/writer.go:46-76); host function, no GPU needed.  Used by hotspin_b200.dump. */
+uint64_t hsb_crc64_iso(const void* data, int64_t n);
 
 /* Allocate device state, build the demag kernel (FP64 Kernel_Arne on the GPU), set the
  * initial state m = (0,0,1), Te = Tl = temperature.  Runs on the current CUDA device. */

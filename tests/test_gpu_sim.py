@@ -292,3 +292,21 @@ def test_thermal_dp45_equilibrium_is_boltzmann(cuda):
     # 4096 spins x ~10 decorrelated samples: standard error ~0.002
     assert abs(got - want) < 0.015
 
+
+
+def test_dump_of_a_simulation(cuda, tmp_path):
+    """hotspin_b200.dump.write_simulation writes the handle's m and time as a #dump002 frame."""
+    from hotspin_b200 import dump
+    kw = dict(LLG, thermal=False)
+    spec, desc = pair(**kw)
+    y = state(kw)
+    p = str(tmp_path / "m.dump")
+    with Simulation(**desc, solver="rk4", dt=1e-14) as sim:
+        sim.set("m", y["m"])
+        sim.step(3)
+        dump.write_simulation(p, sim)
+        m = sim.get("m")
+        t = sim.status()["t"]
+    (data, hdr), = dump.read(p)
+    assert np.array_equal(data, m.astype(np.float32))
+    assert hdr["time"] == t and hdr["label"] == "m" and hdr["mesh"] == kw["size"]
