@@ -199,8 +199,7 @@ __device__ __forceinline__ void rhs_cell(const HsbPhys& P, const float* __restri
         }
         float Qe = lapE + P.g_ep * (Tl - Te);
         if (P.laser_p0 != 0.f) {
-            const float ts = (float)(t - (double)P.laser_t0);
-            float q = P.laser_p0 * expf(-P.laser_c * ts * ts);
+            float q = hsb_laser_power(P, t);
             if (P.laser_inv2s2 != 0.f) {
                 const float yy = ((float)a1 + 0.5f - 0.5f * (float)P.N1) * P.cs1;
                 const float xx = ((float)a2 + 0.5f - 0.5f * (float)P.N2) * P.cs2;
@@ -360,11 +359,7 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const __grid_constant__ HsbPh
     // per-launch constants
     const double dte = dt > P.cutoff_dt ? dt : P.cutoff_dt;
     const float th_amp = (float)(P.th_pre / dte);
-    float laser_t = 0.f;
-    if (CH >= 5 && P.laser_p0 != 0.f) {
-        const float tt = (float)(ts - (double)P.laser_t0);
-        laser_t = P.laser_p0 * expf(-P.laser_c * tt * tt);
-    }
+    const float laser_t = (CH >= 5) ? hsb_laser_power(P, ts) : 0.f;
     float emax = 0.f;
     bool bad = false;
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < ngroups; g += (long)gridDim.x * blockDim.x) {
@@ -692,11 +687,7 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
     const long ngroups = n / W;
     const double dte = dt > P.cutoff_dt ? dt : P.cutoff_dt;
     const float th_amp = (float)(P.th_pre / dte);
-    float laser_t = 0.f;
-    if (CH >= 5 && P.laser_p0 != 0.f) {
-        const float tt = (float)(ts - (double)P.laser_t0);
-        laser_t = P.laser_p0 * expf(-P.laser_c * tt * tt);
-    }
+    const float laser_t = (CH >= 5) ? hsb_laser_power(P, ts) : 0.f;
     float emax = 0.f;
     bool bad = false;
     const float dt_rtol = A.err ? fdt / A.rtol : 0.f;

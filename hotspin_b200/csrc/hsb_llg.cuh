@@ -40,6 +40,8 @@ struct HsbPhys {
     float g_ep, gamma_e, c_l;
     float laser_p0, laser_t0, laser_c;  // c = 4 ln2 / fwhm^2
     float laser_inv2s2;                 // 1/(2 sigma^2), 0 = uniform spot
+    const double2* laser_tab;           // pointwise time profile (t, factor), laser_npts >= 2
+    int laser_npts;                     // 0: Gaussian pulse in time
     float cs1, cs2;
     int normalize;       // renormalise m at stage formation (LLG mode); used by batched launches
     float ms0;           // Ms0 (A/m), the demag scale of this simulation
@@ -47,6 +49,30 @@ struct HsbPhys {
     // (round-up reciprocal, Granlund & Montgomery 1994): q = umulhi(x, mul) >> shr
     unsigned div2_mul, div2_shr, div1_mul, div1_shr;
 };
+
+// Absorbed laser power density (W/m^3, before the lateral spot) at time t: laser_p0 times a
+// Gaussian of the given FWHM around laser_t0, or times the piecewise-linear interpolation of
+// a (time, factor) table as hotspin's pointwise quantities evaluate theirs
+// (engine/update_pointwiseof.go:31-98); zero outside the table's time range.  Uniform over a
+// launch: every thread finds the same table interval.
+__device__ __forceinline__ float hsb_laser_power(const HsbPhys& P, double t) {
+    if (P.laser_p0 == 0.f) return 0.f;
+    if (P.laser_npts >= 2) {
+        const double2* tab = P.laser_tab;
+        int lo = 0, hi = P.laser_npts - 1;
+        if (t < tab[0].x || t > tab[hi].x) return 0.f;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (tab[mid].x <= t) lo = mid;
+            else hi = mid;
+        }
+        const double2 a = tab[lo], b = tab[hi];
+        const double f = a.y + (t - a.x) / (b.x - a.x) * (b.y - a.y);
+        return (float)((double)P.laser_p0 * f);
+    }
+    const float tt = (float)(t - (double)P.laser_t0);
+    return P.laser_p0 * expf(-P.laser_c * tt * tt);
+}
 
 // Quotient by the divisor encoded in (mul, shr); mul == 0 encodes a divisor of 1.
 __host__ __device__ __forceinline__ unsigned hsb_fastdiv(unsigned x, unsigned mul, unsigned shr) {

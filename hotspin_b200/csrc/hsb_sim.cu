@@ -55,6 +55,8 @@ struct hsb_sim_desc {
     double laser_p0, laser_t0, laser_fwhm, laser_sigma;
     int32_t solver;
     double dt, rtol, mindt, maxdt;
+    const double* laser_table;   // 2 x laser_npts (t, factor); copied at creation
+    int32_t laser_npts;
 };
 
 enum { SOLVER_EULER = 0, SOLVER_HEUN = 1, SOLVER_RK4 = 2, SOLVER_DP45 = 3 };
@@ -118,6 +120,7 @@ struct hsb_sim_s {
     cudaGraphExec_t graph;
     cudaGraphExec_t graph1;  // one attempt: short runs (a few steps) launch no gated attempts
     bool sd_fresh;      // sd_host equals the device words: read back, nothing enqueued since
+    double2* laser_tab; // device copy of the pointwise laser profile (or null)
     int graph_steps;    // attempts captured in one graph launch
     bool initialized;   // k1 / hd01 of the current state computed (DP45)
     // eager profiling: events around every launch group of one attempt
@@ -799,6 +802,8 @@ static void phys_from_desc(const hsb_sim_desc& d, int nch, long ncell, HsbPhys& 
 
 static void fill_phys(hsb_sim_s* S) {
     phys_from_desc(S->d, S->nch, S->n, S->P);
+    S->P.laser_tab = S->laser_tab;
+    S->P.laser_npts = S->laser_tab ? S->d.laser_npts : 0;
     S->P.msat_mask = S->msat_mask;
     S->P.lex_mask = S->lex_mask;
 }
@@ -869,6 +874,7 @@ static void free_sim(hsb_sim_s* S) {
     cudaFree(S->lex_mask);
     cudaFree(S->sd);
     cudaFree(S->red);
+    cudaFree(S->laser_tab);
     cudaFree(S->stage_f);
     cudaFree(S->stage_d);
     if (S->sd_host) cudaFreeHost(S->sd_host);
@@ -998,6 +1004,19 @@ static int check_desc(const hsb_sim_desc& d, const char* who) {
         hsb_set_error("%s: %ld cells exceed the 2^28 limit", who, n);
         return HSB_ERR_UNSUPPORTED;
     }
+    if (d.laser_npts != 0) {
+        if (d.laser_npts < 2 || d.laser_npts > 4096 || !d.laser_table) {
+            hsb_set_error("%s: laser_npts must be 0 or 2..4096 with a table, got %d", who, d.laser_npts);
+            return HSB_ERR_INVALID;
+        }
+        for (int i = 0; i < d.laser_npts; i++) {
+            const double t = d.laser_table[2 * i], v = d.laser_table[2 * i + 1];
+            if (!isfinite(t) || !isfinite(v) || (i > 0 && !(t > d.laser_table[2 * i - 2]))) {
+                hsb_set_error("%s: laser table point %d is not finite or its time is not increasing", who, i);
+                return HSB_ERR_INVALID;
+            }
+        }
+    }
     return HSB_OK;
 }
 
@@ -1012,10 +1031,15 @@ HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     const long n = (long)d.size[0] * d.size[1] * d.size[2];
     hsb_sim_s* S = new hsb_sim_s();
     S->d = d;
+    S->d.laser_table = nullptr;    // the caller's array is copied to the device below
     S->n = n;
     S->nch = d.ttm ? 5 : 3;
     S->nslot = 1;
     STRY(cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking));
+    if (d.laser_npts >= 2) {
+        STRY(cudaMalloc(&S->laser_tab, sizeof(double2) * d.laser_npts));
+        STRY(cudaMemcpy(S->laser_tab, d.laser_table, sizeof(double2) * d.laser_npts, cudaMemcpyHostToDevice));
+    }
     const SlotLayout L = slot_layout(d, n);
     STRY(cudaMalloc(&S->arena, sizeof(float) * L.total));
     STRY(cudaMemsetAsync(S->arena, 0, sizeof(float) * L.total, S->st));
@@ -1407,6 +1431,10 @@ HSB_EXPORT int hsb_sim_average_m(hsb_sim_s* S, double* avg3) {
 // kernel spectrum, damping, field, anisotropy, temperature, LLB or LLG, seed) is per slot.
 static int batch_check_class(const hsb_sim_desc& d, int32_t nslot, const char* who) {
     RC(check_desc(d, who));
+    if (d.laser_npts != 0) {
+        hsb_set_error("%s: pointwise laser profiles are not supported in batches", who);
+        return HSB_ERR_UNSUPPORTED;
+    }
     if (nslot < 1 || nslot > 65535) {
         hsb_set_error("%s: nslot = %d outside [1, 65535]", who, nslot);
         return HSB_ERR_INVALID;
@@ -1552,6 +1580,10 @@ HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* d
     const hsb_sim_desc& d = *desc;
     const hsb_sim_desc& c = B->d;
     RC(check_desc(d, "hsb_batch_admit"));
+    if (d.laser_npts != 0) {
+        hsb_set_error("hsb_batch_admit: pointwise laser profiles are not supported in batches");
+        return HSB_ERR_UNSUPPORTED;
+    }
     for (int a = 0; a < 3; a++) {
         if (d.size[a] != c.size[a] || d.pbc[a] != c.pbc[a]) {
             hsb_set_error("hsb_batch_admit: grid size / boundaries differ from the class");

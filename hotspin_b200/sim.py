@@ -24,7 +24,14 @@ def make_desc(**kw):
     d.maxdt = 1e-12
     d.laser_fwhm = 1e-13
     for k, v in kw.items():
-        if k not in _FIELDS:
+        if k == "laser_table":
+            # pointwise laser time profile: (t, factor) pairs, copied by hsb_sim_create
+            tab = np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(-1, 2))
+            d._laser_keep = tab          # alive as long as the descriptor
+            d.laser_table = tab.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            d.laser_npts = tab.shape[0]
+            continue
+        if k not in _FIELDS or k == "laser_npts":
             raise KeyError("unknown simulation parameter %r" % k)
         if k == "solver" and isinstance(v, str):
             v = SOLVERS[v.lower()]

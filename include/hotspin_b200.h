@@ -85,6 +85,14 @@ typedef struct hsb_sim_desc {
     double dt;              /* initial / fixed time step, s                        */
     double rtol;            /* DP45 tolerance                                      */
     double mindt, maxdt;    /* DP45 step bounds                                    */
+    /* Pointwise laser time profile (hotspin's PointwiseOf quantities,
+     * engine/update_pointwiseof.go:31-98): laser_npts >= 2 pairs (t_i in s, strictly
+     * increasing; factor_i) as 2 * laser_npts doubles; the absorbed power is laser_p0 times
+     * their piecewise-linear interpolation, zero outside [t_0, t_last] (the reference stops
+     * with an error past the last point).  laser_npts = 0: the Gaussian pulse above.  Copied
+     * at creation; not available in batches.                                            */
+    const double* laser_table;
+    int32_t laser_npts;     /* 0 or 2..4096                                          */
 } hsb_sim_desc;
 
 typedef struct hsb_sim_s* hsb_sim;

@@ -60,6 +60,7 @@ class Spec:
     laser_t0: float = 0.0            # s, pulse centre
     laser_fwhm: float = 1.0e-13      # s
     laser_sigma: float = 0.0         # m, lateral Gaussian spot (0 = uniform)
+    laser_table: object = None       # (t, factor) pairs: pointwise time profile instead of the Gaussian
     msat_mask: Optional[np.ndarray] = None
     lex_mask: Optional[np.ndarray] = None
 
@@ -78,7 +79,17 @@ def laser_profile(spec):
 
 
 def laser_time(spec, t):
-    """Gaussian time envelope with the given FWHM, peak 1 at t0."""
+    """Time factor of the absorbed power: a Gaussian with the given FWHM, peak 1 at t0; or,
+    with a (t, factor) table, its piecewise-linear interpolation as a hotspin pointwise
+    quantity (engine/update_pointwiseof.go:31-98), zero outside the table's time range."""
+    if spec.laser_table is not None:
+        tab = np.asarray(spec.laser_table, dtype=np.float64).reshape(-1, 2)
+        if t < tab[0, 0] or t > tab[-1, 0]:
+            return 0.0
+        i = int(np.searchsorted(tab[:, 0], t, side="right")) - 1
+        i = min(max(i, 0), len(tab) - 2)
+        (t1, v1), (t2, v2) = tab[i], tab[i + 1]
+        return float(v1 + (t - t1) / (t2 - t1) * (v2 - v1))
     s = (t - spec.laser_t0) / spec.laser_fwhm
     return math.exp(-4.0 * math.log(2.0) * s * s)
 

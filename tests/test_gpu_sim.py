@@ -310,3 +310,37 @@ def test_dump_of_a_simulation(cuda, tmp_path):
     (data, hdr), = dump.read(p)
     assert np.array_equal(data, m.astype(np.float32))
     assert hdr["time"] == t and hdr["label"] == "m" and hdr["mesh"] == kw["size"]
+
+
+def test_pointwise_laser_profile(cuda):
+    """A (time, factor) laser table is interpolated linearly as hotspin's pointwise quantities
+    are, zero outside its range: the two-temperature RHS matches the oracle's at times on a
+    ramp, on a knot and past the table, and DP45 through the pulse matches the oracle's run.
+    Batches refuse such tables."""
+    from hotspin_b200 import _lib
+    from hotspin_b200.sim import Batch
+    tab = [(0.0, 0.0), (5e-14, 1.0), (1.2e-13, 0.3), (2.0e-13, 0.0)]
+    kw = dict(TTM, thermal=False, laser_table=tab)
+    spec, desc = pair(**kw)
+    y = state(kw, seed=13)
+    model = Model(spec)
+    with Simulation(**desc, solver="rk4", dt=1e-15) as sim:
+        for name, v in y.items():
+            sim.set(name, v)
+        for t in (2.5e-14, 5e-14, 9e-14, 2.5e-13):
+            sim.set_time(t)
+            k = sim.get("k")
+            want = model.rhs(t, y)
+            assert rel_err(k[3], want["Te"]) < 3e-5, t
+            assert rel_err(k[:3], want["m"]) < 3e-5, t
+    it = Integrator(Model(spec), y, "dp45", 1e-15, rtol=1e-4, mindt=1e-20, maxdt=1e-12)
+    it.run_until(2e-13)
+    with Simulation(**desc, solver="dp45", dt=1e-15, rtol=1e-4, mindt=1e-20, maxdt=1e-12) as sim:
+        for name, v in y.items():
+            sim.set(name, v)
+        sim.run_until(2e-13)
+        m, T = sim.get("m"), sim.get("Te")
+    assert np.abs(m - it.y["m"]).max() < 2e-4
+    assert rel_err(T, it.y["Te"]) < 1e-4
+    with pytest.raises(_lib.HsbError, match="batches"):
+        Batch(2, **dict(desc, size=(2, 16, 32)), solver="dp45", dt=1e-15)
