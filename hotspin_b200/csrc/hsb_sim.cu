@@ -1020,6 +1020,9 @@ static int check_desc(const hsb_sim_desc& d, const char* who) {
     return HSB_OK;
 }
 
+// Size of the descriptor as compiled into the library, for bindings to check their layout.
+HSB_EXPORT int hsb_sim_desc_bytes(void) { return (int)sizeof(hsb_sim_desc); }
+
 HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     if (!desc || !out) {
         hsb_set_error("hsb_sim_create: null argument");
