@@ -1334,14 +1334,18 @@ static int tune_x(hsb_demag_plan_s* P, cudaStream_t st) {
             dim3 g(hsb_div_up(N1, rows), 3 * N0);
             for (int which = 0; which < 2; which++) {
                 float best_ms = 1e30f;
+                // each timing covers 8 back-to-back launches: single ~20 us launches between
+                // events were noisy enough to pick a slower shape on some runs
                 for (int rep = 0; rep < 4; rep++) {
                     cudaEventRecord(e0, st);
-                    if (which == 0)
-                        P->xfwd4<<<g, th, smem, st>>>(m, m, nullptr, 0, nullptr, ncell, N0, N1, N2, N1, P->X1, P->tw,
-                                                      P->twL, P->tw4x, rows, nullptr, ss);
-                    else
-                        P->xinv4<<<g, th, smem, st>>>(P->X1, N1, N0, N1, N2, H, H, nullptr, 0, ncell, 1.0f, P->tw,
-                                                      P->twL, P->tw4x, rows, nullptr, ss);
+                    for (int k = 0; k < 8; k++) {
+                        if (which == 0)
+                            P->xfwd4<<<g, th, smem, st>>>(m, m, nullptr, 0, nullptr, ncell, N0, N1, N2, N1, P->X1,
+                                                          P->tw, P->twL, P->tw4x, rows, nullptr, ss);
+                        else
+                            P->xinv4<<<g, th, smem, st>>>(P->X1, N1, N0, N1, N2, H, H, nullptr, 0, ncell, 1.0f,
+                                                          P->tw, P->twL, P->tw4x, rows, nullptr, ss);
+                    }
                     cudaEventRecord(e1, st);
                     if (cudaEventSynchronize(e1) != cudaSuccess) {
                         rc = HSB_ERR_CUDA;
@@ -1349,7 +1353,7 @@ static int tune_x(hsb_demag_plan_s* P, cudaStream_t st) {
                     }
                     float ms = 0;
                     cudaEventElapsedTime(&ms, e0, e1);
-                    if (rep > 0 && ms < best_ms) best_ms = ms;   // first launch is a warm-up
+                    if (rep > 0 && ms < best_ms) best_ms = ms;   // the first rep is a warm-up
                 }
                 if (which == 0 && best_ms < bf) {
                     bf = best_ms;
