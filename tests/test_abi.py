@@ -61,3 +61,53 @@ int main(void) {
     assert (seed, maxdt, tab, npts) == (D.seed.offset, D.maxdt.offset, D.laser_table.offset, D.laser_npts.offset)
     assert version >= 1
     assert crc == 0xB90956C775A41001      # CRC-64/GO-ISO check value of "123456789"
+
+
+def _desc(**kw):
+    from hotspin_b200.sim import make_desc
+    base = dict(size=(1, 8, 8), cellsize=(1e-9,) * 3, msat0T0=8e5, lex=5e-9, solver="rk4", dt=1e-14)
+    base.update(kw)
+    return make_desc(**base)
+
+
+def _create(d):
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    return lib.hsb_sim_create(ctypes.byref(d), ctypes.byref(h)), lib.hsb_last_error()
+
+
+def test_limits_are_checked_before_any_device_work():
+    """Argument checks run on the host before the first CUDA call (so they also hold here):
+    grids above 2^28 cells, bad laser tables, solver/tolerance errors, and demag plans whose
+    padded lengths are not powers of two."""
+    rc, msg = _create(_desc(size=(1024, 1024, 512)))
+    assert rc == 4 and b"2^28" in msg
+    rc, msg = _create(_desc(ttm=True, gamma_e=700.0, c_l=3e6, laser_p0=1e20,
+                            laser_table=[(0.0, 0.0), (1e-13, 1.0), (1e-13, 0.5)]))
+    assert rc == 1 and b"not increasing" in msg
+    rc, msg = _create(_desc(ttm=True, gamma_e=700.0, c_l=3e6, laser_table=[(0.0, 1.0)]))
+    assert rc == 1 and b"laser_npts" in msg
+    rc, msg = _create(_desc(solver="dp45", rtol=0.0))
+    assert rc == 1 and b"rtol" in msg
+    rc, msg = _create(_desc(llb=True, tc=0.0))
+    assert rc == 1 and b"llb" in msg
+    lib = _lib.load()
+    plan = ctypes.c_void_p()
+    size = (ctypes.c_int * 3)(3, 8, 8)          # padded z length 6
+    cs = (ctypes.c_double * 3)(1e-9, 1e-9, 1e-9)
+    pbc = (ctypes.c_int * 3)(0, 0, 0)
+    assert lib.hsb_demag_plan_create(size, cs, pbc, 6, None, ctypes.byref(plan)) == 4
+    assert b"power of two" in lib.hsb_last_error()
+
+
+def test_batches_refuse_what_they_do_not_support():
+    lib = _lib.load()
+    nbytes = ctypes.c_int64()
+    d = _desc(size=(1, 8, 10), solver="dp45")            # a2 not a multiple of 4
+    assert lib.hsb_batch_footprint(ctypes.byref(d), 4, ctypes.byref(nbytes)) == 4
+    d = _desc(size=(1, 8, 8), solver="dp45", ttm=True, gamma_e=700.0, c_l=3e6, laser_p0=1e20,
+              laser_table=[(0.0, 0.0), (1e-13, 1.0)])
+    assert lib.hsb_batch_footprint(ctypes.byref(d), 4, ctypes.byref(nbytes)) == 4
+    assert b"batches" in lib.hsb_last_error()
+    d = _desc(size=(1, 8, 8), solver="dp45")
+    assert lib.hsb_batch_footprint(ctypes.byref(d), 0, ctypes.byref(nbytes)) == 1
