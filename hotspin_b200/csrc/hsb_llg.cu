@@ -141,8 +141,12 @@ __device__ __forceinline__ void rhs_cell(const HsbPhys& P, const float* __restri
 #pragma unroll
         for (int c = 0; c < 3; c++) H[c] += __ldg(hd + c * n + i);
     }
+    {
+        float hb[3];
+        hsb_bext(P, t, hb);
 #pragma unroll
-    for (int c = 0; c < 3; c++) H[c] += P.bext[c];
+        for (int c = 0; c < 3; c++) H[c] += hb[c];
+    }
     // ---- spin temperature
     float Ts = P.T_uniform;
     if (CH >= 5) Ts = y[3];
@@ -360,6 +364,8 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const __grid_constant__ HsbPh
     const double dte = dt > P.cutoff_dt ? dt : P.cutoff_dt;
     const float th_amp = (float)(P.th_pre / dte);
     const float laser_t = (CH >= 5) ? hsb_laser_power(P, ts) : 0.f;
+    float hb[3];
+    hsb_bext(P, ts, hb);
     float emax = 0.f;
     bool bad = false;
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < ngroups; g += (long)gridDim.x * blockDim.x) {
@@ -378,13 +384,13 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const __grid_constant__ HsbPh
                 float h[4];
                 un4(ld4(hd + c * n + i), h);
 #pragma unroll
-                for (int q = 0; q < 4; q++) H[c][q] = h[q] + P.bext[c];
+                for (int q = 0; q < 4; q++) H[c][q] = h[q] + hb[c];
             }
         } else {
 #pragma unroll
             for (int c = 0; c < 3; c++)
 #pragma unroll
-                for (int q = 0; q < 4; q++) H[c][q] = P.bext[c];
+                for (int q = 0; q < 4; q++) H[c][q] = hb[c];
         }
         float lapE[4] = {0.f, 0.f, 0.f, 0.f}, lapL[4] = {0.f, 0.f, 0.f, 0.f};
         // ---- a0 / a1 neighbours: whole float4 rows
@@ -688,6 +694,8 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
     const double dte = dt > P.cutoff_dt ? dt : P.cutoff_dt;
     const float th_amp = (float)(P.th_pre / dte);
     const float laser_t = (CH >= 5) ? hsb_laser_power(P, ts) : 0.f;
+    float hb[3];
+    hsb_bext(P, ts, hb);
     float emax = 0.f;
     bool bad = false;
     const float dt_rtol = A.err ? fdt / A.rtol : 0.f;
@@ -765,7 +773,7 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
 #pragma unroll
             for (int c = 0; c < 3; c++)
 #pragma unroll
-                for (int q = 0; q < W; q++) H[c][q] = (has_hd ? hv[c][q] : 0.f) + P.bext[c];
+                for (int q = 0; q < W; q++) H[c][q] = (has_hd ? hv[c][q] : 0.f) + hb[c];
 #pragma unroll
             for (int q = 0; q < W; q++) lapE[q] = lapL[q] = 0.f;
 #pragma unroll

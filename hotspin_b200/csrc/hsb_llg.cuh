@@ -42,6 +42,8 @@ struct HsbPhys {
     float laser_inv2s2;                 // 1/(2 sigma^2), 0 = uniform spot
     const double2* laser_tab;           // pointwise time profile (t, factor), laser_npts >= 2
     int laser_npts;                     // 0: Gaussian pulse in time
+    const double* bext_tab;             // pointwise applied field: rows (t, Bx, By, Bz) in tesla
+    int bext_npts;                      // 0: the constant bext
     float cs1, cs2;
     int normalize;       // renormalise m at stage formation (LLG mode); used by batched launches
     float ms0;           // Ms0 (A/m), the demag scale of this simulation
@@ -72,6 +74,35 @@ __device__ __forceinline__ float hsb_laser_power(const HsbPhys& P, double t) {
     }
     const float tt = (float)(t - (double)P.laser_t0);
     return P.laser_p0 * expf(-P.laser_c * tt * tt);
+}
+
+// Applied field H_ext (A/m) at time t: the constant bext, or the piecewise-linear interpolation
+// of the (time, B) table divided by mu0 (a pointwise quantity as in
+// engine/update_pointwiseof.go:31-98), zero outside the table's time range.
+__device__ __forceinline__ void hsb_bext(const HsbPhys& P, double t, float* h) {
+    if (P.bext_npts >= 2) {
+        const double* tab = P.bext_tab;
+        int lo = 0, hi = P.bext_npts - 1;
+        if (t < tab[0] || t > tab[4 * hi]) {
+            h[0] = h[1] = h[2] = 0.f;
+            return;
+        }
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (tab[4 * mid] <= t) lo = mid;
+            else hi = mid;
+        }
+        const double f = (t - tab[4 * lo]) / (tab[4 * hi] - tab[4 * lo]);
+        const double inv_mu0 = 1.0 / (4e-7 * 3.14159265358979323846);
+        for (int c = 0; c < 3; c++) {
+            const double a = tab[4 * lo + 1 + c], b = tab[4 * hi + 1 + c];
+            h[c] = (float)((a + f * (b - a)) * inv_mu0);
+        }
+        return;
+    }
+    h[0] = P.bext[0];
+    h[1] = P.bext[1];
+    h[2] = P.bext[2];
 }
 
 // Quotient by the divisor encoded in (mul, shr); mul == 0 encodes a divisor of 1.

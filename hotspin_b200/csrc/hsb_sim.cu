@@ -57,6 +57,8 @@ struct hsb_sim_desc {
     double dt, rtol, mindt, maxdt;
     const double* laser_table;   // 2 x laser_npts (t, factor); copied at creation
     int32_t laser_npts;
+    const double* bext_table;    // 4 x bext_npts (t, Bx, By, Bz); copied at creation
+    int32_t bext_npts;
 };
 
 enum { SOLVER_EULER = 0, SOLVER_HEUN = 1, SOLVER_RK4 = 2, SOLVER_DP45 = 3 };
@@ -121,6 +123,7 @@ struct hsb_sim_s {
     cudaGraphExec_t graph1;  // one attempt: short runs (a few steps) launch no gated attempts
     bool sd_fresh;      // sd_host equals the device words: read back, nothing enqueued since
     double2* laser_tab; // device copy of the pointwise laser profile (or null)
+    double* bext_tab;   // device copy of the pointwise applied field (or null)
     int graph_steps;    // attempts captured in one graph launch
     bool initialized;   // k1 / hd01 of the current state computed (DP45)
     // eager profiling: events around every launch group of one attempt
@@ -184,7 +187,9 @@ __global__ void k_f2d(const float* __restrict__ in, double* __restrict__ out, lo
 //   lf      -(m . H_lf) ms              (times V mu0 Ms0)
 // plus sum of m (3) for the average.
 __global__ void k_energy(const HsbPhys P, const float* __restrict__ y, const float* __restrict__ hd, int normalize,
-                         double* partial, unsigned int* counter, double* out) {
+                         double* partial, unsigned int* counter, double* out, double t) {
+    float hb[3];
+    hsb_bext(P, t, hb);       // the applied field at the state's time
     double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     double comp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const long n = P.ncell;
@@ -230,7 +235,7 @@ __global__ void k_energy(const HsbPhys P, const float* __restrict__ y, const flo
                     hex[c] += (double)P.ex_c[d] * ((w1 * mm[c] + w2 * mp[c]) - (w1 * m[c] + w2 * m[c]));
             }
         }
-        term[0] = -(m[0] * (double)P.bext[0] + m[1] * (double)P.bext[1] + m[2] * (double)P.bext[2]) * ms;
+        term[0] = -(m[0] * (double)hb[0] + m[1] * (double)hb[1] + m[2] * (double)hb[2]) * ms;
         term[1] = -0.5 * (m[0] * hex[0] + m[1] * hex[1] + m[2] * hex[2]) * ms;
         term[2] = 0;
         if (hd) term[2] = -0.5 * (m[0] * (double)hd[i] + m[1] * (double)hd[n + i] + m[2] * (double)hd[2 * n + i]) * ms;
@@ -804,6 +809,8 @@ static void fill_phys(hsb_sim_s* S) {
     phys_from_desc(S->d, S->nch, S->n, S->P);
     S->P.laser_tab = S->laser_tab;
     S->P.laser_npts = S->laser_tab ? S->d.laser_npts : 0;
+    S->P.bext_tab = S->bext_tab;
+    S->P.bext_npts = S->bext_tab ? S->d.bext_npts : 0;
     S->P.msat_mask = S->msat_mask;
     S->P.lex_mask = S->lex_mask;
 }
@@ -875,6 +882,7 @@ static void free_sim(hsb_sim_s* S) {
     cudaFree(S->sd);
     cudaFree(S->red);
     cudaFree(S->laser_tab);
+    cudaFree(S->bext_tab);
     cudaFree(S->stage_f);
     cudaFree(S->stage_d);
     if (S->sd_host) cudaFreeHost(S->sd_host);
@@ -1017,6 +1025,20 @@ static int check_desc(const hsb_sim_desc& d, const char* who) {
             }
         }
     }
+    if (d.bext_npts != 0) {
+        if (d.bext_npts < 2 || d.bext_npts > 4096 || !d.bext_table) {
+            hsb_set_error("%s: bext_npts must be 0 or 2..4096 with a table, got %d", who, d.bext_npts);
+            return HSB_ERR_INVALID;
+        }
+        for (int i = 0; i < d.bext_npts; i++) {
+            const double* r = d.bext_table + 4 * i;
+            if (!isfinite(r[0]) || !isfinite(r[1]) || !isfinite(r[2]) || !isfinite(r[3]) ||
+                (i > 0 && !(r[0] > r[-4]))) {
+                hsb_set_error("%s: field table point %d is not finite or its time is not increasing", who, i);
+                return HSB_ERR_INVALID;
+            }
+        }
+    }
     return HSB_OK;
 }
 
@@ -1034,7 +1056,8 @@ HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     const long n = (long)d.size[0] * d.size[1] * d.size[2];
     hsb_sim_s* S = new hsb_sim_s();
     S->d = d;
-    S->d.laser_table = nullptr;    // the caller's array is copied to the device below
+    S->d.laser_table = nullptr;    // the caller's arrays are copied to the device below
+    S->d.bext_table = nullptr;
     S->n = n;
     S->nch = d.ttm ? 5 : 3;
     S->nslot = 1;
@@ -1042,6 +1065,10 @@ HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     if (d.laser_npts >= 2) {
         STRY(cudaMalloc(&S->laser_tab, sizeof(double2) * d.laser_npts));
         STRY(cudaMemcpy(S->laser_tab, d.laser_table, sizeof(double2) * d.laser_npts, cudaMemcpyHostToDevice));
+    }
+    if (d.bext_npts >= 2) {
+        STRY(cudaMalloc(&S->bext_tab, sizeof(double) * 4 * d.bext_npts));
+        STRY(cudaMemcpy(S->bext_tab, d.bext_table, sizeof(double) * 4 * d.bext_npts, cudaMemcpyHostToDevice));
     }
     const SlotLayout L = slot_layout(d, n);
     STRY(cudaMalloc(&S->arena, sizeof(float) * L.total));
@@ -1275,7 +1302,7 @@ static int reduce_terms(hsb_sim_s* S, double* out8) {
     double* partial = S->red;
     double* res = S->red + RED_BLOCKS * 8;
     unsigned int* counter = (unsigned int*)(S->red + RED_BLOCKS * 8 + 8);
-    k_energy<<<RED_BLOCKS, 256, 0, S->st>>>(S->P, y, hd, S->d.normalize, partial, counter, res);
+    k_energy<<<RED_BLOCKS, 256, 0, S->st>>>(S->P, y, hd, S->d.normalize, partial, counter, res, S->sd_host->t);
     HSB_CUDA_TRY(cudaGetLastError());
     HSB_CUDA_TRY(cudaMemcpyAsync(S->red_host, res, sizeof(double) * 8, cudaMemcpyDeviceToHost, S->st));
     HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
@@ -1434,8 +1461,8 @@ HSB_EXPORT int hsb_sim_average_m(hsb_sim_s* S, double* avg3) {
 // kernel spectrum, damping, field, anisotropy, temperature, LLB or LLG, seed) is per slot.
 static int batch_check_class(const hsb_sim_desc& d, int32_t nslot, const char* who) {
     RC(check_desc(d, who));
-    if (d.laser_npts != 0) {
-        hsb_set_error("%s: pointwise laser profiles are not supported in batches", who);
+    if (d.laser_npts != 0 || d.bext_npts != 0) {
+        hsb_set_error("%s: pointwise laser profiles and field tables are not supported in batches", who);
         return HSB_ERR_UNSUPPORTED;
     }
     if (nslot < 1 || nslot > 65535) {
@@ -1583,8 +1610,8 @@ HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* d
     const hsb_sim_desc& d = *desc;
     const hsb_sim_desc& c = B->d;
     RC(check_desc(d, "hsb_batch_admit"));
-    if (d.laser_npts != 0) {
-        hsb_set_error("hsb_batch_admit: pointwise laser profiles are not supported in batches");
+    if (d.laser_npts != 0 || d.bext_npts != 0) {
+        hsb_set_error("hsb_batch_admit: pointwise laser profiles and field tables are not supported in batches");
         return HSB_ERR_UNSUPPORTED;
     }
     for (int a = 0; a < 3; a++) {

@@ -31,7 +31,14 @@ def make_desc(**kw):
             d.laser_table = tab.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
             d.laser_npts = tab.shape[0]
             continue
-        if k not in _FIELDS or k == "laser_npts":
+        if k == "bext_table":
+            # pointwise applied field: (t, Bx, By, Bz) rows in tesla, program components
+            tab = np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(-1, 4))
+            d._bext_keep = tab
+            d.bext_table = tab.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            d.bext_npts = tab.shape[0]
+            continue
+        if k not in _FIELDS or k in ("laser_npts", "bext_npts"):
             raise KeyError("unknown simulation parameter %r" % k)
         if k == "solver" and isinstance(v, str):
             v = SOLVERS[v.lower()]

@@ -93,6 +93,12 @@ typedef struct hsb_sim_desc {
      * at creation; not available in batches.                                            */
     const double* laser_table;
     int32_t laser_npts;     /* 0 or 2..4096                                          */
+    /* Pointwise applied field: bext_npts >= 2 rows (t_i in s, strictly increasing; Bx, By,
+     * Bz in tesla, program components) as 4 * bext_npts doubles, interpolated linearly at
+     * each stage's time and zero outside [t_0, t_last]; replaces b_ext.  bext_npts = 0: the
+     * constant b_ext.  Copied at creation; not available in batches.                     */
+    const double* bext_table;
+    int32_t bext_npts;      /* 0 or 2..4096                                          */
 } hsb_sim_desc;
 
 typedef struct hsb_sim_s* hsb_sim;

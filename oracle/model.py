@@ -61,6 +61,7 @@ class Spec:
     laser_fwhm: float = 1.0e-13      # s
     laser_sigma: float = 0.0         # m, lateral Gaussian spot (0 = uniform)
     laser_table: object = None       # (t, factor) pairs: pointwise time profile instead of the Gaussian
+    bext_table: object = None        # (t, Bx, By, Bz) rows (tesla): pointwise applied field instead of b_ext
     msat_mask: Optional[np.ndarray] = None
     lex_mask: Optional[np.ndarray] = None
 
@@ -76,6 +77,20 @@ def laser_profile(spec):
     r2 = y[:, None] ** 2 + x[None, :] ** 2
     g = np.exp(-r2 / (2.0 * spec.laser_sigma ** 2))
     return np.broadcast_to(g[None], spec.size).copy()
+
+
+def bext_at(spec, t):
+    """Applied field (tesla, program components) at time t: b_ext, or the piecewise-linear
+    interpolation of the (t, B) table (engine/update_pointwiseof.go:31-98), zero outside it."""
+    if spec.bext_table is None or t is None:
+        return np.asarray(spec.b_ext, dtype=np.float64)
+    tab = np.asarray(spec.bext_table, dtype=np.float64).reshape(-1, 4)
+    if t < tab[0, 0] or t > tab[-1, 0]:
+        return np.zeros(3)
+    i = int(np.searchsorted(tab[:, 0], t, side="right")) - 1
+    i = min(max(i, 0), len(tab) - 2)
+    f = (t - tab[i, 0]) / (tab[i + 1, 0] - tab[i, 0])
+    return tab[i, 1:] + f * (tab[i + 1, 1:] - tab[i, 1:])
 
 
 def laser_time(spec, t):
@@ -141,14 +156,15 @@ class Model:
                                          s.msat0T0, s.spin_j, s.n_spins, s.tc, 1.0)
         return terms
 
-    def heff(self, y):
+    def heff(self, y, time=None):
         s = self.s
         t = self.heff_terms(y)
         H = np.zeros_like(y["m"])
         for name, v in t.items():
             H += v / F.MU0 if name == "B" else v
+        b = bext_at(s, time)
         for c in range(3):
-            H[c] += s.b_ext[c] / F.MU0
+            H[c] += b[c] / F.MU0
         if self.noise is not None:
             H += self.noise
         return H
@@ -158,7 +174,7 @@ class Model:
         m = F.normalize(y["m"]) if s.normalize else y["m"]
         yy = dict(y)
         yy["m"] = m
-        H = self.heff(yy)
+        H = self.heff(yy, t)
         dm = F.llbar_torque(m, H, s.msat_mask, s.gamma_ll)
         dm = dm + F.llbar_local00nc(H, s.msat_mask, None, s.alpha, s.gamma_ll)
         out = {"m": dm}
@@ -175,8 +191,9 @@ class Model:
         return out
 
     # -- energy -------------------------------------------------------------------
-    def energy(self, y):
-        """Total micromagnetic energy as mod_energy.go:20-66 sums it (J)."""
+    def energy(self, y, time=None):
+        """Total micromagnetic energy as mod_energy.go:20-66 sums it (J), with the applied
+        field at `time` when it is given pointwise."""
         s = self.s
         m = F.normalize(y["m"]) if s.normalize else y["m"]
         yy = dict(y)
@@ -184,8 +201,9 @@ class Model:
         V = float(np.prod(s.cellsize))
         t = self.heff_terms(yy)
         E = 0.0
-        bext = np.stack([np.full(s.size, b) for b in s.b_ext])
-        if any(b != 0.0 for b in s.b_ext):
+        b_now = bext_at(s, time)
+        bext = np.stack([np.full(s.size, b) for b in b_now])
+        if any(b != 0.0 for b in b_now):
             E += F.energy_term(m, bext, s.msat_mask, s.msat0T0, -V)
         if "H_ex" in t:
             E += F.energy_term(m, t["H_ex"], s.msat_mask, s.msat0T0, -0.5 * V * F.MU0)

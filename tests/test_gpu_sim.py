@@ -344,3 +344,34 @@ def test_pointwise_laser_profile(cuda):
     assert rel_err(T, it.y["Te"]) < 1e-4
     with pytest.raises(_lib.HsbError, match="batches"):
         Batch(2, **dict(desc, size=(2, 16, 32)), solver="dp45", dt=1e-15)
+
+
+def test_pointwise_applied_field(cuda):
+    """A (t, Bx, By, Bz) table replaces the constant applied field, interpolated linearly at
+    each stage's time and zero outside its range: the RHS and the energy match the oracle's at
+    times on a ramp, on a knot and past the table, and RK4 across the ramps matches the
+    oracle's steps."""
+    from hotspin_b200 import _lib
+    from hotspin_b200.sim import Batch
+    tab = [(0.0, 0.0, 0.0, 0.0), (1e-12, 0.05, 0.0, 0.02), (2e-12, -0.05, 0.01, 0.0)]
+    kw = dict(LLG, thermal=False, bext_table=tab)
+    spec, desc = pair(**kw)
+    y = state(kw, seed=17)
+    model = Model(spec)
+    with Simulation(**desc, solver="rk4", dt=1e-14) as sim:
+        sim.set("m", y["m"])
+        for t in (0.5e-12, 1e-12, 1.7e-12, 3e-12):
+            sim.set_time(t)
+            k = sim.get("k")
+            assert rel_err(k[:3], model.rhs(t, y)["m"]) < 3e-5, t
+            E, Eo = sim.energy(), model.energy(y, t)
+            assert abs(E - Eo) < 1e-5 * abs(Eo), t
+    it = Integrator(Model(spec), y, "rk4", 2e-14)
+    it.run_steps(100)                      # 0 .. 2 ps: both ramps
+    with Simulation(**desc, solver="rk4", dt=2e-14) as sim:
+        sim.set("m", y["m"])
+        sim.step(100)
+        m = sim.get("m")
+    assert np.abs(m - it.y["m"]).max() < 1e-5
+    with pytest.raises(_lib.HsbError, match="batches"):
+        Batch(2, **dict(desc, size=(2, 16, 32)), solver="dp45", dt=1e-15)
