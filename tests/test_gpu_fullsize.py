@@ -1,7 +1,7 @@
 """Size-independent properties at the benchmark's full size (512 x 512 x 4, demag padded to
-1024 x 1024 x 8), where the FP64 oracle is too slow to run: linearity and reciprocity of the
-demag convolution, the thin-film demag limit, energy conservation without damping and energy
-decay with damping."""
+1024 x 1024 x 8) and at the large-instance size (1024 x 1024 x 32, padded 2048 x 2048 x 64),
+where the FP64 oracle is too slow to run: linearity and reciprocity of the demag convolution,
+the thin-film demag limit, energy conservation without damping and energy decay with damping."""
 import ctypes
 
 import numpy as np
@@ -88,3 +88,34 @@ def test_energy_conserved_without_damping_and_decays_with_it(cuda):
         else:
             assert np.all(np.diff(E) < 0)
             assert E[0] - E[-1] > 10 * drift
+
+
+def test_multipass_demag_properties_at_large_size(cuda):
+    """The multi-pass y/z path at the large-instance size (1024x1024x32 cells of 2 nm, padded
+    2048x2048x64: 2048-point y columns, 64-point z convolution): linearity and reciprocity of
+    the convolution, and a uniform film's interior field along its normal near -Ms."""
+    size, cs = (32, 1024, 1024), (2e-9, 2e-9, 2e-9)
+    lib = _lib.load()
+    p = demag_plan(size, cs, (0, 0, 0))
+    try:
+        def field(m):
+            dm = dev(cuda, m, np.float32)
+            H = cuda.empty_like(dm)
+            _lib.check(lib.hsb_demag_field(p, ptr(dm), None, MS, ptr(H), None), "hsb_demag_field")
+            return host(cuda, H).astype(np.float64)
+
+        rng = np.random.default_rng(9)
+        m1 = rng.normal(size=(3,) + size).astype(np.float32)
+        m2 = rng.normal(size=(3,) + size).astype(np.float32)
+        h1, h2 = field(m1), field(m2)
+        h12 = field(0.3 * m1 - 0.7 * m2)
+        assert np.abs(h12 - (0.3 * h1 - 0.7 * h2)).max() / np.abs(h12).max() < 1e-5
+        a, b = float((m1 * h2).sum()), float((m2 * h1).sum())
+        assert abs(a - b) < 1e-5 * max(abs(a), abs(b))
+        m = np.zeros((3,) + size, np.float32)
+        m[0] = 1.0                     # along the thickness (program axis 0)
+        h = field(m)
+        core = h[0][12:20, 384:640, 384:640]
+        assert -1.0 < core.mean() / MS < -0.9
+    finally:
+        lib.hsb_demag_plan_destroy(p)
