@@ -732,9 +732,12 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
         float y[CH][W], H[3][W], lapE[W], lapL[W];
         float thT[W], hthv[3][W];
         {
-            if (hmode == 2) {
+            {
+                // loaded unconditionally (the state's channels when there is no kept field,
+                // then discarded) so the phase's loads carry no branch
+                const float* hsrc = (hmode == 2) ? hth : ys;
 #pragma unroll
-                for (int c = 0; c < 3; c++) ldw<W>(hth + c * n + i, hthv[c]);
+                for (int c = 0; c < 3; c++) ldw<W>(hsrc + c * n + i, hthv[c]);
             }
             float hv[3][W], nb[4][CH][W], sl[CH], sr[CH];
 #pragma unroll
@@ -768,7 +771,7 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
                 sl[c] = __ldg(ys + c * n + il);
                 sr[c] = __ldg(ys + c * n + ir);
             }
-            if (CH >= 5 && th_field) ldw<W>(yth + 3 * n + i, thT);
+            if (CH >= 5) ldw<W>(yth + 3 * n + i, thT);   // yth is the state itself without a field
             // consume
 #pragma unroll
             for (int c = 0; c < 3; c++)
