@@ -545,13 +545,17 @@ __global__ void __launch_bounds__(256, 3) k_xinv4(const float2* __restrict__ in,
     if (r < ny) {
         float* dst = out + comp * out_cstride + ((long)a0 * N1 + y0 + r) * N2;
         const bool even = (N2 & 1) == 0;
+        if (even) {
 #pragma unroll
-        for (int j = 0; j < A; j++) {
-            const int n = fft4_out_index<M>(lane, j);
-            if (2 * n < N2) {
-                if (even) {
-                    reinterpret_cast<float2*>(dst)[n] = make_float2(scale * v[j].x, scale * v[j].y);
-                } else {
+            for (int j = 0; j < A; j++) {
+                const int n = fft4_out_index<M>(lane, j);
+                if (2 * n < N2) reinterpret_cast<float2*>(dst)[n] = make_float2(scale * v[j].x, scale * v[j].y);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < A; j++) {
+                const int n = fft4_out_index<M>(lane, j);
+                if (2 * n < N2) {
                     dst[2 * n] = scale * v[j].x;
                     if (2 * n + 1 < N2) dst[2 * n + 1] = scale * v[j].y;
                 }
