@@ -66,6 +66,9 @@ _SIGS = {
     "hsb_sim_stream": (c_vp, [c_vp]),
     "hsb_sim_profile": (c_int, [c_vp, c_int, c_dp]),
     "hsb_sim_launches_per_attempt": (c_int, [c_vp, c_ip]),
+    "hsb_sim_launch_count": (c_int, [c_vp, ctypes.POINTER(c_i64)]),
+    "hsb_sim_checkpoint": (c_int, [c_vp]),
+    "hsb_sim_restore": (c_int, [c_vp]),
     "hsb_average_m_noalloc": (c_int, [c_vp, c_i64, c_vp, c_vp]),
     "hsb_set_stage_variant": (c_int, [c_int]),
     "hsb_stage_variant_of": (c_int, [c_vp]),

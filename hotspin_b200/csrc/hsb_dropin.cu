@@ -309,8 +309,7 @@ HSB_EXPORT void long_field_async(double* hx, double* hy, double* hz, double* mx,
     check_launch("long_field_async");
 }
 
-// Ridders root bracket exactly as findroot_Ridders (brillouin.cu:13-71) on
-// f(n) = W(pre n) - n.
+// The self-consistency model of brillouinKern: f(n) = W(pre n) - n.
 __device__ double d_model(double nn, double J, double pre) {
     const double x = pre * nn;
     return ((J > HSB_INF_SPIN) ? d_L(x) : d_Bj(J, x)) - nn;
@@ -321,17 +320,22 @@ __device__ double d_sign(double x) {
     return (x == 0.0) ? 0.0 : v;
 }
 
-__device__ double d_ridders(double J, double pre, double xa, double xb) {
-    const double ya = d_model(xa, J, pre);
+// Ridders bracketing root search of findroot_Ridders (brillouin.cu:13-71) on any model f:
+// the same midpoint / exponential-correction update, bracket bookkeeping, 1e10 seeds, the
+// relative-change stop at 1e-8 and the 1000-iteration cap, so the roots (m_e(T) here, the spin
+// temperature in tsAsync) equal the reference's to the last bit where the models agree.
+template <typename F>
+__device__ double d_ridders(const F& f, double xa, double xb) {
+    const double ya = f(xa);
     if (fabs(ya) < HSB_ZERO) return xa;
-    const double yb = d_model(xb, J, pre);
+    const double yb = f(xb);
     if (fabs(yb) < HSB_ZERO) return xb;
     double y1 = ya, x1 = xa, y2 = yb, x2 = xb;
     double x = 1.0e10, tx = x, teps = x;
     int iter = 0;
     while (teps > 1.0e-8 && iter < 1000) {
         const double x3 = 0.5 * (x2 + x1);
-        const double y3 = d_model(x3, J, pre);
+        const double y3 = f(x3);
         const double dy = (y3 * y3 - y1 * y2);
         if (dy == 0.0) {
             x = x3;
@@ -339,7 +343,7 @@ __device__ double d_ridders(double J, double pre, double xa, double xb) {
         }
         const double dx = (x3 - x1) * d_sign(y1 - y2) * y3 / (sqrt(dy));
         x = x3 + dx;
-        const double y = d_model(x, J, pre);
+        const double y = f(x);
         const bool s3 = signbit(y) == signbit(y3);
         y2 = s3 ? y2 : y3;
         x2 = s3 ? x2 : x3;
@@ -370,7 +374,7 @@ __global__ void d_brillouin(double* msat0, const double* ms0T0m, const double* T
         const double dT = (Tc - Temp) / Tc;
         const double lo = (dT < 0.0004) ? -0.1 : 0.01;
         const double hi = (dT < 0.0004) ? 0.5 : 1.1;
-        const double me = d_ridders(Sp, pre, lo, hi);
+        const double me = d_ridders([&](double nn) { return d_model(nn, Sp, pre); }, lo, hi);
         msat0[i] = ms0T0 * fabs(me) / msat0Mul;
     }
 }
@@ -828,7 +832,8 @@ __global__ void d_mfa_table(double Tc, double J, int n, double* T, double* me, d
         } else if (t < Tc) {
             const double pre = 3.0 * preS * (Tc / t);
             const double dT = (Tc - t) / Tc;
-            m = fabs(d_ridders(J, pre, dT < 0.0004 ? -0.1 : 0.01, dT < 0.0004 ? 0.5 : 1.1));
+            m = fabs(d_ridders([&](double nn) { return d_model(nn, J, pre); }, dT < 0.0004 ? -0.1 : 0.01,
+                               dT < 0.0004 ? 0.5 : 1.1));
             const double b = preS * 3.0 * Tc / t;
             double f = (J > HSB_INF_SPIN) ? d_dLdx(m * b) : d_dBjdx(J, m * b);
             f = b * f;
@@ -893,40 +898,6 @@ __device__ double d_ts_model(double T, double S_, double pre, double m) {
     return d_Bj(S_, x) - m;
 }
 
-__device__ double d_ridders_ts(double S_, double pre, double m, double xa, double xb) {
-    const double ya = d_ts_model(xa, S_, pre, m);
-    if (fabs(ya) < HSB_ZERO) return xa;
-    const double yb = d_ts_model(xb, S_, pre, m);
-    if (fabs(yb) < HSB_ZERO) return xb;
-    double y1 = ya, x1 = xa, y2 = yb, x2 = xb;
-    double x = 1.0e10, tx = x, teps = x;
-    int iter = 0;
-    while (teps > 1.0e-8 && iter < 1000) {
-        const double x3 = 0.5 * (x2 + x1);
-        const double y3 = d_ts_model(x3, S_, pre, m);
-        const double dy = (y3 * y3 - y1 * y2);
-        if (dy == 0.0) {
-            x = x3;
-            break;
-        }
-        const double dx = (x3 - x1) * d_sign(y1 - y2) * y3 / (sqrt(dy));
-        x = x3 + dx;
-        const double y = d_ts_model(x, S_, pre, m);
-        const bool s3 = signbit(y) == signbit(y3);
-        y2 = s3 ? y2 : y3;
-        x2 = s3 ? x2 : x3;
-        const bool s1 = (signbit(y) == signbit(y1)) || x2 == x3;
-        y2 = s1 ? y2 : y1;
-        x2 = s1 ? x2 : x1;
-        y1 = y;
-        x1 = x;
-        teps = fabs((x - tx) / (tx + x));
-        tx = x;
-        iter++;
-    }
-    return x;
-}
-
 __global__ void d_ts(double* Ts, const double* msm, const double* ms0T0m, const double* Tcm, const double* Sm,
                      double msMul, double ms0T0Mul, double TcMul, double SMul, int n) {
     GRID_STRIDE(i, n) {
@@ -948,7 +919,8 @@ __global__ void d_ts(double* Ts, const double* msm, const double* ms0T0m, const 
         const double Sp = SMul * mu1(Sm, i);
         const double J0 = 3.0 * Tc / (Sp * (Sp + 1.0));
         const double m = ms / ms0T0;
-        Ts[i] = d_ridders_ts(Sp, Sp * Sp * J0 * m, m, 0.0, Tc);
+        const double pre = Sp * Sp * J0 * m;
+        Ts[i] = d_ridders([&](double T) { return d_ts_model(T, Sp, pre, m); }, 0.0, Tc);
     }
 }
 

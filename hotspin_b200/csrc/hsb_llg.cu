@@ -1021,6 +1021,9 @@ __global__ void k_dp45_control(HsbSolverDev* sd0, int nslot) {
     sd->err = finite ? err : INFINITY;
     sd->attempts += 1;
     if (!finite && h <= sd->mindt) sd->status |= 1;
+    // a step taken at the floor without meeting the tolerance (accepted because dt cannot
+    // shrink further; hotspin's rk12 accepts such steps the same way, solve_rk12.go:196-198)
+    if (finite && err > 1.0 && h <= sd->mindt) sd->status |= 2;
     if (accept) {
         sd->t += h;
         sd->step += 1;

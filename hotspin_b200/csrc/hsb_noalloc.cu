@@ -17,8 +17,6 @@
 //     call's contents afterwards;
 //   * calls that overlap on the GPU (two streams, or two host threads) race on it and give
 //     wrong results: serialise them.
-#include <mutex>
-
 #include "hsb_common.cuh"
 #include "hsb_reduce.cuh"
 
@@ -46,36 +44,26 @@ __global__ void k_average_m_static(const float* __restrict__ m, long n, double* 
     block_reduce_store<3>(v, partial, counter, out, gridDim.x, scale);
 }
 
-// Device address of the scratch on each device, resolved once per device with that
-// device current (host code cannot use the symbol itself as a device pointer).
-static std::mutex g_noalloc_mu;
-static double* g_noalloc_ptr[64];
-
+// Device address of the scratch in the current device's context (host code cannot use the
+// symbol itself as a device pointer).  Resolved on every call, with the caller's device
+// current: it is a host-side runtime query that allocates nothing, and a cached address
+// would go stale when the context is destroyed and recreated (cudaDeviceReset).
 static int noalloc_scratch(double** out) {
-    int dev = 0;
-    HSB_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) {
-        hsb_set_error("hsb_average_m_noalloc: device %d out of range", dev);
-        return HSB_ERR_INVALID;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        hsb_set_error("hsb_average_m_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        return HSB_ERR_CUDA;
     }
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            hsb_set_error("hsb_average_m_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-            return HSB_ERR_CUDA;
-        }
-        g_noalloc_ptr[dev] = (double*)p;
-    }
-    *out = g_noalloc_ptr[dev];
+    *out = (double*)p;
     return HSB_OK;
 }
 
 // avg3[c] = (1/ncell) * sum_i m[c * ncell + i] for c = 0, 1, 2, into caller-owned device
 // memory, enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream).
-// Allocates nothing.  The first call on a device resolves the scratch address (a host-side
-// runtime query, no allocation); make that first call before any stream capture.
+// Allocates nothing.  Each call resolves the scratch address in the current context (a
+// host-side runtime query, no allocation); the first call on a device also loads the
+// library's device code there, so make that first call before any stream capture.
 HSB_EXPORT int hsb_average_m_noalloc(const float* m, int64_t ncell, double* avg3, void* stream) {
     if (!m || !avg3) {
         hsb_set_error("hsb_average_m_noalloc: null pointer");

@@ -131,6 +131,10 @@ struct hsb_sim_s {
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof;  // category, start, stop
     int launches;       // kernel launches of one attempt (counted while enqueuing)
+    int launches_g, launches_g1;  // kernels in the full graph and in the one-attempt graph
+    long long launch_total;       // kernels enqueued for stepping since creation
+    float* ckpt;                  // checkpoint: the state channels [nch][n] (device)
+    HsbSolverDev* ckpt_sd;        // checkpoint: the solver word (device)
 };
 
 enum { PROF_STAGE = 0, PROF_XFWD = 1, PROF_YZ = 2, PROF_XINV = 3, PROF_OTHER = 4, PROF_NCAT = 5 };
@@ -606,10 +610,15 @@ static int prepare(hsb_sim_s* S) {
     // ungated: the state's first-stage data are computed even when the run about to start is
     // already inactive (target reached), so `initialized` always describes the buffers
     if (S->d.thermal) {
-        if (S->demag) RC(run_demag(S, nullptr, 0, nullptr, 0, false));
+        if (S->demag) {
+            RC(run_demag(S, nullptr, 0, nullptr, 0, false));
+            S->launch_total += hsb_demag_nlaunch(S->demag);
+        }
     } else {
         float* hd = S->demag ? S->hd : nullptr;
         RC(run_demag(S, nullptr, 0, hd, -1, false));
+        if (S->demag) S->launch_total += hsb_demag_nlaunch(S->demag);
+        S->launch_total += 1;
         StageArgs A = empty_args();
         A.ungated = 1;
         A.ys = YC;
@@ -648,7 +657,9 @@ static int capture_attempts(hsb_sim_s* S, int attempts, cudaGraphExec_t* out) {
 
 static int build_graph(hsb_sim_s* S) {
     if (S->graph) return HSB_OK;
-    return capture_attempts(S, S->graph_steps, &S->graph);
+    const int rc = capture_attempts(S, S->graph_steps, &S->graph);
+    S->launches_g = S->launches;
+    return rc;
 }
 
 // The one-attempt graph (S->launches keeps the count of the full graph).
@@ -656,6 +667,7 @@ static int build_graph1(hsb_sim_s* S) {
     if (S->graph1) return HSB_OK;
     const long keep = S->launches;
     const int rc = capture_attempts(S, 1, &S->graph1);
+    S->launches_g1 = S->launches;
     S->launches = keep;
     return rc;
 }
@@ -706,6 +718,7 @@ static int advance(hsb_sim_s* S, int64_t nsteps, double t_stop) {
     S->sd_fresh = false;
     k_arm<<<1, 1, 0, S->st>>>(S->sd, (long long)nsteps, t_stop);
     HSB_CUDA_TRY(cudaGetLastError());
+    S->launch_total += 1;
     RC(prepare(S));
     RC(build_graph(S));
     const bool fixed_step = S->d.solver != SOLVER_DP45;
@@ -721,15 +734,18 @@ static int advance(hsb_sim_s* S, int64_t nsteps, double t_stop) {
             if (nsteps - launched >= G) {
                 HSB_CUDA_TRY(cudaGraphLaunch(S->graph, S->st));
                 launched += G;
+                S->launch_total += S->launches_g;
             } else {
                 HSB_CUDA_TRY(cudaGraphLaunch(S->graph1, S->st));
                 launched += 1;
+                S->launch_total += S->launches_g1;
             }
             if (launched >= nsteps) break;
             continue;
         }
         HSB_CUDA_TRY(cudaGraphLaunch(short_run ? S->graph1 : S->graph, S->st));
         launched += short_run ? 1 : G;
+        S->launch_total += short_run ? S->launches_g1 : S->launches_g;
         // the whole solver word block (one round trip either way): current when the loop ends
         RC(get_sd(S));
         if (!S->sd_host->active) break;
@@ -885,6 +901,8 @@ static void free_sim(hsb_sim_s* S) {
     cudaFree(S->bext_tab);
     cudaFree(S->stage_f);
     cudaFree(S->stage_d);
+    cudaFree(S->ckpt);
+    cudaFree(S->ckpt_sd);
     if (S->sd_host) cudaFreeHost(S->sd_host);
     if (S->stage_pin) cudaFreeHost(S->stage_pin);
     if (S->red_host) cudaFreeHost(S->red_host);
@@ -1175,13 +1193,20 @@ HSB_EXPORT int hsb_sim_set(hsb_sim_s* S, const char* name, const double* host, i
         hsb_set_error("hsb_sim_set(%s): expected %ld values, got %ld", name, (long)nc * S->n, (long)count);
         return HSB_ERR_INVALID;
     }
-    RC(get_sd(S));
+    if (!S->sd_fresh) RC(get_sd(S));   // the current buffer index
     float* y = S->y[S->sd_host->cur];
+    // one copy (a DMA straight from the caller's array when it is page-locked) and one
+    // conversion, then a single synchronisation so the caller may reuse its array on return
     HSB_CUDA_TRY(cudaMemcpyAsync(S->stage_d, host, sizeof(double) * count, cudaMemcpyHostToDevice, S->st));
     k_d2f<<<hsb_grid_1d(count, 256), 256, 0, S->st>>>(S->stage_d, y + (long)first * S->n, count);
     HSB_CUDA_TRY(cudaGetLastError());
     S->initialized = false;
+    if (S->sd_host->status) {       // the flags described the state just replaced
+        S->sd_host->status = 0;
+        RC(set_sd_fields(S));
+    }
     HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
+    S->sd_fresh = true;    // the device words equal the host mirror
     return HSB_OK;
 }
 
@@ -1192,7 +1217,7 @@ HSB_EXPORT int hsb_sim_get(hsb_sim_s* S, const char* name, double* host, int64_t
         return HSB_ERR_INVALID;
     }
     RC(stage_buffers(S, count));
-    RC(get_sd(S));
+    if (!S->sd_fresh) RC(get_sd(S));
     float* y = S->y[S->sd_host->cur];
     std::string s(name);
     const float* src = nullptr;
@@ -1348,6 +1373,55 @@ HSB_EXPORT int hsb_sim_profile(hsb_sim_s* S, int reps, double* out) {
     out[5] = launches;
     RC(get_sd(S));
     out[6] = (double)(S->sd_host->step - step0);
+    return HSB_OK;
+}
+
+// Device-side checkpoint of the whole solver position: the current state (every channel, FP32
+// as held) and the solver word (time, dt, counters, buffer selectors).  hsb_sim_restore puts
+// both back and recomputes the first-stage data of the restored state, so a run from a
+// restored checkpoint repeats the original continuation bit for bit (the thermal field's
+// Philox counter is the step count, restored with it).  The checkpoint buffer is allocated
+// by the first checkpoint.
+HSB_EXPORT int hsb_sim_checkpoint(hsb_sim_s* S) {
+    RC(plain_only(S, "hsb_sim_checkpoint"));
+    if (!S) return HSB_ERR_INVALID;
+    if (!S->ckpt) {
+        HSB_CUDA_TRY(cudaMalloc(&S->ckpt, sizeof(float) * S->nch * S->n));
+        HSB_CUDA_TRY(cudaMalloc(&S->ckpt_sd, sizeof(HsbSolverDev)));
+    }
+    if (!S->sd_fresh) RC(get_sd(S));
+    HSB_CUDA_TRY(cudaMemcpyAsync(S->ckpt, S->y[S->sd_host->cur], sizeof(float) * S->nch * S->n,
+                                 cudaMemcpyDeviceToDevice, S->st));
+    HSB_CUDA_TRY(cudaMemcpyAsync(S->ckpt_sd, S->sd, sizeof(HsbSolverDev), cudaMemcpyDeviceToDevice, S->st));
+    HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
+    return HSB_OK;
+}
+
+HSB_EXPORT int hsb_sim_restore(hsb_sim_s* S) {
+    RC(plain_only(S, "hsb_sim_restore"));
+    if (!S) return HSB_ERR_INVALID;
+    if (!S->ckpt) {
+        hsb_set_error("hsb_sim_restore: no checkpoint taken");
+        return HSB_ERR_INVALID;
+    }
+    HSB_CUDA_TRY(cudaMemcpyAsync(S->sd, S->ckpt_sd, sizeof(HsbSolverDev), cudaMemcpyDeviceToDevice, S->st));
+    RC(get_sd(S));
+    HSB_CUDA_TRY(cudaMemcpyAsync(S->y[S->sd_host->cur], S->ckpt, sizeof(float) * S->nch * S->n,
+                                 cudaMemcpyDeviceToDevice, S->st));
+    S->initialized = false;
+    RC(prepare(S));
+    HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
+    S->sd_fresh = false;
+    return HSB_OK;
+}
+
+// Kernels this handle has enqueued for stepping since its creation: the arming kernel of
+// each step or run call, the first-stage preparation and every kernel node of each graph
+// launch (gated attempts included).
+HSB_EXPORT int hsb_sim_launch_count(hsb_sim_s* S, int64_t* n) {
+    RC(plain_only(S, "hsb_sim_launch_count"));
+    if (!S || !n) return HSB_ERR_INVALID;
+    *n = S->launch_total;
     return HSB_OK;
 }
 

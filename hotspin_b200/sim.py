@@ -90,13 +90,19 @@ class Simulation:
         _lib.check(self._lib.hsb_sim_set(self._h, name.encode(), a.ctypes.data_as(_lib.c_dp), a.size),
                    "hsb_sim_set(%s)" % name)
 
-    def get(self, name):
+    def get(self, name, out=None):
+        """The quantity as a new float64 array, or written into ``out`` (C-contiguous float64
+        of the quantity's shape, e.g. a view of page-locked host memory)."""
         ncomp = {"m": 3, "H_demag": 3, "Te": 1, "Tl": 1}.get(name)
         if name == "k":
             ncomp = 5 if self.desc.ttm else 3
         if ncomp is None:
             raise KeyError(name)
-        out = np.empty((ncomp,) + self.size if ncomp > 1 else self.size, dtype=np.float64)
+        shape = (ncomp,) + self.size if ncomp > 1 else self.size
+        if out is None:
+            out = np.empty(shape, dtype=np.float64)
+        elif out.shape != shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be C-contiguous float64 of shape %s" % (shape,))
         _lib.check(self._lib.hsb_sim_get(self._h, name.encode(), out.ctypes.data_as(_lib.c_dp), out.size),
                    "hsb_sim_get(%s)" % name)
         return out
@@ -139,6 +145,20 @@ class Simulation:
         a = (ctypes.c_double * 3)()
         _lib.check(self._lib.hsb_sim_average_m(self._h, a), "hsb_sim_average_m")
         return np.array(list(a))
+
+    def checkpoint(self):
+        """Keep the current state and solver position on the device (see restore)."""
+        _lib.check(self._lib.hsb_sim_checkpoint(self._h), "hsb_sim_checkpoint")
+
+    def restore(self):
+        """Return to the last checkpoint; stepping then repeats the original continuation."""
+        _lib.check(self._lib.hsb_sim_restore(self._h), "hsb_sim_restore")
+
+    def launch_count(self):
+        """Kernels the handle has enqueued for stepping since creation."""
+        n = ctypes.c_int64()
+        _lib.check(self._lib.hsb_sim_launch_count(self._h, ctypes.byref(n)), "hsb_sim_launch_count")
+        return n.value
 
     def max_torque(self):
         """max over cells of |gamma (m x H_eff)| (1/s), reduced on the device."""

@@ -121,7 +121,8 @@ int hsb_sim_destroy(hsb_sim sim);
 /* Host <-> device state transfer in double.  name: "m" (3 N values), "Te", "Tl" (N),
  * "msat_mask", "lex_mask" (N; set before stepping, NULL host pointer clears the mask),
  * read-only "H_demag" (3 N, A/m, of the current state), "k" (3 N or 5 N, the right-hand
- * side of the current state). */
+ * side of the current state).  Setting a state quantity clears the status flags, which
+ * describe the state it replaces.  A page-locked host array is copied by DMA directly. */
 int hsb_sim_set(hsb_sim sim, const char* name, const double* host, int64_t count);
 int hsb_sim_get(hsb_sim sim, const char* name, double* host, int64_t count);
 
@@ -132,7 +133,8 @@ int hsb_sim_run_until(hsb_sim sim, double t);
 int hsb_sim_sync(hsb_sim sim);
 
 /* Solver bookkeeping: time, current dt, accepted steps, attempts, rejected attempts,
- * last error norm, status bits (1: non-finite state, 2: dt at mindt). */
+ * last error norm, status bits (1: non-finite state, 2: a step was taken at mindt without
+ * meeting the tolerance). */
 int hsb_sim_status(hsb_sim sim, double* t, double* dt, int64_t* steps, int64_t* attempts,
                    int64_t* rejects, double* err, int32_t* status);
 int hsb_sim_set_time(hsb_sim sim, double t, double dt);
@@ -155,6 +157,17 @@ int hsb_sim_max_torque(hsb_sim sim, double* out);
  * out[4] combine / step control, out[5] launches per attempt, out[6] accepted steps. */
 int hsb_sim_profile(hsb_sim sim, int reps, double* out7);
 int hsb_sim_launches_per_attempt(hsb_sim sim, int* n);
+/* Checkpoint / resume on the device (hotspin saves and reloads state through dump files,
+ * dump/writer.go:46-76; this keeps the FP32 state and the solver word in device memory):
+ * hsb_sim_checkpoint copies the current state and solver position (t, dt, counters) aside;
+ * hsb_sim_restore puts them back, after which stepping repeats the original continuation
+ * bit for bit (the thermal field's counter is restored with the step count). */
+int hsb_sim_checkpoint(hsb_sim sim);
+int hsb_sim_restore(hsb_sim sim);
+/* Kernels the handle has enqueued for stepping since creation (no reference counterpart):
+ * the arming kernel of each step / run call, the first-stage preparation and every kernel
+ * node of each graph launch, gated attempts included. */
+int hsb_sim_launch_count(hsb_sim sim, int64_t* n);
 
 /* Mean-field tables in FP64 on the GPU: T_i = Tc i/(npts-1), m_e(T_i) by the Ridders
  * iteration of brillouinKern (src/libhotspin/brillouin.cu:88-138) and the reduced
@@ -169,8 +182,9 @@ int hsb_mfa_equilibrium(double T, double Tc, double J, double* me);
  * No counterpart in the reference: it is the device-finished FP64 reduction of
  * hsb_sim_average_m for callers that own all device memory (as hotspin's Go layer does),
  * with its scratch in a fixed static device array (about 7 KB per GPU, held until exit).
- * ncell must be in [1, 2^28]; larger sizes are rejected.  The first call on a device
- * resolves the scratch address (make it before any stream capture).  All calls share the
+ * ncell must be in [1, 2^28]; larger sizes are rejected.  Every call resolves the scratch
+ * address in the current context; the first call on a device also loads the library's
+ * device code there (make it before any stream capture).  All calls share the
  * scratch: calls that overlap on the GPU race and must be serialised. */
 int hsb_average_m_noalloc(const float* m, int64_t ncell, double* avg3, void* stream);
 

@@ -21,3 +21,8 @@ the reference's *program order* -- shape ``(N0, N1, N2)`` with N2 the fastest in
 is the user's x -- and vector fields are ``(3, N0, N1, N2)`` with component 0 the program X
 axis (user z).
 """
+import os
+
+# The reference checkout (read by the fixture script, the dump-file test and the build of
+# oracle/_ref); HOTSPIN_REF overrides the default location.
+REF_ROOT = os.environ.get("HOTSPIN_REF", "/root/reference")

@@ -2,10 +2,12 @@
 # sm_100a, into oracle/_ref/.  TEST INFRASTRUCTURE: the reference kernels are the parity and
 # timing baseline of the replayed reference path; nothing in the product links them.
 #
-#   make -f oracle/ref.mk            (needs the reference checkout at REF)
+#   make -f oracle/ref.mk            (needs the reference checkout: $HOTSPIN_REF, default
+#                                     /root/reference, or REF=<its src/libhotspin>)
 #
 # The flags are those of src/Make.inc with the gencode list replaced by sm_100a.
-REF  ?= /root/reference/src/libhotspin
+HOTSPIN_REF ?= /root/reference
+REF  ?= $(HOTSPIN_REF)/src/libhotspin
 OUT  ?= $(dir $(abspath $(lastword $(MAKEFILE_LIST))))_ref
 NVCC ?= nvcc
 ARCH  = -gencode arch=compute_100a,code=sm_100a

@@ -354,12 +354,15 @@ class RefSim:
 
 
 def bench_reference(args):
-    """bench.py --impl reference: the reference's kernels on the bench workload."""
+    """bench.py --impl reference: the reference's kernels on the bench workload, exactly the
+    driver's --warmup and --steps.  Nothing of the product library is loaded here: m_e(300 K)
+    of the initial state comes from the oracle's FP64 Ridders solve (oracle.fields)."""
     import json
 
     import torch
+
+    from . import fields
     rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     import bench as B
@@ -369,15 +372,15 @@ def bench_reference(args):
         return
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     kw = B.workload()
-    st0 = B.initial_state(kw)
+    st0 = B.initial_state(kw, fields.equilibrium_m(300.0, kw["tc"], kw["spin_j"]))
     sim = RefSim(kw, dt=2e-16)
     for k, v in st0.items():
         sim.set(k, v)
-    steps = max(1, min(args.steps, 50))
-    warm = max(1, min(args.warmup, 3))
+    steps, warm = args.steps, args.warmup
     for _ in range(warm):
         sim.step()
     torch.cuda.synchronize()
+    a0, r0 = sim.attempts, sim.rejects
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     e0.record()
@@ -392,11 +395,12 @@ def bench_reference(args):
     out = {"impl": "reference", "metric": B.METRIC, "value": round(value, 3), "unit": B.UNIT, "n_gpus": 1,
            "steps": steps, "warmup": warm, "ms_per_step": round(ms / steps, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "TTM+LLB 512x512x4 (demag 1024x1024x8), DP45 rtol 1e-5, thermal field",
-                      "cells": ncell, "attempts": sim.attempts, "rejected": sim.rejects,
-                      "path": "hotspin's own CUDA kernels (libhotspin.so built from the reference sources for "
-                              "sm_100a) driven by a replay of the Go updaters' call sequence with a stream sync "
-                              "after each call; cuFFT FP64; DP45 composed from the reference's madd kernels"},
+           "parallelism": "single", "config": B.run_config(kw),
+           "progress": {"attempts": sim.attempts - a0, "rejected": sim.rejects - r0,
+                        "sim_time_ps_at_end": round(sim.t * 1e12, 4)},
+           "path": "hotspin's own CUDA kernels (libhotspin.so built from the reference sources for sm_100a) "
+                   "driven by a replay of the Go updaters' call sequence with a stream sync after each call; "
+                   "cuFFT FP64; DP45 composed from the reference's madd kernels",
            "cpu_baseline": {"value": round(value, 3), "unit": B.UNIT, "cores": 1, "kind": "reference",
                             "sample": "%d accepted DP45 steps of the full workload on the reference's own "
                                       "GPU kernels (the reference has no CPU implementation of this path)"

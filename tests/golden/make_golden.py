@@ -1,6 +1,6 @@
 """Extract subsampled golden fixtures from the reference's test dumps and pin the oracle.
 
-Run in a container that has the reference checkout (``/root/reference``):
+Run in a container that has the reference checkout (``$HOTSPIN_REF``, default ``/root/reference``):
 
     python tests/golden/make_golden.py
 
@@ -28,10 +28,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
-from oracle import demag, fields, native  # noqa: E402
+from oracle import REF_ROOT, demag, fields, native  # noqa: E402
 from oracle.dump import read_dump  # noqa: E402
 
-REF = "/root/reference/tests"
+REF = os.path.join(REF_ROOT, "tests")
 N = 64
 MU0_PY = 1.25663706e-6        # the Python client's mu0 (src/python/hotspin.py.tail:4)
 CELL_PROGRAM = (64e-9 / N, 160e-9 / N, 320e-9 / N)   # (z, y, x) user -> program order

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from hotspin_b200 import dump
+from oracle import REF_ROOT
 from oracle import dump as odump
 
 
@@ -47,7 +48,7 @@ def test_corrupted_frame_is_refused(tmp_path):
         dump.read(p)
 
 
-REF_DUMPS = sorted(glob.glob("/root/reference/tests/*/*.dump"))
+REF_DUMPS = sorted(glob.glob(os.path.join(REF_ROOT, "tests", "*", "*.dump")))
 
 
 @pytest.mark.skipif(not REF_DUMPS, reason="the reference checkout is not present")

@@ -55,7 +55,7 @@ CASES = {
                 alpha=(0.1,) * 3, ku=7e6, anis_u=(1.0, 0.0, 0.0), demag=True, llb=True, tc=700.0, spin_j=0.5,
                 n_spins=1.1e6 / (2 * MUB * 0.5), temperature=300.0),
         init=lambda size: {"m": _tilted(size, 5.0, 2, F.equilibrium_m(300.0, 700.0, 0.5))},
-        solver="dp45", dt=1e-16, t_end=1e-12, tol_m=1e-4, tol_e=1e-3),
+        solver="dp45", dt=1e-16, t_end=1e-12, tol_m=1e-5, tol_e=5e-4),
     # two-temperature model + LLB with the laser pulse, DP45 1e-5
     "ttm_llb_laser_dp45": dict(
         kw=dict(size=(4, 32, 32), cellsize=(4e-9,) * 3, msat0T0=8e5, lex=_lex(8e5, 1.3e-11),
@@ -65,13 +65,13 @@ CASES = {
                 laser_sigma=40e-9),
         init=lambda size: dict(m=_tilted(size, 5.0, 3, F.equilibrium_m(300.0, 630.0, 0.5)),
                                Te=np.full(size, 300.0), Tl=np.full(size, 300.0)),
-        solver="dp45", dt=2e-16, t_end=5e-13, tol_m=1e-4, tol_e=1e-3),
+        solver="dp45", dt=2e-16, t_end=5e-13, tol_m=1e-5, tol_e=1e-5),
     # large-instance LLG physics on the multi-pass FFT path (L0 = 64), RK4 20 fs, alpha 0.5
     "llg_multipass_rk4": dict(
         kw=dict(size=(32, 16, 16), cellsize=(2e-9,) * 3, msat0T0=8e5, lex=_lex(8e5, 1.3e-11),
                 gamma_ll=F.GAMMA0 / (1 + 0.5 ** 2), alpha=(0.5,) * 3, demag=True, normalize=True),
         init=lambda size: {"m": _random_unit(size, 5)},
-        solver="rk4", dt=20e-15, steps=100, tol_m=1e-4, tol_e=1e-4),
+        solver="rk4", dt=20e-15, steps=100, tol_m=1e-5, tol_e=1e-5),
 }
 
 

@@ -146,7 +146,7 @@ def test_fixed_step_trajectory(cuda, method):
         st = sim.status()
         m = sim.get("m")
     assert st["steps"] == 25 and st["t"] == pytest.approx(25 * 2e-14, rel=1e-12)
-    assert np.abs(m - it.y["m"]).max() < 2e-5
+    assert np.abs(m - it.y["m"]).max() < 1e-5
 
 
 def test_rk4_smooth_4000_steps_parity(cuda):
@@ -176,10 +176,10 @@ def test_dp45_matches_oracle(cuda, kw):
     kw = dict(kw, thermal=False)
     spec, desc = pair(**kw)
     y = state(kw, seed=11)
-    it = Integrator(Model(spec), y, "dp45", 1e-15, rtol=1e-4, mindt=1e-20, maxdt=1e-12)
+    it = Integrator(Model(spec), y, "dp45", 1e-15, rtol=1e-5, mindt=1e-20, maxdt=1e-12)
     t_end = 2e-13
     it.run_until(t_end)
-    with Simulation(**desc, solver="dp45", dt=1e-15, rtol=1e-4, mindt=1e-20, maxdt=1e-12) as sim:
+    with Simulation(**desc, solver="dp45", dt=1e-15, rtol=1e-5, mindt=1e-20, maxdt=1e-12) as sim:
         for name, v in y.items():
             sim.set(name, v)
         sim.run_until(t_end)
@@ -188,9 +188,9 @@ def test_dp45_matches_oracle(cuda, kw):
         T = sim.get("Te") if kw.get("ttm") else None
     assert st["t"] == pytest.approx(t_end, rel=1e-9)
     assert abs(st["steps"] - it.step_count) <= max(2, it.step_count // 10)
-    assert np.abs(m - it.y["m"]).max() < 2e-4
+    assert np.abs(m - it.y["m"]).max() < 1e-5
     if T is not None:
-        assert rel_err(T, it.y["Te"]) < 1e-4
+        assert rel_err(T, it.y["Te"]) < 1e-5
 
 
 def test_thermal_field_statistics(cuda):
@@ -333,15 +333,15 @@ def test_pointwise_laser_profile(cuda):
             want = model.rhs(t, y)
             assert rel_err(k[3], want["Te"]) < 3e-5, t
             assert rel_err(k[:3], want["m"]) < 3e-5, t
-    it = Integrator(Model(spec), y, "dp45", 1e-15, rtol=1e-4, mindt=1e-20, maxdt=1e-12)
+    it = Integrator(Model(spec), y, "dp45", 1e-15, rtol=1e-5, mindt=1e-20, maxdt=1e-12)
     it.run_until(2e-13)
-    with Simulation(**desc, solver="dp45", dt=1e-15, rtol=1e-4, mindt=1e-20, maxdt=1e-12) as sim:
+    with Simulation(**desc, solver="dp45", dt=1e-15, rtol=1e-5, mindt=1e-20, maxdt=1e-12) as sim:
         for name, v in y.items():
             sim.set(name, v)
         sim.run_until(2e-13)
         m, T = sim.get("m"), sim.get("Te")
-    assert np.abs(m - it.y["m"]).max() < 2e-4
-    assert rel_err(T, it.y["Te"]) < 1e-4
+    assert np.abs(m - it.y["m"]).max() < 1e-5
+    assert rel_err(T, it.y["Te"]) < 1e-5
     with pytest.raises(_lib.HsbError, match="batches"):
         Batch(2, **dict(desc, size=(2, 16, 32)), solver="dp45", dt=1e-15)
 
