@@ -38,7 +38,7 @@ class SimDesc(ctypes.Structure):
         ("k_l", c_dbl), ("laser_p0", c_dbl), ("laser_t0", c_dbl), ("laser_fwhm", c_dbl),
         ("laser_sigma", c_dbl), ("solver", c_i32), ("dt", c_dbl), ("rtol", c_dbl),
         ("mindt", c_dbl), ("maxdt", c_dbl), ("laser_table", ctypes.POINTER(c_dbl)), ("laser_npts", c_i32),
-        ("bext_table", ctypes.POINTER(c_dbl)), ("bext_npts", c_i32),
+        ("bext_table", ctypes.POINTER(c_dbl)), ("bext_npts", c_i32), ("maxerr", c_dbl * 3),
     ]
 
 

@@ -222,6 +222,31 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned int* a, float v) {
     atomicMax(a, __float_as_uint(v));
 }
 
+// Per-equation absolute error of one cell (err_abs mode, hotspin's rk12 estimate
+// dt max |k1 - k0|): eeq[0] over the three m components, eeq[1], eeq[2] for Te, Tl.
+template <int CH, int W = 1>
+__device__ __forceinline__ void err_abs_cell(const float (&e)[CH], float fdt, float (&eeq)[3], bool& bad) {
+    float em = fmaxf(fabsf(e[0]), fmaxf(fabsf(e[1]), fabsf(e[2]))) * fdt;
+    if (!(e[0] == e[0]) || !(e[1] == e[1]) || !(e[2] == e[2])) bad = true;
+    eeq[0] = fmaxf(eeq[0], em);
+#pragma unroll
+    for (int c = 3; c < CH; c++) {
+        const float ec = fabsf(e[c]) * fdt;
+        if (!(ec == ec)) bad = true;
+        eeq[c - 2] = fmaxf(eeq[c - 2], ec);
+    }
+}
+
+// Warp maxima of the per-equation errors into the solver word.
+template <int CH>
+__device__ __forceinline__ void err_abs_store(float (&eeq)[3], HsbSolverDev* sd) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const float v = warp_max_f(eeq[q]);
+        if ((threadIdx.x & 31) == 0 && (q == 0 || q + 2 < CH)) atomic_max_nonneg(&sd->err_eq[q], v);
+    }
+}
+
 template <int CH>
 __global__ void __launch_bounds__(256) k_stage(const HsbPhys P, const StageArgs A, HsbSolverDev* sd) {
     if (!A.ungated && !sd->active) return;
@@ -243,6 +268,7 @@ __global__ void __launch_bounds__(256) k_stage(const HsbPhys P, const StageArgs 
     const float fdt = (float)dt;
     const long n = P.ncell;
     float emax = 0.f;
+    float eeq[3] = {0.f, 0.f, 0.f};
     bool bad = false;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         const int a2 = (int)(i % P.N2);
@@ -297,20 +323,28 @@ __global__ void __launch_bounds__(256) k_stage(const HsbPhys P, const StageArgs 
                     for (int c = 0; c < CH; c++) e[c] += A.ce[j] * __ldg(kin[j] + c * n + i);
                 }
             }
-            float em = fmaxf(fabsf(e[0]), fmaxf(fabsf(e[1]), fabsf(e[2]))) * fdt / A.rtol;
+            if (A.err_abs) {
+                err_abs_cell<CH>(e, fdt, eeq, bad);
+            } else {
+                float em = fmaxf(fabsf(e[0]), fmaxf(fabsf(e[1]), fabsf(e[2]))) * fdt / A.rtol;
 #pragma unroll
-            for (int c = 3; c < CH; c++) {
-                const float sc = A.rtol * fmaxf(fabsf(__ldg(yerr0 + c * n + i)), fabsf(y[c]));
-                const float ec = fabsf(e[c]) * fdt;
-                em = fmaxf(em, sc > 0.f ? ec / sc : (ec > 0.f ? INFINITY : 0.f));
+                for (int c = 3; c < CH; c++) {
+                    const float sc = A.rtol * fmaxf(fabsf(__ldg(yerr0 + c * n + i)), fabsf(y[c]));
+                    const float ec = fabsf(e[c]) * fdt;
+                    em = fmaxf(em, sc > 0.f ? ec / sc : (ec > 0.f ? INFINITY : 0.f));
+                }
+                if (!(em == em)) bad = true;   // NaN
+                emax = fmaxf(emax, em);
             }
-            if (!(em == em)) bad = true;   // NaN
-            emax = fmaxf(emax, em);
         }
     }
     if (A.err) {
-        emax = warp_max_f(emax);
-        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&sd->err_acc, emax);
+        if (A.err_abs) {
+            err_abs_store<CH>(eeq, sd);
+        } else {
+            emax = warp_max_f(emax);
+            if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&sd->err_acc, emax);
+        }
     }
     if (bad) atomicOr(&sd->nonfinite, 1u);
 }
@@ -367,6 +401,7 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const __grid_constant__ HsbPh
     float hb[3];
     hsb_bext(P, ts, hb);
     float emax = 0.f;
+    float eeq[3] = {0.f, 0.f, 0.f};
     bool bad = false;
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < ngroups; g += (long)gridDim.x * blockDim.x) {
         const long i = g << 2;
@@ -586,6 +621,15 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const __grid_constant__ HsbPh
                     }
                 }
             }
+            if (A.err_abs) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    float ec[CH];
+#pragma unroll
+                    for (int c = 0; c < CH; c++) ec[c] = e[c][q];
+                    err_abs_cell<CH>(ec, fdt, eeq, bad);
+                }
+            } else {
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 float em = fmaxf(fabsf(e[0][q]), fmaxf(fabsf(e[1][q]), fabsf(e[2][q]))) * fdt / A.rtol;
@@ -607,11 +651,16 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const __grid_constant__ HsbPh
                     }
                 }
             }
+            }
         }
     }
     if (A.err) {
-        emax = warp_max_f(emax);
-        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&sd->err_acc, emax);
+        if (A.err_abs) {
+            err_abs_store<CH>(eeq, sd);
+        } else {
+            emax = warp_max_f(emax);
+            if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&sd->err_acc, emax);
+        }
     }
     if (bad) atomicOr(&sd->nonfinite, 1u);
 }
@@ -1043,6 +1092,36 @@ __global__ void k_dp45_control(HsbSolverDev* sd0, int nslot) {
     sd->dt = nd;
 }
 
+// hotspin's adaptive Heun (rk12) step control, one thread per slot: consumes the attempt's
+// per-equation errors (hsb_rk12_rule in hsb_llg.cuh).
+struct Rk12Limits {
+    double maxerr[3];
+    int neq;
+};
+
+__global__ void k_rk12_control(HsbSolverDev* sd0, int nslot, const Rk12Limits lim) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslot) return;
+    HsbSolverDev* sd = sd0 + slot;
+    if (!sd->active) return;
+    float err[3];
+    for (int q = 0; q < 3; q++) {
+        err[q] = __uint_as_float(sd->err_eq[q]);
+        sd->err_eq[q] = 0u;
+    }
+    const bool nf = sd->nonfinite != 0u;
+    sd->nonfinite = 0u;
+    hsb_rk12_rule(*sd, err, lim.maxerr, lim.neq, nf);
+}
+
+int hsb_launch_rk12_control(HsbSolverDev* sd, int nslot, const double* maxerr, int neq, cudaStream_t st) {
+    Rk12Limits lim;
+    for (int q = 0; q < 3; q++) lim.maxerr[q] = maxerr[q];
+    lim.neq = neq;
+    k_rk12_control<<<(nslot + 31) / 32, 32, 0, st>>>(sd, nslot, lim);
+    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+}
+
 // Fixed-step bookkeeping: t += dt, step++, swap state buffers, stop at the target.
 __global__ void k_fixed_advance(HsbSolverDev* sd0, int nslot) {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1111,7 +1190,9 @@ static void launch_c(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, con
 template <int CH, bool BATCH>
 static void launch_vec(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt, int nslot,
                        cudaStream_t st, int variant) {
-    const int v = (A.err && (A.ynext.p[0] || A.ynext.p[1])) ? 0 : stage_variant(variant);
+    // the load-first kernel forms either the next state or the DP45 error norm: launches that
+    // need both, or the per-equation absolute errors, take the four-cell kernel
+    const int v = (A.err && (A.ynext.p[0] || A.ynext.p[1] || A.err_abs)) ? 0 : stage_variant(variant);
     if (v == 0) {
         const int threads = 256;
         long g = (P.ncell / 4 + threads - 1) / threads;

@@ -1,6 +1,7 @@
 // Fused right-hand side + Runge-Kutta stage kernel: shared declarations.
 #pragma once
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 // Maximum number of stored stages any integrator reads (Dormand-Prince: 7).
@@ -155,7 +156,77 @@ struct HsbSolverDev {
     unsigned int nonfinite;
     int prep;              // batched slots: 1 while the slot's first-stage data is being prepared
     int pad_;
+    unsigned int err_eq[3];  // rk12: float bits of the attempt's per-equation errors (m, Te, Tl)
+    int tries;             // rk12: rejected attempts of the current step
 };
+
+// Step-size rule of hotspin's adaptive Heun solver (solve_rk12.go:91-214), applied to one
+// solver word after an attempt.  err[q] = dt max_i |k1_i - k0_i| over the cells and
+// components of equation q (m, Te, Tl in this order; neq of them), maxerr[q] its
+// per-step limit (<m>_maxError; +inf leaves an equation uncontrolled), nonfinite the
+// attempt's non-finite flag.  The equations are visited in order with the reference's
+// running bad-step flag: a bad equation and every one after it take the cube-root factor,
+// the others the square root; factor x 0.8 clamped to [0.1, 1.5], the smallest over the
+// equations; dt_new = dt factor clamped to [mindt, maxdt].  The attempt is kept when no
+// equation was bad or dt_new is at mindt (status bit 2 if it was bad).  A step that still
+// fails after 10 retries sets status bit 4 and stops, where the reference panics.  A
+// non-finite attempt is rejected with the smallest factor; at mindt it sets status bit 1.
+// Host and device share this code.
+__host__ __device__ inline void hsb_rk12_rule(HsbSolverDev& sd, const float* err, const double* maxerr, int neq,
+                                             bool nonfinite) {
+    const double h = sd.dt;
+    bool finite = !nonfinite;
+    for (int q = 0; q < neq; q++) finite = finite && isfinite((double)err[q]);
+    bool bad = false;
+    double fmin = 2.0;
+    double emax = 0.0;
+    if (finite) {
+        for (int q = 0; q < neq; q++) {
+            const double e = (double)err[q];
+            const double r = maxerr[q] / e;            // inf when e == 0 or uncontrolled
+            if (e > maxerr[q]) bad = true;
+            double f = bad ? cbrt(r) : sqrt(r);
+            f *= 0.8;
+            if (f > 1.5) f = 1.5;
+            if (f < 0.1) f = 0.1;
+            if (f < fmin) fmin = f;
+            const double en = e / maxerr[q];
+            if (en > emax) emax = en;
+        }
+    } else {
+        fmin = 0.1;
+    }
+    double nd = h * fmin;
+    if (nd < sd.mindt) nd = sd.mindt;
+    if (nd > sd.maxdt) nd = sd.maxdt;
+    const bool accept = finite && (!bad || nd == sd.mindt);
+    sd.err = finite ? emax : INFINITY;
+    sd.attempts += 1;
+    if (!finite && h <= sd.mindt) sd.status |= 1;
+    if (accept) {
+        if (bad) sd.status |= 2;
+        sd.t += h;
+        sd.step += 1;
+        sd.cur = 1 - sd.cur;
+        sd.tries = 0;
+    } else {
+        sd.rejects += 1;
+        if (sd.tries > 10) {
+            sd.status |= 4;
+            sd.active = 0;
+        } else {
+            sd.tries += 1;
+        }
+    }
+    if (sd.t_stop > 0.0) {
+        const double rem = sd.t_stop - sd.t;
+        if (rem <= 1e-6 * nd || rem <= 0.0) sd.active = 0;
+        else if (nd > rem) nd = rem;
+    }
+    if (sd.step_stop >= 0 && sd.step >= sd.step_stop) sd.active = 0;
+    if (sd.status & 1) sd.active = 0;
+    sd.dt = nd;
+}
 
 // Pointer selectors resolved on the device against HsbSolverDev.
 enum { SEL_FIXED = 0, SEL_CUR = 1, SEL_NEXT = 2, SEL_K1 = 3, SEL_K7 = 4 };
@@ -195,4 +266,7 @@ struct StageArgs {
     int hth_mode;
     PtrSel hth;              // [3][ncell]
     int torque_only;         // generic kernel only: k = gamma (m x H), without the relaxation term
+    // error mode: 0 = the DP45 norm (m: |e| / rtol, T: |e| / (rtol max(|T0|, |T|)), one
+    // maximum); 1 = per-equation absolute errors dt |e| into HsbSolverDev.err_eq (rk12)
+    int err_abs;
 };

@@ -34,6 +34,7 @@ int hsb_launch_combine_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDe
 int hsb_launch_dp45_control_batched(HsbSolverDev* sd, int nslot, cudaStream_t st);
 int hsb_launch_fixed_advance_batched(HsbSolverDev* sd, int nslot, cudaStream_t st);
 int hsb_launch_activate_prepped(HsbSolverDev* sd, int nslot, cudaStream_t st);
+int hsb_launch_rk12_control(HsbSolverDev* sd, int nslot, const double* maxerr, int neq, cudaStream_t st);
 
 // Mirror of the public descriptor (include/hotspin_b200.h).
 struct hsb_sim_desc {
@@ -59,9 +60,13 @@ struct hsb_sim_desc {
     int32_t laser_npts;
     const double* bext_table;    // 4 x bext_npts (t, Bx, By, Bz); copied at creation
     int32_t bext_npts;
+    double maxerr[3];            // rk12: per-step error limits of m, Te, Tl
 };
 
-enum { SOLVER_EULER = 0, SOLVER_HEUN = 1, SOLVER_RK4 = 2, SOLVER_DP45 = 3 };
+enum { SOLVER_EULER = 0, SOLVER_HEUN = 1, SOLVER_RK4 = 2, SOLVER_DP45 = 3, SOLVER_RK12 = 4 };
+
+// Solvers whose step size is chosen on the device (accept / reject per attempt).
+static inline bool adaptive_solver(int s) { return s == SOLVER_DP45 || s == SOLVER_RK12; }
 
 static const double MU0 = 4.0e-7 * M_PI;
 static const double KB = 1.38064881313131313e-23;
@@ -133,6 +138,7 @@ struct hsb_sim_s {
     int launches;       // kernel launches of one attempt (counted while enqueuing)
     int launches_g, launches_g1;  // kernels in the full graph and in the one-attempt graph
     long long launch_total;       // kernels enqueued for stepping since creation
+    double rk12_maxerr[3];        // rk12: per-step error limits (m, Te, Tl; +inf = uncontrolled)
     float* ckpt;                  // checkpoint: the state channels [nch][n] (device)
     HsbSolverDev* ckpt_sd;        // checkpoint: the solver word (device)
 };
@@ -590,6 +596,46 @@ static int enqueue_attempt(hsb_sim_s* S) {
             RC(timed(S, PROF_OTHER, [&] { return L_control(S); }));
             break;
         }
+        case SOLVER_RK12: {  // solve_rk12.go:91-214: Euler predictor, Heun corrector, error |k1 - k0| dt
+            RC(run_demag(S, nullptr, 0, hd, -1));
+            StageArgs A = empty_args();
+            A.ys = YC;
+            A.hd = fixed(hd);
+            A.ytherm = YC;
+            A.kout = fixed(S->k[0]);
+            A.kself_w = 1.0f;
+            A.ynext = fixed(ya);
+            A.ybase = YC;
+            A.cself = 1.0f;
+            A.normalize = norm;
+            thermal_keep(S, A, true);
+            RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
+            RC(run_demag(S, ya, -1, hd, -1));
+            StageArgs B = empty_args();
+            B.ys = fixed(ya);
+            B.hd = fixed(hd);
+            B.ytherm = YC;
+            B.tfrac = 1.0f;
+            B.ynext = YN;
+            B.ybase = fixed(ya);
+            B.nk = 1;
+            B.kin[0] = fixed(S->k[0]);
+            B.ck[0] = -0.5f;
+            B.cself = 0.5f;
+            B.normalize = norm;
+            B.err = 1;
+            B.err_abs = 1;
+            B.ce[0] = -1.0f;
+            B.ceself = 1.0f;
+            thermal_keep(S, B, false);
+            RC(timed(S, PROF_STAGE, [&] { return L_stage(S, B); }));
+            RC(timed(S, PROF_OTHER, [&] {
+                S->sd_fresh = false;
+                return hsb_launch_rk12_control(S->sd, S->batched ? S->nslot : 1, S->rk12_maxerr, S->nch == 5 ? 3 : 1,
+                                               S->st);
+            }));
+            break;
+        }
         default:
             hsb_set_error("unknown solver %d", S->d.solver);
             return HSB_ERR_INVALID;
@@ -691,6 +737,7 @@ static int plain_only(hsb_sim_s* S, const char* who) {
 // a non-finite state stays inactive (reported after the run); a time target already
 // reached leaves it inactive; dt is clipped to land on the target.
 __global__ void k_arm(HsbSolverDev* sd, long long nsteps, double t_stop) {
+    sd->tries = 0;
     if (sd->status & 1) {
         sd->active = 0;
         return;
@@ -721,7 +768,7 @@ static int advance(hsb_sim_s* S, int64_t nsteps, double t_stop) {
     S->launch_total += 1;
     RC(prepare(S));
     RC(build_graph(S));
-    const bool fixed_step = S->d.solver != SOLVER_DP45;
+    const bool fixed_step = !adaptive_solver(S->d.solver);
     const int G = S->graph_steps;
     // fewer steps than a graph holds (e.g. one step per call): one-attempt graphs, so no
     // launch carries attempts that the device would gate off
@@ -758,6 +805,10 @@ static int advance(hsb_sim_s* S, int64_t nsteps, double t_stop) {
     if (S->sd_host->status & 1) {
         hsb_set_error("state became non-finite at t = %g", S->sd_host->t);
         return HSB_ERR_NONFINITE;
+    }
+    if (S->sd_host->status & 4) {
+        hsb_set_error("rk12: the step at t = %g still exceeded maxerr after 10 retries", S->sd_host->t);
+        return HSB_ERR_SOLVER;
     }
     return HSB_OK;
 }
@@ -1002,6 +1053,14 @@ static int tune_stage(hsb_sim_s* S) {
     return HSB_OK;
 }
 
+// rk12 per-step error limits of the handle's equations (m, Te, Tl): maxerr[0] or rtol for
+// m; a temperature limit <= 0 leaves that equation uncontrolled (+inf).
+static void set_rk12_limits(hsb_sim_s* S) {
+    const hsb_sim_desc& d = S->d;
+    S->rk12_maxerr[0] = d.maxerr[0] > 0 ? d.maxerr[0] : d.rtol;
+    for (int q = 1; q < 3; q++) S->rk12_maxerr[q] = d.maxerr[q] > 0 ? d.maxerr[q] : INFINITY;
+}
+
 static int check_desc(const hsb_sim_desc& d, const char* who) {
     for (int a = 0; a < 3; a++) {
         if (d.size[a] < 1 || d.cellsize[a] <= 0 || d.pbc[a] < 0) {
@@ -1009,13 +1068,23 @@ static int check_desc(const hsb_sim_desc& d, const char* who) {
             return HSB_ERR_INVALID;
         }
     }
-    if (d.solver < SOLVER_EULER || d.solver > SOLVER_DP45) {
+    if (d.solver < SOLVER_EULER || d.solver > SOLVER_RK12) {
         hsb_set_error("%s: unknown solver %d", who, d.solver);
         return HSB_ERR_INVALID;
     }
     if (!(d.dt > 0) || !(d.msat0T0 > 0) || (d.solver == SOLVER_DP45 && !(d.rtol > 0))) {
         hsb_set_error("%s: dt, msat0T0 (and rtol for DP45) must be positive", who);
         return HSB_ERR_INVALID;
+    }
+    if (d.solver == SOLVER_RK12 && !(d.maxerr[0] > 0) && !(d.rtol > 0)) {
+        hsb_set_error("%s: rk12 needs maxerr[0] (or rtol) > 0", who);
+        return HSB_ERR_INVALID;
+    }
+    for (int q = 0; q < 3; q++) {
+        if (isnan(d.maxerr[q])) {
+            hsb_set_error("%s: maxerr[%d] is not a number", who, q);
+            return HSB_ERR_INVALID;
+        }
     }
     if (d.llb && !(d.tc > 0 && d.spin_j > 0 && d.n_spins > 0)) {
         hsb_set_error("%s: llb needs tc, spin_j and n_spins > 0", who);
@@ -1127,7 +1196,8 @@ HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     STRY(cudaStreamSynchronize(S->st));
     // launch-bound grids batch more steps per graph launch
     S->graph_steps = n < 65536 ? 16 : (n < 1048576 ? 8 : 4);
-    if (d.solver == SOLVER_DP45) S->graph_steps = n < 65536 ? 8 : 4;
+    if (adaptive_solver(d.solver)) S->graph_steps = n < 65536 ? 8 : 4;
+    set_rk12_limits(S);
     *out = S;
     return HSB_OK;
 }
@@ -1273,7 +1343,7 @@ HSB_EXPORT int hsb_sim_run_until(hsb_sim_s* S, double t) {
         hsb_set_error("hsb_sim_run_until: null handle");
         return HSB_ERR_INVALID;
     }
-    if (S->d.solver != SOLVER_DP45) {
+    if (!adaptive_solver(S->d.solver)) {
         RC(get_sd(S));
         const double rem = t - S->sd_host->t;
         if (rem <= 0) return HSB_OK;
@@ -1639,7 +1709,8 @@ HSB_EXPORT int hsb_batch_create(const hsb_sim_desc* cls, int32_t nslot, hsb_sim_
     S->bt.nslot = nslot;
     const long tot = n * nslot;
     S->graph_steps = tot < 65536 ? 16 : (tot < 1048576 ? 8 : 4);
-    if (d.solver == SOLVER_DP45) S->graph_steps = tot < 65536 ? 8 : 4;
+    if (adaptive_solver(d.solver)) S->graph_steps = tot < 65536 ? 8 : 4;
+    set_rk12_limits(S);
     S->initialized = true;
     {
         // tune with a valid dt in every solver word, then clear them again (all slots empty)
@@ -1695,7 +1766,9 @@ HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* d
         }
     }
     if (d.solver != c.solver || d.ttm != c.ttm || d.demag != c.demag || (d.thermal && !c.thermal) ||
-        (c.solver == SOLVER_DP45 && d.rtol != c.rtol)) {
+        (adaptive_solver(c.solver) && d.rtol != c.rtol) ||
+        (c.solver == SOLVER_RK12 &&
+         (d.maxerr[0] != c.maxerr[0] || d.maxerr[1] != c.maxerr[1] || d.maxerr[2] != c.maxerr[2]))) {
         hsb_set_error("hsb_batch_admit: solver, tolerance, two-temperature model, demag or thermal field differ "
                       "from the class");
         return HSB_ERR_INVALID;

@@ -45,7 +45,7 @@ enum {
     HSB_ERR_SOLVER = 6
 };
 
-enum { HSB_SOLVER_EULER = 0, HSB_SOLVER_HEUN = 1, HSB_SOLVER_RK4 = 2, HSB_SOLVER_DP45 = 3 };
+enum { HSB_SOLVER_EULER = 0, HSB_SOLVER_HEUN = 1, HSB_SOLVER_RK4 = 2, HSB_SOLVER_DP45 = 3, HSB_SOLVER_RK12 = 4 };
 
 /* Simulation description.  Replaces the module graph a hotspin script builds with
  * load(...)/setv(...): exchange6, anisotropy/uniaxial, zeeman, demag, llbar +
@@ -84,7 +84,7 @@ typedef struct hsb_sim_desc {
     int32_t solver;         /* HSB_SOLVER_*                                        */
     double dt;              /* initial / fixed time step, s                        */
     double rtol;            /* DP45 tolerance                                      */
-    double mindt, maxdt;    /* DP45 step bounds                                    */
+    double mindt, maxdt;    /* DP45 / RK12 step bounds                             */
     /* Pointwise laser time profile (hotspin's PointwiseOf quantities,
      * engine/update_pointwiseof.go:31-98): laser_npts >= 2 pairs (t_i in s, strictly
      * increasing; factor_i) as 2 * laser_npts doubles; the absorbed power is laser_p0 times
@@ -99,6 +99,11 @@ typedef struct hsb_sim_desc {
      * constant b_ext.  Copied at creation; not available in batches.                     */
     const double* bext_table;
     int32_t bext_npts;      /* 0 or 2..4096                                          */
+    /* HSB_SOLVER_RK12 (hotspin's solver/rk12, solve_rk12.go:91-214): the largest error per
+     * step of each equation, dt max |k1 - k0| (<m>_maxError, <Te>_maxError, <Tl>_maxError).
+     * maxerr[0] <= 0 takes rtol; a temperature entry <= 0 leaves that equation
+     * uncontrolled.                                                                     */
+    double maxerr[3];
 } hsb_sim_desc;
 
 typedef struct hsb_sim_s* hsb_sim;
@@ -134,7 +139,8 @@ int hsb_sim_sync(hsb_sim sim);
 
 /* Solver bookkeeping: time, current dt, accepted steps, attempts, rejected attempts,
  * last error norm, status bits (1: non-finite state, 2: a step was taken at mindt without
- * meeting the tolerance). */
+ * meeting the tolerance, 4: an RK12 step still failed after 10 retries, where hotspin
+ * panics; the run stops with HSB_ERR_SOLVER). */
 int hsb_sim_status(hsb_sim sim, double* t, double* dt, int64_t* steps, int64_t* attempts,
                    int64_t* rejects, double* err, int32_t* status);
 int hsb_sim_set_time(hsb_sim sim, double t, double dt);

@@ -59,6 +59,8 @@ _SIGS = {
     "QinterAsync": [P, P, P, P, D, I, P],
     "divAsync": [P, P, P, P, I],
     "partialMaxAbsAsync": [P, P, I, I, I, P],
+    "partialMaxDiffAsync": [P, P, P, I, I, I, P],
+    "madd2Async": [P, P, D, P, D, P, I],
     "normalizeAsync": [P, P, P, P, I],
 }
 
@@ -306,6 +308,76 @@ class RefSim:
             if c != 0.0:
                 L.madd1Async(p(dst), p(kj), D(h * c), s, I(nn))
         self.sync()
+
+    def _maxdiff(self, a, b):
+        """max |a - b| as gpu.Reductor.MaxDiff (reductor.go:141-154): partialMaxDiffAsync, then
+        the host finishes the block maxima.  512 threads per block: at 1024 (what the Go
+        reductor picks on this GPU) the kernel's first shared-memory fold reads
+        sdata[tid + 256] where it needs sdata[tid + 512] (reduce.cu, _gpu_maxdiff_kernel), so
+        the upper half of each block never enters the maximum."""
+        L, p, s = self.lib, self.p, self.sh
+        nn = a.numel()
+        threads = 512
+        while nn <= threads:
+            threads //= 2
+        blocks = (nn + 2 * threads - 1) // (2 * threads)
+        if self.part.numel() < blocks:
+            self.part = self.torch.zeros(blocks, dtype=self.torch.float64, device="cuda")
+        L.partialMaxDiffAsync(p(a), p(b), p(self.part), I(blocks), I(threads), I(nn), s)
+        self.stream.synchronize()
+        return float(self.part[:blocks].max().item())
+
+    def _normalize(self, y):
+        """The normalizer module's in-place renormalisation of m (mod_normalize.go:45-55)."""
+        if self.kw.get("normalize"):
+            self.lib.normalizeAsync(self.p(y[0]), self.p(y[1]), self.p(y[2]), self.sh, I(self.n))
+            self.sync()
+
+    def step_rk12(self, maxerr):
+        """One step of hotspin's adaptive Heun solver (solve_rk12.go:91-214) on the reference
+        kernels: inputs updated (m renormalised, dy0 = f(y0)), y0 and dy0 kept; per attempt
+        the Euler predictor y = y0 + dt dy0 (Madd), m renormalised by its update, dy1 at
+        t0 + dt, the corrector y += dt/2 dy1 - dt/2 dy0 (madd2Async), and per equation
+        err = MaxDiff(dy1, dy0) dt; the step-size rule is the oracle's restatement of
+        solve_rk12.go:148-199 (oracle.solvers.rk12_rule).  maxerr: {"m": .., "Te": .., "Tl": ..},
+        a missing temperature limit leaving that equation uncontrolled.  Without a thermal
+        field (the reference redraws its noise at every update)."""
+        from .solvers import rk12_rule
+        L, p, s = self.lib, self.p, self.sh
+        assert not self.kw.get("thermal")
+        nn = self.nch * self.n
+        if not hasattr(self, "y0b"):
+            self.y0b = self.torch.zeros_like(self.y)
+        keys = [("m", slice(0, 3))] + ([("Te", slice(3, 4)), ("Tl", slice(4, 5))] if self.ttm else [])
+        limits = [maxerr.get(k, math.inf) for k, _ in keys]
+        t0 = self.t
+        self._normalize(self.y)
+        dy0, dy1 = self.k[0], self.k[1]
+        self.rhs(t0, self.y, dy0)
+        self.y0b.copy_(self.y)
+        self.sync()
+        tr = 0
+        while True:
+            dt = self.dt
+            L.maddAsync(p(self.y), p(self.y0b), p(dy0), D(dt), s, I(nn))
+            self.sync()
+            self._normalize(self.y)
+            self.rhs(t0 + dt, self.y, dy1)
+            L.madd2Async(p(self.y), p(dy1), D(0.5 * dt), p(dy0), D(-0.5 * dt), s, I(nn))
+            self.sync()
+            errs = [self._maxdiff(dy1[sl], dy0[sl]) * dt for _, sl in keys]
+            accept, bad, newdt, _ = rk12_rule(dt, errs, limits, self.mindt, self.maxdt)
+            self.attempts += 1
+            self.dt = newdt
+            if accept:
+                break
+            if tr > 10:
+                raise RuntimeError("The solver cannot converge after 10 badsteps")
+            self.rejects += 1
+            tr += 1
+        self._normalize(self.y)          # the next update of m renormalises it
+        self.t = t0 + dt
+        self.steps += 1
 
     def _maxabs(self, a):
         L, p, s = self.lib, self.p, self.sh

@@ -46,6 +46,25 @@ def _comb(y0, ks, coefs, h):
     return out
 
 
+def rk12_rule(dt, errs, limits, mindt, maxdt):
+    """The step-size rule of solve_rk12.go:148-199 for one attempt: errs[q] = dt max|k1 - k0|
+    of equation q, limits[q] its maxError, visited in order with the running bad-step flag.
+    Returns (accept, bad, dt_new, max errs[q] / limits[q])."""
+    bad = False
+    fmin = 2.0
+    emax = 0.0
+    for err, lim in zip(errs, limits):
+        if err > lim:
+            bad = True
+        r = lim / err if err > 0 else math.inf
+        fac = r ** (1.0 / 3.0) if bad else math.sqrt(r)
+        fac = min(max(fac * 0.8, 0.1), 1.5)
+        fmin = min(fmin, fac)
+        emax = max(emax, err / lim)
+    newdt = min(max(dt * fmin, mindt), maxdt)
+    return (not bad) or newdt == mindt, bad, newdt, emax
+
+
 class Integrator:
     """Drives a ``Model``.  ``y`` is a dict of arrays; ``t``, ``dt``, ``step`` as in the
     reference engine (engine/engine.go:473-508)."""
@@ -89,7 +108,7 @@ class Integrator:
     def run_until(self, t_end):
         """Step until t_end; adaptive steps are clamped to land on it (as the device does)."""
         while t_end - self.t > 1e-6 * self.dt:
-            if self.method == "dp45":
+            if self.method in ("dp45", "rk12"):
                 self.dt = min(self.dt, t_end - self.t)
             self.step()
 
@@ -112,35 +131,49 @@ class Integrator:
         self.y = self._fix(_comb(y1, [k1, k0], [0.5, -0.5], h))
         self.step_count += 1
 
+    def _rk12_limits(self):
+        """Per-equation error limits: a float applies to m (and to every equation when it is
+        the only limit given); a dict maps equation names (m, Te, Tl) to limits, a missing or
+        non-positive temperature entry leaving that equation uncontrolled."""
+        me = self.maxerr
+        if isinstance(me, dict):
+            return [(k, me.get(k, 0.0) if me.get(k, 0.0) > 0 else math.inf) for k in ("m", "Te", "Tl") if k in self.y]
+        return [(k, me) for k in ("m", "Te", "Tl") if k in self.y]
+
     def _rk12(self):
-        """solve_rk12.go:91-214 with a single maxError for all equations."""
+        """solve_rk12.go:91-214.  k0 = f(y0) once per step (the reference restores it on a
+        retry; recomputing gives the same values), Euler predictor y1 (renormalised),
+        Heun corrector y1 + dt/2 (k1 - k0); per equation err = dt max|k1 - k0|, visited in
+        the order m, Te, Tl with the reference's running bad-step flag (a bad equation and
+        every later one take the cube-root factor, the others the square root), factor x 0.8
+        clamped to [0.1, 1.5], the smallest over the equations; dt_new clamped to
+        [mindt, maxdt]; the attempt is kept when no equation was bad or dt_new == mindt;
+        the 12th bad attempt of a step raises, as the reference panics.  The thermal field
+        is drawn for each attempt with the attempt's dt (as the device does)."""
         f = self.model.rhs
         t0 = self.t
-        self._thermal(self.dt)
-        k0 = f(t0, self.y)
         y0 = self.y
-        for tr in range(11):
+        limits = self._rk12_limits()
+        tr = 0
+        while True:
             dt = self.dt
+            self._thermal(dt)
+            k0 = f(t0, y0)
             y1 = self._fix(_comb(y0, [k0], [1.0], dt))
             k1 = f(t0 + dt, y1)
             ynew = self._fix(_comb(y1, [k1, k0], [0.5, -0.5], dt))
-            err = max(float(np.abs(k1[key] - k0[key]).max()) for key in k0) * dt
-            bad = err > self.maxerr
-            if bad:
-                self.bad_steps += 1
-                factor = (self.maxerr / err) ** (1.0 / 3.0)
-            else:
-                factor = math.sqrt(self.maxerr / err) if err > 0 else 1.5 / 0.8
-            factor = min(max(factor * 0.8, 0.1), 1.5)
-            newdt = min(max(dt * factor, self.mindt), self.maxdt)
+            errs = [float(np.abs(k1[key] - k0[key]).max()) * dt for key, _ in limits]
+            accept, bad, newdt, emax = rk12_rule(dt, errs, [lim for _, lim in limits], self.mindt, self.maxdt)
             self.dt = newdt
-            self.last_err = err
-            if not bad or newdt == self.mindt:
+            self.last_err = emax
+            if accept:
                 self.y = ynew
                 self.t = t0 + dt
                 break
             if tr > 10:
                 raise RuntimeError("The solver cannot converge after 10 badsteps")
+            self.bad_steps += 1
+            tr += 1
         self.step_count += 1
 
     # -- new integrators ----------------------------------------------------------
