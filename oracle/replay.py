@@ -69,8 +69,10 @@ def available():
     return os.path.exists(REF_LIB)
 
 
-def load():
-    lib = ctypes.CDLL(REF_LIB)
+def load(path=None):
+    """The kernel library the replay drives: the reference's own build (default), or any
+    library exporting the same names, e.g. the product's FP64 drop-ins (libhsb200.so)."""
+    lib = ctypes.CDLL(path or REF_LIB)
     for name, args in _SIGS.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -81,11 +83,11 @@ def load():
 class RefSim:
     """One simulation driven through the reference kernels (FP64 device arrays)."""
 
-    def __init__(self, kw, dt, rtol=1e-5, mindt=1e-20, maxdt=1e-13, sync_each_call=True):
+    def __init__(self, kw, dt, rtol=1e-5, mindt=1e-20, maxdt=1e-13, sync_each_call=True, lib_path=None):
         import torch
         from . import demag, native
         self.torch = torch
-        self.lib = load()
+        self.lib = load(lib_path)
         self.kw = dict(kw)
         self.sync_each = sync_each_call
         self.size = tuple(kw["size"])

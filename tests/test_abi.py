@@ -111,3 +111,15 @@ def test_batches_refuse_what_they_do_not_support():
     assert b"batches" in lib.hsb_last_error()
     d = _desc(size=(1, 8, 8), solver="dp45")
     assert lib.hsb_batch_footprint(ctypes.byref(d), 0, ctypes.byref(nbytes)) == 1
+
+
+def test_dropins_export_every_name_the_go_sequence_replay_binds():
+    """oracle/replay.py binds these reference names through ctypes; libhsb200.so must export
+    each of them so the replay (and a Go build linking the drop-ins) can run on it."""
+    import ctypes
+
+    from hotspin_b200 import _lib
+    from oracle import replay
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in replay._SIGS if not hasattr(lib, n)]
+    assert not missing, missing
