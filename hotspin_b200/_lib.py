@@ -39,6 +39,7 @@ class SimDesc(ctypes.Structure):
         ("laser_sigma", c_dbl), ("solver", c_i32), ("dt", c_dbl), ("rtol", c_dbl),
         ("mindt", c_dbl), ("maxdt", c_dbl), ("laser_table", ctypes.POINTER(c_dbl)), ("laser_npts", c_i32),
         ("bext_table", ctypes.POINTER(c_dbl)), ("bext_npts", c_i32), ("maxerr", c_dbl * 3),
+        ("maxrelerr", c_dbl * 3), ("max_iter", c_i32),
     ]
 
 

@@ -13,8 +13,9 @@ Supported modules: exchange6, demag, zeeman, anisotropy/uniaxial, llbar, llbar/t
 llbar/damping/nonconservative/00/local, normalizer, mfa/longfield, mfa/msat0,
 temperature/brown, temperature/ETM, temperature/PTM, temperature/E-P, temperature/Drude,
 temperature/ETM/diffusion, solver/euler, solver/heun, solver/rk12 (errors per step set with
-setv('m_maxerror' / 'Te_maxerror' / 'Tp_maxerror', ...)), solver/rk4, solver/rk45,
-micromag/energy.  Anything else raises (no silent fallback).
+setv('m_maxerror' / 'Te_maxerror' / 'Tp_maxerror', ...)), solver/am12 ('<q>_maxabserror',
+'<q>_maxrelerror'), solver/bdf-euler ('m_maxitererror', 'm_maxiterations'), solver/rk4,
+solver/rk45, micromag/energy.  Anything else raises (no silent fallback).
 """
 import math
 
@@ -30,7 +31,7 @@ SUPPORTED = {
     "llbar/damping/nonconservative/00/local", "normalizer", "mfa/longfield", "mfa/msat0",
     "temperature/brown", "temperature/ETM", "temperature/PTM", "temperature/E-P",
     "temperature/Drude", "temperature/ETM/diffusion", "solver/euler", "solver/heun",
-    "solver/rk12", "solver/rk4", "solver/rk45", "micromag/energy",
+    "solver/rk12", "solver/am12", "solver/bdf-euler", "solver/rk4", "solver/rk45", "micromag/energy",
 }
 
 
@@ -171,13 +172,20 @@ class Engine:
         mods = self.modules
         msat = g("Msat0T0", g("msat0T0", 0.0))
         solver = "rk4"
-        for s in ("euler", "heun", "rk12", "rk4", "rk45"):
+        for s in ("euler", "heun", "rk12", "am12", "bdf-euler", "rk4", "rk45"):
             if "solver/" + s in mods:
                 solver = "dp45" if s == "rk45" else s
         # quantity names are matched without case, as the reference's engine does
         lv = {k.lower(): v for k, v in self.v.items()}
-        maxerr = (float(lv.get("m_maxerror", 0.0)), float(lv.get("te_maxerror", 0.0)),
-                  float(lv.get("tp_maxerror", lv.get("tl_maxerror", 0.0))))
+        per_eq = lambda suffix: (float(lv.get("m_" + suffix, 0.0)), float(lv.get("te_" + suffix, 0.0)),
+                                 float(lv.get("tp_" + suffix, lv.get("tl_" + suffix, 0.0))))
+        if solver == "am12":
+            maxerr, maxrelerr = per_eq("maxabserror"), per_eq("maxrelerror")
+        elif solver == "bdf-euler":
+            maxerr, maxrelerr = per_eq("maxitererror"), (0.0, 0.0, 0.0)
+        else:
+            maxerr, maxrelerr = per_eq("maxerror"), (0.0, 0.0, 0.0)
+        max_iter = int(lv.get("m_maxiterations", 0))
         d = dict(size=self.size, cellsize=self.cellsize, pbc=self.pbc, msat0T0=msat,
                  lex=g("lex") if "exchange6" in mods else 0.0,
                  gamma_ll=g("γ_LL", g("γ_ll", 2.211e5)),
@@ -188,7 +196,8 @@ class Engine:
                  tc=g("Tc"), spin_j=g("J", 0.5), n_spins=g("n"), temperature=g("Temp", 0.0),
                  thermal="temperature/brown" in mods, seed=int(g("Therm_seed", 0)), cutoff_dt=g("cutoff_dt"),
                  ttm="temperature/ETM" in mods, solver=solver, dt=g("dt", 1e-15), rtol=g("m_maxrelerror", 1e-5),
-                 mindt=g("mindt", 1e-22), maxdt=g("maxdt", 1e-12), maxerr=maxerr)
+                 mindt=g("mindt", 1e-22), maxdt=g("maxdt", 1e-12), maxerr=maxerr, maxrelerr=maxrelerr,
+                 max_iter=max_iter)
         if d["ttm"]:
             d.update(gamma_e=g("γ") * g("n") / 6.02214129272727272e23 if "temperature/Drude" in mods else 0.0,
                      c_l=g("Cp"), g_ep=g("Ge-p"), k_e=g("Ke") if "temperature/ETM/diffusion" in mods else 0.0)

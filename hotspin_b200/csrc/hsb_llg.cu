@@ -249,7 +249,7 @@ __device__ __forceinline__ void err_abs_store(float (&eeq)[3], HsbSolverDev* sd)
 
 template <int CH>
 __global__ void __launch_bounds__(256) k_stage(const HsbPhys P, const StageArgs A, HsbSolverDev* sd) {
-    if (!A.ungated && !sd->active) return;
+    if (!A.ungated && !hsb_gate(sd, A.gate_word)) return;
     const double t = sd->t;
     const double dt = sd->dt;
     const long long step = sd->step;
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(256, 2) k_stage4(const __grid_constant__ HsbPh
                                                    HsbSolverDev* sd0, const BatchArgs Bt) {
     const int slot = BATCH ? (int)blockIdx.z : 0;
     HsbSolverDev* sd = sd0 + slot;
-    if (!A.ungated && !(A.prep_gated ? sd->prep : sd->active)) return;
+    if (!A.ungated && !(A.prep_gated ? sd->prep : hsb_gate(sd, A.gate_word))) return;
     const HsbPhys& P = BATCH ? Bt.phys[slot] : P0;
     const long off = BATCH ? (long)slot * Bt.stride : 0;
     const int normalize = BATCH ? (A.normalize && P.normalize) : A.normalize;
@@ -705,7 +705,7 @@ __global__ void __launch_bounds__(256, W == 1 ? 3 : (W == 2 ? 2 : 1))
              const BatchArgs Bt) {
     const int slot = BATCH ? (int)blockIdx.z : 0;
     HsbSolverDev* sd = sd0 + slot;
-    if (!A.ungated && !(A.prep_gated ? sd->prep : sd->active)) return;
+    if (!A.ungated && !(A.prep_gated ? sd->prep : hsb_gate(sd, A.gate_word))) return;
     const HsbPhys& P = BATCH ? Bt.phys[slot] : P0;
     const long off = BATCH ? (long)slot * Bt.stride : 0;
     const int normalize = BATCH ? (A.normalize && P.normalize) : A.normalize;

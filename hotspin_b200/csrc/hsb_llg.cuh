@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
 
 // Maximum number of stored stages any integrator reads (Dormand-Prince: 7).
 #define HSB_MAXK 7
@@ -157,7 +158,22 @@ struct HsbSolverDev {
     int prep;              // batched slots: 1 while the slot's first-stage data is being prepared
     int pad_;
     unsigned int err_eq[3];  // rk12: float bits of the attempt's per-equation errors (m, Te, Tl)
-    int tries;             // rk12: rejected attempts of the current step
+    int tries;             // rk12 / am12: rejected attempts of the current step
+    // am12 / bdf-euler fixed-point iterations
+    int it_active;         // 1 while the current iteration continues (gates its kernels)
+    int it_count;          // sweeps of the current iteration
+    int it_flags;          // bit 0: the iteration failed; bit 1: limit the next dt by the
+                           // predictor's alpha; bit 2: the attempt was abandoned
+    int aborts;            // abandoned attempts of the current step
+    int dysel;             // derivative a sweep uses: 0 = at the explicit Euler point, 1 = latest
+    int prevsel;           // previous iterate a sweep compares with: 0 = renormalised, 1 = raw predictor
+    int eq;                // bdf-euler: the equation being iterated (0 m, 1 Te, 2 Tl)
+    int rhs_due;           // bdf-euler: 1 when the last sweep ran (its result's derivative is due)
+    double er[3];          // am12: the previous sweep's errors, sorted ascending
+    double alpha[3];       // am12: the predictor's last per-equation convergence ratios
+    double alpha_max;      // am12: the last sweep's largest ratio
+    unsigned int red[10];  // float bits of a sweep's maxima: |prev - new| per channel (0..4), the
+                           // scale per channel (5..9: |new|, |predictor| or |prev + new|)
 };
 
 // Step-size rule of hotspin's adaptive Heun solver (solve_rk12.go:91-214), applied to one
@@ -269,4 +285,306 @@ struct StageArgs {
     // error mode: 0 = the DP45 norm (m: |e| / rtol, T: |e| / (rtol max(|T0|, |T|)), one
     // maximum); 1 = per-equation absolute errors dt |e| into HsbSolverDev.err_eq (rk12)
     int err_abs;
+    // gate word: 0 = HsbSolverDev.active; else the byte offset of an int word of the solver
+    // word that must also be nonzero (the fixed-point iterations of am12 / bdf-euler)
+    int gate_word;
 };
+
+// Whether a launch gated on `gate_word` (see StageArgs) runs for this solver word.
+__host__ __device__ inline bool hsb_gate(const HsbSolverDev* sd, int gate_word) {
+    if (!sd->active) return false;
+    return gate_word == 0 || *(const int*)((const char*)sd + gate_word) != 0;
+}
+
+// ------------------------------------------------------------------ am12 / bdf-euler sweeps
+enum { IMP_AM_PRED = 0, IMP_AM_CORR = 1, IMP_AM_ERR = 2, IMP_BDF_EULER = 3, IMP_BDF_SWEEP = 4 };
+enum {
+    IMP_RULE_AM_BEGIN = 0, IMP_RULE_AM_ITER_PRED = 1, IMP_RULE_AM_ITER_CORR = 2, IMP_RULE_AM_PRED_END = 3,
+    IMP_RULE_AM_CORR_END = 4, IMP_RULE_AM_FINAL = 5, IMP_RULE_BDF_BEGIN = 6, IMP_RULE_BDF_ITER = 7,
+    IMP_RULE_BDF_CLEAR = 8
+};
+
+// Buffers of a sweep (k_imp_sweep): new iterates are formed from y0 and a derivative, compared
+// with the previous iterate, and written (m renormalised in LLG mode) to w.
+struct ImpArgs {
+    PtrSel y0;         // state at the start of the step (y[cur])
+    PtrSel w;          // renormalised iterate / working state (y[next])
+    float* up;         // am12: raw predictor iterate
+    float* uc;         // am12: raw corrector iterate
+    float* k0;         // am12: f(y0); bdf-euler: the latest derivative
+    float* k1;         // am12: derivative at the explicit Euler point
+    float* k2;         // am12: derivative of the latest iterate
+    int mode;          // IMP_AM_* / IMP_BDF_*
+    int normalize;     // renormalise m where it is written to w (LLG mode)
+    int eq;            // bdf-euler: equation (0 m, 1 Te, 2 Tl)
+};
+
+// Tolerances of the implicit solvers.
+struct ImpLimits {
+    double abs_err[3], rel_err[3];   // am12: per-equation absolute / relative errors
+    double max_iter_err;             // bdf-euler: iterator error
+    int max_iter;                    // bdf-euler: sweeps
+    int neq;
+    int eq;                          // bdf-euler: the equation a BEGIN starts
+};
+
+// ------------------------------------------------------------------ am12 / bdf-euler rules
+// hotspin's adaptive Adams-Moulton 1-2 solver (solver/am12, solve_am01.go:45-318) and fixed-step
+// backward Euler (solver/bdf-euler, solve_euler_backward.go:29-91) iterate their implicit
+// stages by fixed point; the sweeps run on the device (k_am_sweep) and leave per-channel maxima
+// in HsbSolverDev.red; these rules, shared by host and device, turn them into the decisions.
+
+// Channels of equation q: m = 0..2, Te = 3, Tl = 4.
+__host__ __device__ inline int hsb_eq_first(int q) { return q == 0 ? 0 : q + 2; }
+__host__ __device__ inline int hsb_eq_count(int q) { return q == 0 ? 3 : 1; }
+
+// am12 error norm of equation q from the sweep maxima: per channel d / (abs + scale rel), root
+// mean square over the equation's channels (solve_am01.go:120-131).
+__host__ __device__ inline double hsb_am_norm(const unsigned int* red, int q, double abs_err, double rel_err) {
+    const int c0 = hsb_eq_first(q), nc = hsb_eq_count(q);
+    double t = 0.0;
+    for (int c = c0; c < c0 + nc; c++) {
+        float d, m;
+#ifdef __CUDA_ARCH__
+        d = __uint_as_float(red[c]);
+        m = __uint_as_float(red[5 + c]);
+#else
+        memcpy(&d, &red[c], 4);
+        memcpy(&m, &red[5 + c], 4);
+#endif
+        const double v = (double)d / (abs_err + (double)m * rel_err);
+        t += v * v;
+    }
+    return sqrt(t) / sqrt((double)nc);
+}
+
+// One sweep of an am12 iteration (phase 0 predictor, 1 corrector): alpha_q = tErr_q / er_q
+// against the previous sweep's list, er = the new errors sorted ascending (the reference sorts
+// its list in place, so the next sweep pairs each equation with a rank, not with itself), err
+// and alpha their maxima; converged when err <= 0.1, failed when alpha >= 1 or after the 6th
+// sweep, else another sweep with the latest derivative (solve_am01.go:105-158, 176-223).
+__host__ __device__ inline void hsb_am_iter_rule(HsbSolverDev& sd, const double* abs_err, const double* rel_err,
+                                                 int neq, int phase) {
+    double terr[3], alp[3];
+    for (int q = 0; q < neq; q++) {
+        terr[q] = hsb_am_norm(sd.red, q, abs_err[q], rel_err[q]);
+        alp[q] = terr[q] / sd.er[q];
+    }
+    for (int i = 1; i < neq; i++)       // insertion sort, ascending, NaN last
+        for (int j = i; j > 0 && (terr[j - 1] > terr[j] || (terr[j - 1] != terr[j - 1] && terr[j] == terr[j])); j--) {
+            const double t = terr[j - 1];
+            terr[j - 1] = terr[j];
+            terr[j] = t;
+        }
+    double amax = alp[0];
+    for (int q = 0; q < neq; q++) {
+        sd.er[q] = terr[q];
+        if (phase == 0) sd.alpha[q] = alp[q];
+        if (!(alp[q] <= amax)) amax = alp[q];
+    }
+    const double err = terr[neq - 1];
+    sd.alpha_max = amax;
+    sd.it_count += 1;
+    for (int c = 0; c < 10; c++) sd.red[c] = 0u;
+    if (err <= 0.1) {
+        sd.it_active = 0;
+    } else if (amax >= 1.0 || sd.it_count > 5 || !(err == err)) {
+        sd.it_active = 0;
+        sd.it_flags |= 1;
+    } else {
+        sd.dysel = 1;
+        sd.prevsel = 0;
+    }
+}
+
+// End of an am12 iteration phase.  A failed iteration abandons the attempt: dt is halved, or
+// scaled by sqrt(0.6 / alpha) when alpha > 0.6; after a failed predictor the next step size is
+// limited by the predictor's alphas (solve_am01.go:160-172, 225-236).  The reference panics when
+// this happens on its 10th try (status 4 here) and otherwise retries without counting a bad
+// step; 64 abandoned attempts in one step also stop the run here (the reference keeps halving).
+// A finished predictor starts the corrector with the explicit-Euler-point derivative.
+__host__ __device__ inline void hsb_am_phase_rule(HsbSolverDev& sd, int phase, int neq) {
+    if (sd.it_flags & 1) {
+        sd.it_flags &= ~1;
+        sd.it_flags |= 4;
+        if (phase == 0) sd.it_flags |= 2;
+        if (sd.tries == 9) {
+            sd.status |= 4;
+            sd.active = 0;
+            return;
+        }
+        double h = 0.5 * sd.dt;
+        if (sd.alpha_max > 0.6) h = sd.dt * sqrt(0.6 / sd.alpha_max);
+        sd.dt = h;
+        sd.aborts += 1;
+        sd.attempts += 1;
+        if (sd.aborts > 64) {
+            sd.status |= 4;
+            sd.active = 0;
+        }
+        return;
+    }
+    if (phase == 0) {
+        sd.it_active = 1;
+        sd.it_count = 0;
+        for (int q = 0; q < neq; q++) sd.er[q] = 0.1;
+        sd.dysel = 0;
+        sd.prevsel = 1;
+    }
+}
+
+// End of an am12 attempt: per equation the step error (corrector vs predictor, scale: the
+// predictor), bad when above 1; dt_new = dt sqrt(0.8 / err), limited by dt sqrt(0.6 / alpha_q)
+// for the first equation when the flag is set (the reference clears it inside its loop), clamped
+// to [mindt, maxdt], the smallest over the equations; kept when no equation was bad or dt_new is
+// mindt; the 12th bad attempt stops the run, where the reference panics (solve_am01.go:238-306).
+__host__ __device__ inline void hsb_am_final_rule(HsbSolverDev& sd, const double* abs_err, const double* rel_err,
+                                                  int neq, bool nonfinite) {
+    if (sd.it_flags & 4) {        // abandoned attempt: dt was set by the phase rule
+        sd.it_flags &= ~4;
+        for (int c = 0; c < 10; c++) sd.red[c] = 0u;
+        return;
+    }
+    const double h = sd.dt;
+    bool bad = false;
+    bool finite = !nonfinite;
+    double nd = INFINITY, emax = 0.0;
+    for (int q = 0; q < neq; q++) {
+        const double te = hsb_am_norm(sd.red, q, abs_err[q], rel_err[q]);
+        if (!(te == te)) finite = false;
+        if (te > 1.0) bad = true;
+        const double hr = h * sqrt(0.8 / te);
+        double n = hr;
+        if (sd.it_flags & 2) {
+            const double ha = h * sqrt(0.6 / sd.alpha[q]);
+            n = hr < ha ? hr : ha;
+            sd.it_flags &= ~2;
+        }
+        if (n < sd.mindt) n = sd.mindt;
+        if (n > sd.maxdt) n = sd.maxdt;
+        if (n < nd) nd = n;
+        if (te > emax) emax = te;
+    }
+    for (int c = 0; c < 10; c++) sd.red[c] = 0u;
+    if (!finite) {
+        nd = h * 0.1;
+        if (nd < sd.mindt) nd = sd.mindt;
+        bad = true;
+    }
+    const bool accept = finite && (!bad || nd == sd.mindt);
+    sd.err = finite ? emax : INFINITY;
+    sd.attempts += 1;
+    if (!finite && h <= sd.mindt) sd.status |= 1;
+    if (accept) {
+        if (bad) sd.status |= 2;
+        sd.t += h;
+        sd.step += 1;
+        sd.cur = 1 - sd.cur;
+        sd.tries = 0;
+        sd.aborts = 0;
+        sd.it_flags = 0;
+    } else {
+        sd.rejects += 1;
+        if (sd.tries > 10) {
+            sd.status |= 4;
+            sd.active = 0;
+        } else {
+            sd.tries += 1;
+        }
+    }
+    if (sd.t_stop > 0.0) {
+        const double rem = sd.t_stop - sd.t;
+        if (rem <= 1e-6 * nd || rem <= 0.0) sd.active = 0;
+        else if (nd > rem) nd = rem;
+    }
+    if (sd.step_stop >= 0 && sd.step >= sd.step_stop) sd.active = 0;
+    if (sd.status & 1) sd.active = 0;
+    sd.dt = nd;
+}
+
+// Start of an am12 attempt: the predictor iteration begins with the explicit-Euler-point
+// derivative and the renormalised Euler point as its previous iterate.
+__host__ __device__ inline void hsb_am_begin_rule(HsbSolverDev& sd, int neq) {
+    sd.it_active = 1;
+    sd.it_count = 0;
+    sd.dysel = 0;
+    sd.prevsel = 0;
+    sd.it_flags &= 2;
+    for (int q = 0; q < neq; q++) sd.er[q] = 0.1;
+    for (int c = 0; c < 10; c++) sd.red[c] = 0u;
+}
+
+// One backward-Euler sweep of equation sd.eq: err = MaxDiff / MaxSum over the equation's
+// channels (relative when the sum is positive), converged at err <= max_iter_err; more than
+// max_iter sweeps stop the run (status 4), where the reference panics
+// (solve_euler_backward.go:64-84).
+__host__ __device__ inline void hsb_bdf_iter_rule(HsbSolverDev& sd, double max_iter_err, int max_iter) {
+    const int c0 = hsb_eq_first(sd.eq), nc = hsb_eq_count(sd.eq);
+    float d = 0.f, m = 0.f;
+    for (int c = c0; c < c0 + nc; c++) {
+        float dc, mc;
+#ifdef __CUDA_ARCH__
+        dc = __uint_as_float(sd.red[c]);
+        mc = __uint_as_float(sd.red[5 + c]);
+#else
+        memcpy(&dc, &sd.red[c], 4);
+        memcpy(&mc, &sd.red[5 + c], 4);
+#endif
+        if (!(dc <= d)) d = dc;
+        if (!(mc <= m)) m = mc;
+    }
+    double err = (double)d;
+    if (m > 0.f) err = err / (double)m;
+    sd.err = err;
+    sd.it_count += 1;
+    sd.rhs_due = 1;               // the sweep ran: the derivative of its result is due
+    for (int c = 0; c < 10; c++) sd.red[c] = 0u;
+    // the reference checks the sweep count after every sweep, converged or not
+    if (sd.it_count > max_iter || !(err == err)) {
+        sd.it_active = 0;
+        sd.status |= (err == err) ? 4 : 1;
+        sd.active = 0;
+    } else if (err <= max_iter_err) {
+        sd.it_active = 0;
+    }
+}
+
+// The decision kernel's dispatch (k_imp_rule, one thread per slot): which rule a launch applies
+// to the slot's solver word.  A stopped slot is left alone, except that the due flag of
+// bdf-euler is always cleared.
+__host__ __device__ inline void hsb_imp_rule(HsbSolverDev& sd, const ImpLimits& L, int which) {
+    if (which == IMP_RULE_BDF_CLEAR) {
+        sd.rhs_due = 0;
+        return;
+    }
+    if (!sd.active) return;
+    switch (which) {
+        case IMP_RULE_AM_BEGIN: hsb_am_begin_rule(sd, L.neq); break;
+        case IMP_RULE_AM_ITER_PRED:
+        case IMP_RULE_AM_ITER_CORR:
+            if (sd.it_active) hsb_am_iter_rule(sd, L.abs_err, L.rel_err, L.neq, which == IMP_RULE_AM_ITER_PRED ? 0 : 1);
+            break;
+        case IMP_RULE_AM_PRED_END:
+        case IMP_RULE_AM_CORR_END:
+            if (!(sd.it_flags & 4)) hsb_am_phase_rule(sd, which == IMP_RULE_AM_PRED_END ? 0 : 1, L.neq);
+            break;
+        case IMP_RULE_AM_FINAL: {
+            const bool nf = sd.nonfinite != 0u;
+            sd.nonfinite = 0u;
+            hsb_am_final_rule(sd, L.abs_err, L.rel_err, L.neq, nf);
+            break;
+        }
+        case IMP_RULE_BDF_BEGIN:
+            sd.eq = L.eq;
+            sd.it_active = 1;
+            sd.it_count = 0;
+            sd.rhs_due = 0;
+            for (int c = 0; c < 10; c++) sd.red[c] = 0u;
+            break;
+        case IMP_RULE_BDF_ITER:
+            if (sd.it_active) hsb_bdf_iter_rule(sd, L.max_iter_err, L.max_iter);
+            break;
+        default: break;
+    }
+}
+

@@ -7,6 +7,7 @@
 // device (HsbSolverDev), so a run of steps is captured once into a CUDA graph and replayed
 // with no host round trip; the host only checks completion between graph launches.
 #include <math.h>
+#include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -60,13 +61,21 @@ struct hsb_sim_desc {
     int32_t laser_npts;
     const double* bext_table;    // 4 x bext_npts (t, Bx, By, Bz); copied at creation
     int32_t bext_npts;
-    double maxerr[3];            // rk12: per-step error limits of m, Te, Tl
+    double maxerr[3];            // rk12: maxError; am12: maxAbsError; bdf-euler: maxIterError (m, Te, Tl)
+    double maxrelerr[3];         // am12: maxRelError (m, Te, Tl)
+    int32_t max_iter;            // bdf-euler: sweeps per equation
 };
 
-enum { SOLVER_EULER = 0, SOLVER_HEUN = 1, SOLVER_RK4 = 2, SOLVER_DP45 = 3, SOLVER_RK12 = 4 };
+enum { SOLVER_EULER = 0, SOLVER_HEUN = 1, SOLVER_RK4 = 2, SOLVER_DP45 = 3, SOLVER_RK12 = 4, SOLVER_AM12 = 5,
+       SOLVER_BDF_EULER = 6 };
 
 // Solvers whose step size is chosen on the device (accept / reject per attempt).
-static inline bool adaptive_solver(int s) { return s == SOLVER_DP45 || s == SOLVER_RK12; }
+static inline bool adaptive_solver(int s) { return s == SOLVER_DP45 || s == SOLVER_RK12 || s == SOLVER_AM12; }
+
+// Fixed-point sweeps of the implicit solvers (hsb_implicit.cu).
+int hsb_launch_imp_sweep(const HsbPhys& P, const ImpArgs& A, HsbSolverDev* sd, const BatchArgs& Bt, int nslot,
+                         bool batched, cudaStream_t st);
+int hsb_launch_imp_rule(HsbSolverDev* sd, int nslot, const ImpLimits& L, int which, cudaStream_t st);
 
 static const double MU0 = 4.0e-7 * M_PI;
 static const double KB = 1.38064881313131313e-23;
@@ -139,6 +148,7 @@ struct hsb_sim_s {
     int launches_g, launches_g1;  // kernels in the full graph and in the one-attempt graph
     long long launch_total;       // kernels enqueued for stepping since creation
     double rk12_maxerr[3];        // rk12: per-step error limits (m, Te, Tl; +inf = uncontrolled)
+    ImpLimits imp;                // am12 / bdf-euler limits
     float* ckpt;                  // checkpoint: the state channels [nch][n] (device)
     HsbSolverDev* ckpt_sd;        // checkpoint: the solver word (device)
 };
@@ -306,7 +316,8 @@ static int get_sd(hsb_sim_s* S) {
 
 // Demag of one of the two state buffers (sel: -1 fixed pointer `m`, 0 = y[cur], 1 = y[next])
 // into `h` (or into hd01[cur / next] when hsel >= 0).
-static int run_demag(hsb_sim_s* S, const float* m, int msel, float* h, int hsel, bool gated = true) {
+static int run_demag(hsb_sim_s* S, const float* m, int msel, float* h, int hsel, bool gated = true,
+                     const int* gate_word = nullptr) {
     S->sd_fresh = false;
     if (!S->demag) return HSB_OK;
     HsbDemagIO io;
@@ -337,7 +348,7 @@ static int run_demag(hsb_sim_s* S, const float* m, int msel, float* h, int hsel,
         io.ev = ev;
     }
     S->launches += hsb_demag_nlaunch(S->demag);
-    const int* gate = gated ? (S->prep_mode ? &S->sd->prep : &S->sd->active) : nullptr;
+    const int* gate = gated ? (gate_word ? gate_word : (S->prep_mode ? &S->sd->prep : &S->sd->active)) : nullptr;
     int rc;
     if (S->batched) {
         HsbDemagBatch b;
@@ -405,6 +416,31 @@ static void thermal_keep(hsb_sim_s* S, StageArgs& A, bool first) {
     if (!S->hth || !hsb_stage_keeps_thermal(S->P, S->stage_variant)) return;
     A.hth = fixed(S->hth);
     A.hth_mode = first ? 1 : 2;
+}
+
+static int L_sweep(hsb_sim_s* S, int mode, int eq = 0) {
+    S->sd_fresh = false;
+    ImpArgs A;
+    memset(&A, 0, sizeof(A));
+    A.y0 = pair(S->y[0], S->y[1], SEL_CUR);
+    A.w = pair(S->y[0], S->y[1], SEL_NEXT);
+    A.up = S->ystage[0];
+    A.uc = S->ystage[1];
+    A.k0 = S->k[0];
+    A.k1 = S->k[1];
+    A.k2 = S->k[2];
+    A.mode = mode;
+    A.normalize = S->batched ? 1 : S->d.normalize;
+    A.eq = eq;
+    BatchArgs nb = {0, nullptr, 1};
+    return hsb_launch_imp_sweep(S->P, A, S->sd, S->batched ? S->bt : nb, S->batched ? S->nslot : 1, S->batched,
+                                S->st);
+}
+static int L_rule(hsb_sim_s* S, int which, int eq = 0) {
+    S->sd_fresh = false;
+    ImpLimits L = S->imp;
+    L.eq = eq;
+    return hsb_launch_imp_rule(S->sd, S->batched ? S->nslot : 1, L, which, S->st);
 }
 
 static int L_advance(hsb_sim_s* S) {
@@ -636,6 +672,96 @@ static int enqueue_attempt(hsb_sim_s* S) {
             }));
             break;
         }
+        case SOLVER_AM12: {  // solve_am01.go:45-318 (one try of the reference's loop per attempt)
+            const int itw = (int)offsetof(HsbSolverDev, it_active);
+            const int* itg = &S->sd->it_active;
+            RC(timed(S, PROF_OTHER, [&] { return L_rule(S, IMP_RULE_AM_BEGIN); }));
+            RC(run_demag(S, nullptr, 0, hd, -1));
+            StageArgs A = empty_args();          // dy0 = f(t0, y0) and the explicit Euler point
+            A.ys = YC;
+            A.hd = fixed(hd);
+            A.ytherm = YC;
+            A.kout = fixed(S->k[0]);
+            A.kself_w = 1.0f;
+            A.ynext = YN;
+            A.ybase = YC;
+            A.cself = 1.0f;
+            A.normalize = norm;
+            thermal_keep(S, A, true);
+            RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
+            StageArgs R = empty_args();          // f(t0 + dt, iterate)
+            R.ys = YN;
+            R.hd = fixed(hd);
+            R.ytherm = YC;
+            R.tfrac = 1.0f;
+            R.kself_w = 1.0f;
+            thermal_keep(S, R, false);
+            RC(run_demag(S, nullptr, 1, hd, -1));
+            R.kout = fixed(S->k[1]);
+            RC(timed(S, PROF_STAGE, [&] { return L_stage(S, R); }));
+            R.kout = fixed(S->k[2]);
+            R.gate_word = itw;
+            for (int phase = 0; phase < 2; phase++) {
+                for (int j = 0; j < 6; j++) {
+                    RC(timed(S, PROF_OTHER, [&] { return L_sweep(S, phase == 0 ? IMP_AM_PRED : IMP_AM_CORR); }));
+                    RC(timed(S, PROF_OTHER, [&] {
+                        return L_rule(S, phase == 0 ? IMP_RULE_AM_ITER_PRED : IMP_RULE_AM_ITER_CORR);
+                    }));
+                    if (j < 5) {
+                        RC(run_demag(S, nullptr, 1, hd, -1, true, itg));
+                        RC(timed(S, PROF_STAGE, [&] { return L_stage(S, R); }));
+                    }
+                }
+                RC(timed(S, PROF_OTHER, [&] {
+                    return L_rule(S, phase == 0 ? IMP_RULE_AM_PRED_END : IMP_RULE_AM_CORR_END);
+                }));
+            }
+            RC(timed(S, PROF_OTHER, [&] { return L_sweep(S, IMP_AM_ERR); }));
+            RC(timed(S, PROF_OTHER, [&] { return L_rule(S, IMP_RULE_AM_FINAL); }));
+            break;
+        }
+        case SOLVER_BDF_EULER: {  // solve_euler_backward.go:29-91 (fixed step)
+            const int rdw = (int)offsetof(HsbSolverDev, rhs_due);
+            const int* rdg = &S->sd->rhs_due;
+            RC(run_demag(S, nullptr, 0, hd, -1));
+            StageArgs A = empty_args();          // inputs at t; the working state starts as y0
+            A.ys = YC;
+            A.hd = fixed(hd);
+            A.ytherm = YC;
+            A.kout = fixed(S->k[0]);
+            A.kself_w = 1.0f;
+            A.ynext = YN;
+            A.ybase = YC;
+            A.cself = 0.0f;
+            thermal_keep(S, A, true);
+            RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
+            StageArgs R = empty_args();          // f(t + dt, working state)
+            R.ys = YN;
+            R.hd = fixed(hd);
+            R.ytherm = YC;
+            R.tfrac = 1.0f;
+            R.kout = fixed(S->k[0]);
+            R.kself_w = 1.0f;
+            thermal_keep(S, R, false);
+            const int neq = S->nch == 5 ? 3 : 1;
+            for (int q = 0; q < neq; q++) {
+                RC(timed(S, PROF_OTHER, [&] { return L_rule(S, IMP_RULE_BDF_BEGIN, q); }));
+                RC(timed(S, PROF_OTHER, [&] { return L_sweep(S, IMP_BDF_EULER, q); }));
+                RC(run_demag(S, nullptr, 1, hd, -1));
+                R.gate_word = 0;
+                RC(timed(S, PROF_STAGE, [&] { return L_stage(S, R); }));
+                R.gate_word = rdw;
+                for (int j = 0; j <= S->imp.max_iter; j++) {
+                    RC(timed(S, PROF_OTHER, [&] { return L_sweep(S, IMP_BDF_SWEEP, q); }));
+                    RC(timed(S, PROF_OTHER, [&] { return L_rule(S, IMP_RULE_BDF_ITER, q); }));
+                    RC(run_demag(S, nullptr, 1, hd, -1, true, rdg));
+                    RC(timed(S, PROF_STAGE, [&] { return L_stage(S, R); }));
+                    RC(timed(S, PROF_OTHER, [&] { return L_rule(S, IMP_RULE_BDF_CLEAR, q); }));
+                }
+            }
+            RC(timed(S, PROF_OTHER, [&] { return L_advance(S); }));
+            break;
+        }
         default:
             hsb_set_error("unknown solver %d", S->d.solver);
             return HSB_ERR_INVALID;
@@ -738,6 +864,8 @@ static int plain_only(hsb_sim_s* S, const char* who) {
 // reached leaves it inactive; dt is clipped to land on the target.
 __global__ void k_arm(HsbSolverDev* sd, long long nsteps, double t_stop) {
     sd->tries = 0;
+    sd->aborts = 0;
+    sd->it_flags = 0;
     if (sd->status & 1) {
         sd->active = 0;
         return;
@@ -891,7 +1019,7 @@ static SlotLayout slot_layout(const hsb_sim_desc& d, long n) {
     auto al = [](long x) { return (x + 63) & ~63L; };  // 256-byte boundaries
     SlotLayout L;
     const long ny = (long)(d.ttm ? 5 : 3) * n;
-    L.nk = (d.solver == SOLVER_DP45) ? 7 : 1;
+    L.nk = (d.solver == SOLVER_DP45) ? 7 : (d.solver == SOLVER_AM12 ? 3 : 1);
     long o = 0;
     L.y = o;
     o += al(2 * ny);
@@ -1059,6 +1187,18 @@ static void set_rk12_limits(hsb_sim_s* S) {
     const hsb_sim_desc& d = S->d;
     S->rk12_maxerr[0] = d.maxerr[0] > 0 ? d.maxerr[0] : d.rtol;
     for (int q = 1; q < 3; q++) S->rk12_maxerr[q] = d.maxerr[q] > 0 ? d.maxerr[q] : INFINITY;
+    // am12: maxAbsError / maxRelError per equation, the reference's defaults 1e-4 / 1e-3
+    // (solve_am01.go:395-398); bdf-euler: maxIterError 1e-5 and 3 sweeps
+    // (solve_euler_backward.go:129-130)
+    ImpLimits& L = S->imp;
+    memset(&L, 0, sizeof(L));
+    for (int q = 0; q < 3; q++) {
+        L.abs_err[q] = d.maxerr[q] > 0 ? d.maxerr[q] : 1e-4;
+        L.rel_err[q] = d.maxrelerr[q] > 0 ? d.maxrelerr[q] : 1e-3;
+    }
+    L.max_iter_err = d.maxerr[0] > 0 ? d.maxerr[0] : 1e-5;
+    L.max_iter = d.max_iter > 0 ? d.max_iter : 3;
+    L.neq = S->nch == 5 ? 3 : 1;
 }
 
 static int check_desc(const hsb_sim_desc& d, const char* who) {
@@ -1068,7 +1208,7 @@ static int check_desc(const hsb_sim_desc& d, const char* who) {
             return HSB_ERR_INVALID;
         }
     }
-    if (d.solver < SOLVER_EULER || d.solver > SOLVER_RK12) {
+    if (d.solver < SOLVER_EULER || d.solver > SOLVER_BDF_EULER) {
         hsb_set_error("%s: unknown solver %d", who, d.solver);
         return HSB_ERR_INVALID;
     }
@@ -1081,10 +1221,14 @@ static int check_desc(const hsb_sim_desc& d, const char* who) {
         return HSB_ERR_INVALID;
     }
     for (int q = 0; q < 3; q++) {
-        if (isnan(d.maxerr[q])) {
-            hsb_set_error("%s: maxerr[%d] is not a number", who, q);
+        if (isnan(d.maxerr[q]) || isnan(d.maxrelerr[q])) {
+            hsb_set_error("%s: maxerr[%d] / maxrelerr[%d] is not a number", who, q, q);
             return HSB_ERR_INVALID;
         }
+    }
+    if (d.solver == SOLVER_BDF_EULER && d.max_iter > 64) {
+        hsb_set_error("%s: bdf-euler max_iter %d above 64", who, d.max_iter);
+        return HSB_ERR_INVALID;
     }
     if (d.llb && !(d.tc > 0 && d.spin_j > 0 && d.n_spins > 0)) {
         hsb_set_error("%s: llb needs tc, spin_j and n_spins > 0", who);
@@ -1767,8 +1911,10 @@ HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* d
     }
     if (d.solver != c.solver || d.ttm != c.ttm || d.demag != c.demag || (d.thermal && !c.thermal) ||
         (adaptive_solver(c.solver) && d.rtol != c.rtol) ||
-        (c.solver == SOLVER_RK12 &&
-         (d.maxerr[0] != c.maxerr[0] || d.maxerr[1] != c.maxerr[1] || d.maxerr[2] != c.maxerr[2]))) {
+        (c.solver >= SOLVER_RK12 &&
+         (d.maxerr[0] != c.maxerr[0] || d.maxerr[1] != c.maxerr[1] || d.maxerr[2] != c.maxerr[2] ||
+          d.maxrelerr[0] != c.maxrelerr[0] || d.maxrelerr[1] != c.maxrelerr[1] || d.maxrelerr[2] != c.maxrelerr[2] ||
+          d.max_iter != c.max_iter))) {
         hsb_set_error("hsb_batch_admit: solver, tolerance, two-temperature model, demag or thermal field differ "
                       "from the class");
         return HSB_ERR_INVALID;

@@ -9,7 +9,8 @@ import numpy as np
 
 from . import _lib
 
-SOLVERS = {"euler": 0, "heun": 1, "rk4": 2, "dp45": 3, "rk45": 3, "rk12": 4}
+SOLVERS = {"euler": 0, "heun": 1, "rk4": 2, "dp45": 3, "rk45": 3, "rk12": 4, "am12": 5, "bdf-euler": 6,
+           "bdf_euler": 6}
 
 _FIELDS = {f[0] for f in _lib.SimDesc._fields_}
 

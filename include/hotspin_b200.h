@@ -45,7 +45,15 @@ enum {
     HSB_ERR_SOLVER = 6
 };
 
-enum { HSB_SOLVER_EULER = 0, HSB_SOLVER_HEUN = 1, HSB_SOLVER_RK4 = 2, HSB_SOLVER_DP45 = 3, HSB_SOLVER_RK12 = 4 };
+enum {
+    HSB_SOLVER_EULER = 0,     /* solver/euler  (solve_euler.go:22-50)                  */
+    HSB_SOLVER_HEUN = 1,      /* solver/heun   (solve_heun.go:27-79)                   */
+    HSB_SOLVER_RK4 = 2,       /* classic RK4 (no reference counterpart)               */
+    HSB_SOLVER_DP45 = 3,      /* Dormand-Prince 4(5) (no reference counterpart)       */
+    HSB_SOLVER_RK12 = 4,      /* solver/rk12   (solve_rk12.go:91-214)                  */
+    HSB_SOLVER_AM12 = 5,      /* solver/am12   (solve_am01.go:45-318)                  */
+    HSB_SOLVER_BDF_EULER = 6  /* solver/bdf-euler (solve_euler_backward.go:29-91)      */
+};
 
 /* Simulation description.  Replaces the module graph a hotspin script builds with
  * load(...)/setv(...): exchange6, anisotropy/uniaxial, zeeman, demag, llbar +
@@ -99,11 +107,18 @@ typedef struct hsb_sim_desc {
      * constant b_ext.  Copied at creation; not available in batches.                     */
     const double* bext_table;
     int32_t bext_npts;      /* 0 or 2..4096                                          */
-    /* HSB_SOLVER_RK12 (hotspin's solver/rk12, solve_rk12.go:91-214): the largest error per
-     * step of each equation, dt max |k1 - k0| (<m>_maxError, <Te>_maxError, <Tl>_maxError).
-     * maxerr[0] <= 0 takes rtol; a temperature entry <= 0 leaves that equation
-     * uncontrolled.                                                                     */
+    /* Per-equation tolerances (m, Te, Tl) of hotspin's own solvers:
+     *  HSB_SOLVER_RK12: maxerr = <q>_maxError, the largest dt max |k1 - k0| per step;
+     *    maxerr[0] <= 0 takes rtol, a temperature entry <= 0 leaves that equation
+     *    uncontrolled.
+     *  HSB_SOLVER_AM12: maxerr = <q>_maxAbsError, maxrelerr = <q>_maxRelError
+     *    (defaults when <= 0: 1e-4 and 1e-3, solve_am01.go:395-398).
+     *  HSB_SOLVER_BDF_EULER: maxerr[0] = the iterator error of every equation (default
+     *    1e-5), max_iter = sweeps per equation (default 3, at most 64;
+     *    solve_euler_backward.go:129-130).                                                */
     double maxerr[3];
+    double maxrelerr[3];
+    int32_t max_iter;
 } hsb_sim_desc;
 
 typedef struct hsb_sim_s* hsb_sim;
@@ -139,8 +154,9 @@ int hsb_sim_sync(hsb_sim sim);
 
 /* Solver bookkeeping: time, current dt, accepted steps, attempts, rejected attempts,
  * last error norm, status bits (1: non-finite state, 2: a step was taken at mindt without
- * meeting the tolerance, 4: an RK12 step still failed after 10 retries, where hotspin
- * panics; the run stops with HSB_ERR_SOLVER). */
+ * meeting the tolerance, 4: an RK12 / AM12 step still failed after 10 retries or an
+ * implicit iteration did not converge, where hotspin panics; the run stops with
+ * HSB_ERR_SOLVER). */
 int hsb_sim_status(hsb_sim sim, double* t, double* dt, int64_t* steps, int64_t* attempts,
                    int64_t* rejects, double* err, int32_t* status);
 int hsb_sim_set_time(hsb_sim sim, double t, double dt);

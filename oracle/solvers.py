@@ -65,12 +65,44 @@ def rk12_rule(dt, errs, limits, mindt, maxdt):
     return (not bad) or newdt == mindt, bad, newdt, emax
 
 
+def _div(a, b):
+    """a / b with IEEE results for b == 0 (inf, or nan for 0 / 0), as Go's float64 division."""
+    if b == 0.0:
+        return math.nan if a == 0.0 or a != a else math.copysign(math.inf, a)
+    return a / b
+
+
+def am_error(a, b, scale, abs_err, rel_err):
+    """The error norm of solver/am12 (solve_am01.go:120-131, 247-256): per component p,
+    MaxDiff(a_p, b_p) / (maxAbsError + MaxAbs(scale_p) maxRelError), root mean square over
+    the components.  The iterators compare the previous iterate with the new one (scale: the
+    new one); the step error compares the corrector with the predictor (scale: predictor)."""
+    comps = a.shape[0] if a.ndim == 4 else 1
+    av, bv, sv = a.reshape(comps, -1), b.reshape(comps, -1), scale.reshape(comps, -1)
+    t = 0.0
+    for c in range(comps):
+        d = float(np.abs(av[c] - bv[c]).max())
+        mx = float(np.abs(sv[c]).max())
+        t += _div(d, abs_err + mx * rel_err) ** 2
+    return math.sqrt(t) / math.sqrt(comps)
+
+
+def am_iter_rule(er, terrs):
+    """One fixed-point iteration's bookkeeping (solve_am01.go:116-150): alpha_i = tErr_i / er_i
+    against the error list of the previous iteration, er_i = tErr_i, then the list is sorted in
+    place (so the next iteration pairs tErr_i with the i-th smallest error); returns
+    (new er, per-equation alphas, err = max, alpha = max)."""
+    alp = [_div(t, e) for t, e in zip(terrs, er)]
+    er = sorted(terrs)
+    return er, alp, er[-1], max(alp)
+
+
 class Integrator:
     """Drives a ``Model``.  ``y`` is a dict of arrays; ``t``, ``dt``, ``step`` as in the
     reference engine (engine/engine.go:473-508)."""
 
     def __init__(self, model, y, method, dt, rtol=1e-5, mindt=1e-20, maxdt=1e-10,
-                 maxerr=1e-4, t=0.0):
+                 maxerr=1e-4, t=0.0, maxabserr=None, maxrelerr=None, max_iter=3, max_iter_err=1e-5):
         self.model = model
         self.norm = model.s.normalize
         self.y = {k: np.array(v, dtype=np.float64) for k, v in y.items()}
@@ -84,6 +116,13 @@ class Integrator:
         self.mindt = mindt
         self.maxdt = maxdt
         self.maxerr = maxerr
+        # am12: per-equation absolute / relative error limits (the reference's defaults)
+        self.maxabserr = {k: 1e-4 for k in self.y} if maxabserr is None else dict(maxabserr)
+        self.maxrelerr = {k: 1e-3 for k in self.y} if maxrelerr is None else dict(maxrelerr)
+        # bdf-euler: iterations and iterator error per equation (defaults 3, 1e-5)
+        self.max_iter = max_iter
+        self.max_iter_err = max_iter_err
+        self.iterations = 0
         self.bad_steps = 0
         self.k_fsal = None
         self.last_err = 0.0
@@ -108,7 +147,7 @@ class Integrator:
     def run_until(self, t_end):
         """Step until t_end; adaptive steps are clamped to land on it (as the device does)."""
         while t_end - self.t > 1e-6 * self.dt:
-            if self.method in ("dp45", "rk12"):
+            if self.method in ("dp45", "rk12", "am12"):
                 self.dt = min(self.dt, t_end - self.t)
             self.step()
 
@@ -174,6 +213,147 @@ class Integrator:
                 raise RuntimeError("The solver cannot converge after 10 badsteps")
             self.bad_steps += 1
             tr += 1
+        self.step_count += 1
+
+    def _eq_keys(self):
+        return [k for k in ("m", "Te", "Tl") if k in self.y]
+
+    def _am12(self):
+        """solve_am01.go:45-318 (solver/am12): explicit Euler start, implicit Euler predictor and
+        trapezoidal corrector solved by fixed-point iteration (target error 0.1 of the
+        tolerance, at most 6 sweeps, divergence when alpha >= 1), error = predictor vs
+        corrector in the am_error norm, dt_new = dt sqrt(0.8 / err) (limited by
+        dt sqrt(0.6 / alpha) after a failed iteration, for the first equation only, as the
+        reference resets the flag inside its loop), minimum over the equations.  m is
+        renormalised where the reference's update renormalises it: before every right-hand
+        side, so the iterators compare the renormalised previous iterate with the new raw one,
+        and the final error compares the raw corrector and predictor results.  A failed
+        iteration halves dt (or scales it by sqrt(0.6 / alpha) when alpha > 0.6) and retries
+        without counting a bad step, as the reference does; 64 such retries in one step raise
+        here (the reference keeps halving).  The thermal field is drawn per attempt."""
+        f = self.model.rhs
+        t0 = self.t
+        keys = self._eq_keys()
+        ab = [self.maxabserr[k] for k in keys]
+        rl = [self.maxrelerr[k] for k in keys]
+        y0 = self._fix(self.y)
+        tries = 0
+        aborts = 0
+        restrict = False
+        s_alpha = [0.0] * len(keys)
+        while True:
+            dt = self.dt
+            self._thermal(dt)
+            dy0 = f(t0, y0)
+            y = self._fix(_comb(y0, [dy0], [1.0], dt))
+            dy = f(t0 + dt, y)
+            dybuf = dy
+            failed = False
+            for phase in ("predictor", "corrector"):
+                er = [0.1] * len(keys)
+                it = 0
+                while True:
+                    terrs = []
+                    ynew = {}
+                    for i, k in enumerate(keys):
+                        if phase == "predictor":
+                            ynew[k] = y0[k] + dt * dy[k]
+                        else:
+                            ynew[k] = y0[k] + 0.5 * dt * (dy[k] + dy0[k])
+                        terrs.append(am_error(y[k], ynew[k], ynew[k], ab[i], rl[i]))
+                    er, alp, err, alpha = am_iter_rule(er, terrs)
+                    if phase == "predictor":
+                        s_alpha = alp
+                    y = dict(y, **ynew)
+                    it += 1
+                    self.iterations += 1
+                    if err <= 0.1:
+                        break
+                    if alpha >= 1.0 or it > 5:
+                        failed = True
+                        break
+                    y = self._fix(y)
+                    dy = f(t0 + dt, y)
+                if failed:
+                    if tries == 9:
+                        raise RuntimeError("The BDF iterator cannot converge")
+                    h = 0.5 * dt
+                    if alpha > 0.6:
+                        h = dt * math.sqrt(0.6 / alpha)
+                    self.dt = h
+                    if phase == "predictor":
+                        restrict = True
+                    aborts += 1
+                    if aborts > 64:
+                        raise RuntimeError("am12: 64 failed iterations in one step")
+                    break
+                if phase == "predictor":
+                    y1 = dict(y)
+                    dy = dybuf
+            if failed:
+                continue
+            bad = False
+            ndts = []
+            for i, k in enumerate(keys):
+                terr = am_error(y[k], y1[k], y1[k], ab[i], rl[i])
+                if terr > 1.0:
+                    bad = True
+                h_r = dt * math.sqrt(_div(0.8, terr))
+                nd = h_r
+                if restrict:
+                    nd = min(h_r, dt * math.sqrt(_div(0.6, s_alpha[i])))
+                    restrict = False
+                nd = min(max(nd, self.mindt), self.maxdt)
+                ndts.append(nd)
+                self.last_err = max(self.last_err if i else 0.0, terr)
+            ndt = min(ndts)
+            self.dt = ndt
+            if not bad or ndt == self.mindt:
+                self.y = y
+                self.t = t0 + dt
+                break
+            if tries > 10:
+                raise RuntimeError("The solver cannot converge after 10 badsteps")
+            self.bad_steps += 1
+            tries += 1
+        self.step_count += 1
+
+    def _bdf_euler(self):
+        """solve_euler_backward.go:29-91 (solver/bdf-euler, fixed step): time advanced first;
+        each equation in turn (m, Te, Tl) takes an explicit Euler step and is then iterated,
+        y = y0 + dt f(t + dt, y) with f evaluated on the current state of every equation,
+        until MaxDiff(y, y_new) / MaxSum(y, y_new) <= max_iter_err; more than max_iter
+        sweeps raise, as the reference panics.  m is renormalised before each evaluation."""
+        f = self.model.rhs
+        dt = self.dt
+        self._thermal(dt)
+        y = self._fix(self.y)
+        dy = f(self.t, y)            # the inputs of the step, before time advances
+        self.t += dt
+        for k in self._eq_keys():
+            y0k = y[k]
+            y = dict(y)
+            y[k] = y0k + dt * dy[k]
+            y = self._fix(y)
+            dy = f(self.t, y)
+            self.iterations += 1
+            it = 0
+            err = 1.0e38
+            while err > self.max_iter_err:
+                ynew = y0k + dt * dy[k]
+                err = float(np.abs(y[k] - ynew).max())
+                ssum = float(np.abs(y[k] + ynew).max())
+                if ssum > 0.0:
+                    err = err / ssum
+                it += 1
+                self.iterations += 1
+                y = dict(y)
+                y[k] = ynew
+                y = self._fix(y)
+                dy = f(self.t, y)
+                if it > self.max_iter:
+                    raise RuntimeError("The BDF iterator cannot converge for %s" % k)
+        self.y = y
         self.step_count += 1
 
     # -- new integrators ----------------------------------------------------------
