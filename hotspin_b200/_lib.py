@@ -39,7 +39,7 @@ class SimDesc(ctypes.Structure):
         ("laser_sigma", c_dbl), ("solver", c_i32), ("dt", c_dbl), ("rtol", c_dbl),
         ("mindt", c_dbl), ("maxdt", c_dbl), ("laser_table", ctypes.POINTER(c_dbl)), ("laser_npts", c_i32),
         ("bext_table", ctypes.POINTER(c_dbl)), ("bext_npts", c_i32), ("maxerr", c_dbl * 3),
-        ("maxrelerr", c_dbl * 3), ("max_iter", c_i32),
+        ("maxrelerr", c_dbl * 3), ("max_iter", c_i32), ("demag_tensor", c_i32),
     ]
 
 
@@ -87,6 +87,7 @@ _SIGS = {
     "hsb_mfa_table": (c_int, [c_dbl, c_dbl, c_int, c_dp, c_dp, c_dp]),
     "hsb_mfa_equilibrium": (c_int, [c_dbl, c_dbl, c_dbl, c_dp]),
     "hsb_demag_profile": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_vp, c_vp, c_int, c_dp]),
+    "hsb_demag_plan_create_tensor": (c_int, [c_ip, c_dp, c_ip, c_int, c_int, c_vp, ctypes.POINTER(c_vp)]),
     "hsb_demag_plan_create": (c_int, [c_ip, c_dp, c_ip, c_int, c_vp, ctypes.POINTER(c_vp)]),
     "hsb_demag_plan_destroy": (c_int, [c_vp]),
     "hsb_demag_plan_info": (c_int, [c_vp, c_ip, c_ip, c_dp]),

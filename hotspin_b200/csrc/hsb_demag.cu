@@ -1118,6 +1118,7 @@ struct hsb_demag_plan_s {
     int yc2k, yc_threads, yc_cols, yc_smem, zc_k1, zc_smem;
     float2* tw4c;       // four-step twiddles of the y columns (length L1, or 1024 for yc2k)
     int zdirect;        // the y/z kernel convolves z directly: kern4 rows d < N0 hold k_zdirect
+    int tensor;         // HSB_DEMAG_ARNE (0) or HSB_DEMAG_NEWELL (1)
     float2* tw4z;       // and of the z transform (length L0)
 };
 
@@ -1253,7 +1254,7 @@ int hsb_demag_spectrum_enqueue(hsb_demag_plan P, const double* cs, int accuracy,
     g.Lmin = fmin(cs[0], fmin(cs[1], cs[2]));
     g.accuracy = (double)accuracy;
     HSB_CUDA_TRY(cudaMemsetAsync(s->dmax, 0, sizeof(double), st));
-    HSB_CUDA_TRY(hsb_arne_launch(&g, s->Kc, st));
+    HSB_CUDA_TRY(P->tensor == 1 ? hsb_newell_launch(&g, s->Kc, st) : hsb_arne_launch(&g, s->Kc, st));
     const int M = L2 / 2;
     const int TY = pick_tile(M, sizeof(double2), SMEM_TILE_BUDGET, 16);
     const int smx = 2 * TY * fpad_len(M) * (int)sizeof(double2);
@@ -1402,13 +1403,23 @@ static int tune_x(hsb_demag_plan_s* P, cudaStream_t st) {
 
 HSB_EXPORT int hsb_demag_plan_create(const int* size, const double* cellsize, const int* pbc,
                                      int accuracy, void* stream, hsb_demag_plan* out) {
+    return hsb_demag_plan_create_tensor(size, cellsize, pbc, accuracy, 0, stream, out);
+}
+
+HSB_EXPORT int hsb_demag_plan_create_tensor(const int* size, const double* cellsize, const int* pbc, int accuracy,
+                                            int tensor, void* stream, hsb_demag_plan* out) {
     if (!size || !cellsize || !pbc || !out) {
         hsb_set_error("hsb_demag_plan_create: null argument");
         return HSB_ERR_INVALID;
     }
     *out = nullptr;
+    if (tensor != 0 && tensor != 1) {
+        hsb_set_error("hsb_demag_plan_create: tensor %d is neither Kernel_Arne (0) nor Newell (1)", tensor);
+        return HSB_ERR_INVALID;
+    }
     hsb_demag_plan_s* P = (hsb_demag_plan_s*)calloc(1, sizeof(hsb_demag_plan_s));
     if (!P) return HSB_ERR_NOMEM;
+    P->tensor = tensor;
     for (int a = 0; a < 3; a++) {
         P->N[a] = size[a];
         P->pbc[a] = pbc[a];

@@ -17,6 +17,8 @@ struct ArneGeom {
 };
 
 cudaError_t hsb_arne_launch(const ArneGeom* g, double* Kc, cudaStream_t st);
+// The FP64 Newell tensor K = -N in the same folded layout (hsb_newell.cu).
+cudaError_t hsb_newell_launch(const ArneGeom* g, double* Kc, cudaStream_t st);
 cudaError_t hsb_arne_expand_launch(const double* Kc, int comp, int L0, int L1, int L2, double* out,
                                    cudaStream_t st);
 
@@ -67,6 +69,8 @@ int hsb_demag_spectrum_enqueue(hsb_demag_plan P, const double* cellsize, int acc
                                float* kern, float* kern4, cudaStream_t st);
 extern "C" int hsb_demag_plan_create(const int* size, const double* cellsize, const int* pbc,
                                      int accuracy, void* stream, hsb_demag_plan* out);
+extern "C" int hsb_demag_plan_create_tensor(const int* size, const double* cellsize, const int* pbc, int accuracy,
+                                            int tensor, void* stream, hsb_demag_plan* out);
 extern "C" int hsb_demag_plan_destroy(hsb_demag_plan P);
 // Kernel launches of one convolution (3 fused, 5 multi-pass).
 int hsb_demag_nlaunch(hsb_demag_plan P);

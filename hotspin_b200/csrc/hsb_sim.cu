@@ -64,6 +64,7 @@ struct hsb_sim_desc {
     double maxerr[3];            // rk12: maxError; am12: maxAbsError; bdf-euler: maxIterError (m, Te, Tl)
     double maxrelerr[3];         // am12: maxRelError (m, Te, Tl)
     int32_t max_iter;            // bdf-euler: sweeps per equation
+    int32_t demag_tensor;        // 0 Kernel_Arne, 1 Newell
 };
 
 enum { SOLVER_EULER = 0, SOLVER_HEUN = 1, SOLVER_RK4 = 2, SOLVER_DP45 = 3, SOLVER_RK12 = 4, SOLVER_AM12 = 5,
@@ -1226,6 +1227,10 @@ static int check_desc(const hsb_sim_desc& d, const char* who) {
             return HSB_ERR_INVALID;
         }
     }
+    if (d.demag_tensor != 0 && d.demag_tensor != 1) {
+        hsb_set_error("%s: demag_tensor %d is neither Kernel_Arne (0) nor Newell (1)", who, d.demag_tensor);
+        return HSB_ERR_INVALID;
+    }
     if (d.solver == SOLVER_BDF_EULER && d.max_iter > 64) {
         hsb_set_error("%s: bdf-euler max_iter %d above 64", who, d.max_iter);
         return HSB_ERR_INVALID;
@@ -1311,7 +1316,7 @@ HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     STRY(cudaMallocHost(&S->red_host, sizeof(double) * 16));
     STRY(cudaMemsetAsync(S->red, 0, sizeof(double) * (RED_BLOCKS * 8 + 16) + 64, S->st));
     if (d.demag) {
-        int rc = hsb_demag_plan_create(d.size, d.cellsize, d.pbc, 6, S->st, &S->demag);
+        int rc = hsb_demag_plan_create_tensor(d.size, d.cellsize, d.pbc, 6, d.demag_tensor, S->st, &S->demag);
         if (rc != HSB_OK) {
             free_sim(S);
             return rc;
@@ -1826,7 +1831,7 @@ HSB_EXPORT int hsb_batch_create(const hsb_sim_desc* cls, int32_t nslot, hsb_sim_
     STRY(cudaMallocHost(&S->red_host, sizeof(double) * 16));
     STRY(cudaEventCreateWithFlags(&S->done_ev, cudaEventDisableTiming));
     if (d.demag) {
-        int rc = hsb_demag_plan_create(d.size, d.cellsize, d.pbc, 6, S->st, &S->demag);
+        int rc = hsb_demag_plan_create_tensor(d.size, d.cellsize, d.pbc, 6, d.demag_tensor, S->st, &S->demag);
         if (rc != HSB_OK) {
             free_sim(S);
             return rc;
@@ -1910,6 +1915,7 @@ HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* d
         }
     }
     if (d.solver != c.solver || d.ttm != c.ttm || d.demag != c.demag || (d.thermal && !c.thermal) ||
+        d.demag_tensor != c.demag_tensor ||
         (adaptive_solver(c.solver) && d.rtol != c.rtol) ||
         (c.solver >= SOLVER_RK12 &&
          (d.maxerr[0] != c.maxerr[0] || d.maxerr[1] != c.maxerr[1] || d.maxerr[2] != c.maxerr[2] ||

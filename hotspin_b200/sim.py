@@ -43,6 +43,8 @@ def make_desc(**kw):
             raise KeyError("unknown simulation parameter %r" % k)
         if k == "solver" and isinstance(v, str):
             v = SOLVERS[v.lower()]
+        if k == "demag_tensor" and isinstance(v, str):
+            v = DEMAG_TENSORS[v.lower()]
         cur = getattr(d, k)
         if isinstance(cur, ctypes.Array):
             for i, x in enumerate(v):
@@ -253,12 +255,17 @@ class Batch:
         _lib.check(self._lib.hsb_batch_release(self._h, int(slot)), "hsb_batch_release")
 
 
-def demag_plan(size, cellsize, pbc=(0, 0, 0), accuracy=6, stream=None):
-    """Create a demag plan; returns an opaque handle (ctypes.c_void_p)."""
+DEMAG_TENSORS = {"arne": 0, "newell": 1}
+
+
+def demag_plan(size, cellsize, pbc=(0, 0, 0), accuracy=6, stream=None, tensor="arne"):
+    """Create a demag plan; returns an opaque handle (ctypes.c_void_p).  tensor: "arne"
+    (hotspin's Kernel_Arne) or "newell" (the closed-form FP64 Newell tensor)."""
     lib = _lib.load()
     h = ctypes.c_void_p()
     s = (ctypes.c_int * 3)(*size)
     c = (ctypes.c_double * 3)(*cellsize)
     p = (ctypes.c_int * 3)(*pbc)
-    _lib.check(lib.hsb_demag_plan_create(s, c, p, accuracy, stream, ctypes.byref(h)), "hsb_demag_plan_create")
+    _lib.check(lib.hsb_demag_plan_create_tensor(s, c, p, accuracy, DEMAG_TENSORS[tensor], stream, ctypes.byref(h)),
+               "hsb_demag_plan_create")
     return h

@@ -119,6 +119,7 @@ typedef struct hsb_sim_desc {
     double maxerr[3];
     double maxrelerr[3];
     int32_t max_iter;
+    int32_t demag_tensor;   /* HSB_DEMAG_ARNE (default, the reference's) or HSB_DEMAG_NEWELL */
 } hsb_sim_desc;
 
 typedef struct hsb_sim_s* hsb_sim;
@@ -268,6 +269,14 @@ int hsb_batch_release(hsb_batch b, int32_t slot);
 typedef struct hsb_demag_plan_s* hsb_demag_plan;
 int hsb_demag_plan_create(const int* size, const double* cellsize, const int* pbc, int accuracy,
                           void* stream, hsb_demag_plan* out);
+/* The same with a choice of tensor: HSB_DEMAG_ARNE (hotspin's Kernel_Arne, as above) or
+ * HSB_DEMAG_NEWELL (no reference counterpart: the closed-form cell-averaged tensor of Newell,
+ * Williams and Dunlop (1993) in FP64 on the GPU, near field by its second differences and far
+ * field by the multipole expansion through sixth order; it differs from Kernel_Arne by that
+ * quadrature's error, about 1e-3 of the largest entry at accuracy 6). */
+enum { HSB_DEMAG_ARNE = 0, HSB_DEMAG_NEWELL = 1 };
+int hsb_demag_plan_create_tensor(const int* size, const double* cellsize, const int* pbc, int accuracy,
+                                 int tensor, void* stream, hsb_demag_plan* out);
 int hsb_demag_plan_destroy(hsb_demag_plan plan);
 int hsb_demag_plan_info(hsb_demag_plan plan, int* logic3, int* fused, double* kern_max_imag);
 int hsb_demag_field(hsb_demag_plan plan, const float* m, const float* mask, double msat0T0,

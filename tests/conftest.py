@@ -27,3 +27,21 @@ def cuda():
 def hsb_lib():
     from hotspin_b200 import _lib
     return _lib.load()
+
+
+@pytest.fixture(scope="session")
+def host_rules(tmp_path_factory):
+    """tests/native/rule_check.cu built with nvcc as host code: the device's shared step-control
+    rules and Newell-tensor arithmetic, callable through ctypes without a GPU."""
+    import ctypes
+    import shutil
+    import subprocess
+    nvcc = "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else shutil.which("nvcc")
+    if not nvcc:
+        pytest.skip("nvcc is not available")
+    out = str(tmp_path_factory.mktemp("rules") / "rule_check.so")
+    cmd = [nvcc, "-x", "cu", "-std=c++17", "-O2", "-Xcompiler", "-fPIC", "-shared",
+           "-I" + os.path.join(ROOT, "hotspin_b200", "csrc"), os.path.join(ROOT, "tests", "native", "rule_check.cu"),
+           "-o", out]
+    subprocess.run(cmd, check=True, capture_output=True)
+    return ctypes.CDLL(out)

@@ -76,3 +76,40 @@ extern "C" void imp_rule_host(HsbSolverDev* p, int which, const double* abs_err,
     L.eq = eq;
     hsb_imp_rule(*p, L, which);
 }
+
+// ---- the Newell tensor's shared arithmetic (hsb_newell.cuh), for the oracle comparison
+#include "hsb_newell.cuh"
+
+extern "C" void newell_host(int i, int j, const double* R, const double* cs, double* out3) {
+    out3[0] = newell_exact(i, j, R, cs);
+    out3[1] = newell_asymptotic(i, j, R, cs);
+    out3[2] = newell_N(i, j, R, cs);
+}
+
+// The folded K = -N of a logic grid (program order) as k_newell_kernel computes it:
+// Kc[6][h0+1][h1+1][h2+1].
+extern "C" void newell_kernel_host(const int* L, const int* pbc, const double* cs, double* Kc) {
+    ArneGeom g;
+    for (int a = 0; a < 3; a++) {
+        g.size[a] = L[a];
+        g.cs[a] = cs[a];
+        g.h[a] = L[a] / 2;
+        if (pbc[a] == 0) {
+            g.r1[a] = -(long)((L[a] - 1) / 2);
+            g.r2[a] = (long)((L[a] - 1) / 2);
+        } else {
+            g.r1[a] = -((long)L[a] * pbc[a] - 1);
+            g.r2[a] = (long)L[a] * pbc[a] - 1;
+        }
+    }
+    if (L[2] == 1 && pbc[2] == 0) g.r2[2] = 0;
+    const long n1 = g.h[1] + 1, n2 = g.h[2] + 1, ncell = (g.h[0] + 1) * n1 * n2;
+    const int full[3][3] = {{KXX, KXY, KXZ}, {KXY, KYY, KYZ}, {KXZ, KYZ, KZZ}};
+    for (long q = 0; q < 3 * ncell; q++) {
+        const int s = (int)(q / ncell);
+        const long c = q - s * ncell;
+        double acc[3];
+        newell_target(g, s, (int)(c / (n1 * n2)), (int)((c / n2) % n1), (int)(c % n2), acc);
+        for (int d = s; d < 3; d++) Kc[(long)full[s][d] * ncell + c] = acc[d];
+    }
+}

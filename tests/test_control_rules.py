@@ -7,29 +7,14 @@ through ctypes on random and boundary error sequences.
 """
 import ctypes
 import math
-import os
-import shutil
-import subprocess
-
 import numpy as np
 import pytest
 
 from oracle.solvers import rk12_rule
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-NVCC = "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else shutil.which("nvcc")
-
-
 @pytest.fixture(scope="module")
-def rules(tmp_path_factory):
-    if not NVCC:
-        pytest.skip("nvcc is not available")
-    out = str(tmp_path_factory.mktemp("rules") / "rule_check.so")
-    cmd = [NVCC, "-x", "cu", "-std=c++17", "-O2", "-Xcompiler", "-fPIC", "-shared",
-           "-I" + os.path.join(ROOT, "hotspin_b200", "csrc"), os.path.join(ROOT, "tests", "native", "rule_check.cu"),
-           "-o", out]
-    subprocess.run(cmd, check=True, capture_output=True)
-    lib = ctypes.CDLL(out)
+def rules(host_rules):
+    lib = host_rules
     lib.rk12_rule_host.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double), ctypes.c_int,
                                    ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
