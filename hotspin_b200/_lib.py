@@ -54,6 +54,8 @@ _SIGS = {
     "hsb_sim_destroy": (c_int, [c_vp]),
     "hsb_sim_set": (c_int, [c_vp, ctypes.c_char_p, c_dp, c_i64]),
     "hsb_sim_get": (c_int, [c_vp, ctypes.c_char_p, c_dp, c_i64]),
+    "hsb_sim_set_device": (c_int, [c_vp, ctypes.c_char_p, c_vp, c_i64]),
+    "hsb_sim_get_device": (c_int, [c_vp, ctypes.c_char_p, c_vp, c_i64]),
     "hsb_sim_step": (c_int, [c_vp, c_i64]),
     "hsb_sim_run_until": (c_int, [c_vp, c_dbl]),
     "hsb_sim_sync": (c_int, [c_vp]),

@@ -1479,6 +1479,56 @@ HSB_EXPORT int hsb_sim_get(hsb_sim_s* S, const char* name, double* host, int64_t
     return HSB_OK;
 }
 
+// State transfer between the handle and caller-owned FP64 device arrays (SoA, program order;
+// hotspin's gpu.Array layout, gpu/array.go:26-37), enqueued on the handle's stream and
+// completed before return: the conversion kernels read or write the caller's array directly,
+// with no host copy and no allocation.  name: "m", "Te", "Tl".
+HSB_EXPORT int hsb_sim_set_device(hsb_sim_s* S, const char* name, const double* dev, int64_t count) {
+    RC(plain_only(S, "hsb_sim_set_device"));
+    if (!S || !name || !dev) {
+        hsb_set_error("hsb_sim_set_device: null argument");
+        return HSB_ERR_INVALID;
+    }
+    int first, nc;
+    RC(channel_of(S, name, &first, &nc));
+    if (count != (int64_t)nc * S->n) {
+        hsb_set_error("hsb_sim_set_device(%s): expected %ld values, got %ld", name, (long)nc * S->n, (long)count);
+        return HSB_ERR_INVALID;
+    }
+    if (!S->sd_fresh) RC(get_sd(S));
+    float* y = S->y[S->sd_host->cur];
+    k_d2f<<<hsb_grid_1d(count, 256), 256, 0, S->st>>>(dev, y + (long)first * S->n, count);
+    HSB_CUDA_TRY(cudaGetLastError());
+    S->initialized = false;
+    if (S->sd_host->status) {
+        S->sd_host->status = 0;
+        RC(set_sd_fields(S));
+    }
+    HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
+    S->sd_fresh = true;
+    return HSB_OK;
+}
+
+HSB_EXPORT int hsb_sim_get_device(hsb_sim_s* S, const char* name, double* dev, int64_t count) {
+    RC(plain_only(S, "hsb_sim_get_device"));
+    if (!S || !name || !dev) {
+        hsb_set_error("hsb_sim_get_device: null argument");
+        return HSB_ERR_INVALID;
+    }
+    int first, nc;
+    RC(channel_of(S, name, &first, &nc));
+    if (count != (int64_t)nc * S->n) {
+        hsb_set_error("hsb_sim_get_device(%s): expected %ld values, got %ld", name, (long)nc * S->n, (long)count);
+        return HSB_ERR_INVALID;
+    }
+    if (!S->sd_fresh) RC(get_sd(S));
+    const float* y = S->y[S->sd_host->cur];
+    k_f2d<<<hsb_grid_1d(count, 256), 256, 0, S->st>>>(y + (long)first * S->n, dev, count);
+    HSB_CUDA_TRY(cudaGetLastError());
+    HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
+    return HSB_OK;
+}
+
 HSB_EXPORT int hsb_sim_step(hsb_sim_s* S, int64_t nsteps) {
     if (!S || nsteps < 0) {
         hsb_set_error("hsb_sim_step: bad argument");

@@ -146,6 +146,11 @@ int hsb_sim_destroy(hsb_sim sim);
  * describe the state it replaces.  A page-locked host array is copied by DMA directly. */
 int hsb_sim_set(hsb_sim sim, const char* name, const double* host, int64_t count);
 int hsb_sim_get(hsb_sim sim, const char* name, double* host, int64_t count);
+/* The same for caller-owned FP64 device arrays (hotspin's gpu.Array layout, SoA program order;
+ * no reference counterpart): "m", "Te", "Tl" converted on the device, no host copy, no
+ * allocation; completed before return. */
+int hsb_sim_set_device(hsb_sim sim, const char* name, const double* dev, int64_t count);
+int hsb_sim_get_device(hsb_sim sim, const char* name, double* dev, int64_t count);
 
 /* Advance `nsteps` accepted steps / up to time t.  Asynchronous on the handle's stream
  * except for the periodic completion checks of the adaptive solver. */

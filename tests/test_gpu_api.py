@@ -85,3 +85,29 @@ def test_stdproblem4_geometry_short_run(cuda):
     assert np.abs(got - want).max() < 1e-5
     assert e.getv("t") == pytest.approx(200 * 50e-15)
     e._reset()
+
+
+def test_device_array_transfers(cuda):
+    """hsb_sim_set_device / hsb_sim_get_device move the state to and from caller-owned FP64
+    device arrays (the layout of hotspin's gpu.Array) and equal the host transfers."""
+    import ctypes
+
+    from hotspin_b200 import _lib
+    from hotspin_b200.sim import Simulation
+    size = (2, 8, 16)
+    rng = np.random.default_rng(21)
+    m = rng.normal(size=(3,) + size)
+    m /= np.sqrt((m * m).sum(0))
+    with Simulation(size=size, cellsize=(2e-9,) * 3, msat0T0=8e5, solver="rk4", dt=1e-15, ttm=True, llb=True,
+                    tc=630.0, spin_j=0.5, n_spins=1e28, gamma_e=700.0, c_l=3e6, temperature=300.0) as sim:
+        dm = cuda.from_numpy(m).cuda()
+        _lib.check(sim._lib.hsb_sim_set_device(sim._h, b"m", ctypes.c_void_p(dm.data_ptr()), dm.numel()))
+        np.testing.assert_array_equal(sim.get("m"), m.astype(np.float32).astype(np.float64))
+        Te = cuda.full(size, 412.5, dtype=cuda.float64, device="cuda")
+        _lib.check(sim._lib.hsb_sim_set_device(sim._h, b"Te", ctypes.c_void_p(Te.data_ptr()), Te.numel()))
+        back = cuda.empty((3,) + size, dtype=cuda.float64, device="cuda")
+        _lib.check(sim._lib.hsb_sim_get_device(sim._h, b"m", ctypes.c_void_p(back.data_ptr()), back.numel()))
+        np.testing.assert_array_equal(back.cpu().numpy(), sim.get("m"))
+        assert float(sim.get("Te").max()) == 412.5
+        rc = sim._lib.hsb_sim_get_device(sim._h, b"m", ctypes.c_void_p(back.data_ptr()), 7)
+        assert rc == 1
