@@ -410,8 +410,10 @@ class RefSim:
             self.sync()
             err = self._maxabs(self.err[:3]) / self.rtol
             if self.ttm:
-                L.divAsync(p(self.err[3]), p(self.err[3]), p(self.ys[3]), s, I(self.n))
-                L.divAsync(p(self.err[4]), p(self.err[4]), p(self.ys[4]), s, I(self.n))
+                # temperatures relative to max(|T0|, |T|), the norm of the device and the oracle
+                # (the reference has no DP45 to take it from)
+                scale = self.torch.maximum(y0[3:].abs(), self.ys[3:].abs())
+                self.err[3:] /= scale
                 self.sync()
                 err = max(err, self._maxabs(self.err[3:]) / self.rtol)
             self.attempts += 1
