@@ -372,7 +372,7 @@ def run_ours(args):
     e2e_run()                     # untimed: builds the one-step graph
     e2e_s = statistics.median([e2e_run() for _ in range(3)])
     h2d = sum(v.nbytes for v in host_state.values())
-    per_step_d2h = 112            # the 112-byte solver block each step call reads back
+    per_step_d2h = _lib.load().hsb_solver_word_bytes()   # the solver word each step call reads back
     d2h = mout.nbytes + args.steps * per_step_d2h
     e2e = {"value": round(world * ncell * args.steps / e2e_s / 1e6, 3), "unit": UNIT,
            "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),

@@ -49,6 +49,7 @@ _SIGS = {
     "hsb_clear_error": (None, []),
     "hsb_version": (c_int, []),
     "hsb_sim_desc_bytes": (c_int, []),
+    "hsb_solver_word_bytes": (c_int, []),
     "hsb_crc64_iso": (ctypes.c_uint64, [c_vp, ctypes.c_int64]),
     "hsb_sim_create": (c_int, [ctypes.POINTER(SimDesc), ctypes.POINTER(c_vp)]),
     "hsb_sim_destroy": (c_int, [c_vp]),

@@ -1281,6 +1281,9 @@ static int check_desc(const hsb_sim_desc& d, const char* who) {
 // Size of the descriptor as compiled into the library, for bindings to check their layout.
 HSB_EXPORT int hsb_sim_desc_bytes(void) { return (int)sizeof(hsb_sim_desc); }
 
+// Bytes of the device solver word a step call reads back (the per-step device-to-host read).
+HSB_EXPORT int hsb_solver_word_bytes(void) { return (int)sizeof(HsbSolverDev); }
+
 HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     if (!desc || !out) {
         hsb_set_error("hsb_sim_create: null argument");

@@ -130,6 +130,9 @@ int hsb_version(void);
 /* sizeof(hsb_sim_desc) as compiled into the library (no reference counterpart): a binding
  * compares it with its own mirror of the struct. */
 int hsb_sim_desc_bytes(void);
+/* Bytes of the device solver word that each step call reads back (no reference
+ * counterpart): the per-step device-to-host read of a stepping loop. */
+int hsb_solver_word_bytes(void);
 /* CRC-64 (ISO polynomial, Go hash/crc64 convention) that seals a #dump002 frame
  * (dump/writer.go:46-76); host function, no GPU needed.  Used by hotspin_b200.dump. */
 uint64_t hsb_crc64_iso(const void* data, int64_t n);

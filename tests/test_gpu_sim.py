@@ -263,37 +263,6 @@ def test_stage_tuning_picks_a_variant(cuda):
         assert lib.hsb_stage_variant_of(sim._h) in (1, 2, 4)
 
 
-def test_thermal_dp45_equilibrium_is_boltzmann(cuda):
-    """Uncoupled LLG macrospins (|m| = 1) in a field B along program axis 0 at temperature T,
-    integrated by DP45 with the Brown thermal field: the ensemble- and time-averaged m_0
-    approaches the Langevin function L(xi) = coth xi - 1/xi, xi = Ms V B / (kB T), of the
-    Boltzmann distribution on the sphere.  lambda = 0.05 keeps the (1 + lambda^2) temperature
-    factor of the Landau-Lifshitz form at 0.25 % (a shift of 1e-3 in L)."""
-    size, cs, ms, T, B, lam = (1, 64, 64), 3e-9, 8e5, 300.0, 0.383, 0.05
-    xi = ms * cs ** 3 * B / (F.KB * T)
-    want = 1.0 / np.tanh(xi) - 1.0 / xi
-    kw = dict(size=size, cellsize=(cs,) * 3, msat0T0=ms, gamma_ll=F.GAMMA0, alpha=(lam,) * 3, normalize=True,
-              b_ext=(B, 0.0, 0.0), thermal=True, seed=7, temperature=T, solver="dp45", dt=1e-14, rtol=1e-5,
-              mindt=1e-18, maxdt=1e-12)
-    samples = []
-    with Simulation(**kw) as sim:
-        m = np.zeros((3,) + size)
-        m[0] = 1.0
-        sim.set("m", m)
-        t = 0.6e-9                       # relaxation time 1 / (lambda gamma B) ~ 0.3 ns
-        sim.run_until(t)
-        for _ in range(20):
-            t += 0.05e-9
-            sim.run_until(t)
-            samples.append(float(sim.get("m")[0].mean()))
-        steps = sim.status()["steps"]
-    got = float(np.mean(samples))
-    print("\n[thermal dp45] xi %.3f  <m0> %.4f  Langevin %.4f  steps %d" % (xi, got, want, steps))
-    # 4096 spins x ~10 decorrelated samples: standard error ~0.002
-    assert abs(got - want) < 0.015
-
-
-
 def test_dump_of_a_simulation(cuda, tmp_path):
     """hotspin_b200.dump.write_simulation writes the handle's m and time as a #dump002 frame."""
     from hotspin_b200 import dump

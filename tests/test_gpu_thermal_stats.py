@@ -60,6 +60,30 @@ def test_same_stream_ensemble_matches_oracle_3sigma(cuda, T):
     assert abs(a[1] - b[1]) < 3 * np.hypot(a[3], b[3])
 
 
+@pytest.mark.parametrize("T", [150.0, 600.0])
+def test_dp45_same_stream_ensemble_matches_oracle_3sigma(cuda, T):
+    """The adaptive DP45 path with the thermal field (the benchmark's integrator): step sizes
+    follow FP32 vs FP64 error estimates, so trajectories separate at the noise scale, and the
+    ensembles are compared statistically."""
+    size, B = (1, 64, 64), 0.2
+    kw = _kw(size, T, B, seed=41)
+    rng = np.random.default_rng(19)
+    m0 = rng.normal(size=(3,) + size)
+    m0 /= np.sqrt((m0 * m0).sum(0))
+    t_end = 5e-12
+    it = Integrator(Model(Spec(**kw)), {"m": m0}, "dp45", 1e-15, rtol=1e-5, mindt=1e-20, maxdt=1e-12)
+    it.run_until(t_end)
+    with Simulation(**kw, solver="dp45", dt=1e-15, rtol=1e-5, mindt=1e-20, maxdt=1e-12) as sim:
+        sim.set("m", m0)
+        sim.run_until(t_end)
+        m = sim.get("m")
+    for c in range(3):
+        a = _moments(m[c].ravel())
+        b = _moments(it.y["m"][c].ravel())
+        assert abs(a[0] - b[0]) < 3 * np.hypot(a[2], b[2]), (c, a, b)
+        assert abs(a[1] - b[1]) < 3 * np.hypot(a[3], b[3]), (c, a, b)
+
+
 @pytest.mark.parametrize("T", [150.0, 300.0, 600.0])
 def test_equilibrium_is_boltzmann_3sigma(cuda, T):
     size, B, dt = (4, 128, 128), 0.383, 2e-14
