@@ -113,3 +113,41 @@ extern "C" void newell_kernel_host(const int* L, const int* pbc, const double* c
         for (int d = s; d < 3; d++) Kc[(long)full[s][d] * ncell + c] = acc[d];
     }
 }
+
+// ---- Kernel_Arne's quadrature split over the lanes of a warp (hsb_arne.cuh)
+#include "hsb_arne.cuh"
+
+// The folded Kernel_Arne tensor Kc[6][h0+1][h1+1][h2+1] of a logic grid with every target's
+// quadrature split into `nparts` shares that are summed afterwards, as k_arne_kernel's lanes do.
+extern "C" void arne_kernel_host(const int* L, const int* pbc, const double* cs, int accuracy, int nparts,
+                                 double* Kc) {
+    ArneGeom g;
+    for (int a = 0; a < 3; a++) {
+        g.size[a] = L[a];
+        g.cs[a] = cs[a];
+        g.h[a] = L[a] / 2;
+        if (pbc[a] == 0) {
+            g.r1[a] = -(long)((L[a] - 1) / 2);
+            g.r2[a] = (long)((L[a] - 1) / 2);
+        } else {
+            g.r1[a] = -((long)L[a] * pbc[a] - 1);
+            g.r2[a] = (long)L[a] * pbc[a] - 1;
+        }
+    }
+    if (L[2] == 1 && pbc[2] == 0) g.r2[2] = 0;
+    g.Lmin = fmin(cs[0], fmin(cs[1], cs[2]));
+    g.accuracy = (double)accuracy;
+    const long n1 = g.h[1] + 1, n2 = g.h[2] + 1, ncell = (g.h[0] + 1) * n1 * n2;
+    const int full[3][3] = {{KXX, KXY, KXZ}, {KXY, KYY, KYZ}, {KXZ, KYZ, KZZ}};
+    for (long q = 0; q < 3 * ncell; q++) {
+        const int s = (int)(q / ncell);
+        const long c = q - s * ncell;
+        double acc[3] = {0, 0, 0};
+        for (int part = 0; part < nparts; part++) {
+            double p[3];
+            arne_target_part(g, s, (int)(c / (n1 * n2)), (int)((c / n2) % n1), (int)(c % n2), part, nparts, p);
+            for (int d = s; d < 3; d++) acc[d] += p[d];
+        }
+        for (int d = s; d < 3; d++) Kc[(long)full[s][d] * ncell + c] = acc[d];
+    }
+}

@@ -104,3 +104,24 @@ def test_folded_kernel_matches_oracle_and_stays_near_arne(lib, size, cs, pbc):
     print("\n[newell vs Kernel_Arne] size %s cells %s pbc %s: max |K_newell - K_arne| = %.1e of max |K_ii|"
           % (size, cs, pbc, diff))
     assert diff < 2e-3
+
+
+@pytest.mark.parametrize("size,cs,pbc", CASES)
+def test_arne_quadrature_split_over_lanes_matches_oracle(host_rules, size, cs, pbc):
+    """k_arne_kernel splits each target's quadrature over the 32 lanes of a warp; the shares,
+    summed, equal the oracle's sequential Kernel_Arne (oracle/csrc, the reference's order) to
+    rounding."""
+    f = host_rules.arne_kernel_host
+    f.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                  ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    f.restype = None
+    logic = demag.pad_size(size, pbc)
+    h = [l // 2 for l in logic]
+    want = native.kernel_arne(logic, cs, pbc, 6)[:, :h[0] + 1, :h[1] + 1, :h[2] + 1]
+    scale = np.abs(want[:3]).max()
+    for nparts in (1, 32):
+        K = np.zeros((6, h[0] + 1, h[1] + 1, h[2] + 1))
+        f((ctypes.c_int * 3)(*logic), (ctypes.c_int * 3)(*pbc), D3(*cs), 6, nparts,
+          K.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        # a different order of summation over up to 31104 points of cancelling contributions
+        assert np.abs(K - want).max() <= (0.0 if nparts == 1 else 1e-12) * scale, nparts
