@@ -381,6 +381,29 @@ class RefSim:
         self.t = t0 + dt
         self.steps += 1
 
+    def step_rk4(self):
+        """One classic RK4 step composed from the reference's madd kernels, every stage point
+        and the new state renormalised when the normalizer is loaded (the device's RK4; the
+        reference has no RK4)."""
+        L, p, s = self.lib, self.p, self.sh
+        nn = self.nch * self.n
+        h, t0 = self.dt, self.t
+        self._normalize(self.y)
+        k = self.k
+        self.rhs(t0, self.y, k[0])
+        for i, (c, tf) in enumerate(((0.5, 0.5), (0.5, 0.5), (1.0, 1.0))):
+            L.maddAsync(p(self.ys), p(self.y), p(k[i]), D(c * h), s, I(nn))
+            self.sync()
+            self._normalize(self.ys)
+            self.rhs(t0 + tf * h, self.ys, k[i + 1])
+        for i, w in enumerate((1.0, 2.0, 2.0, 1.0)):
+            L.madd1Async(p(self.y), p(k[i]), D(w * h / 6.0), s, I(nn))
+        self.sync()
+        self._normalize(self.y)
+        self.t = t0 + h
+        self.steps += 1
+        self.attempts += 1
+
     def _maxabs(self, a):
         L, p, s = self.lib, self.p, self.sh
         nn = a.numel()
