@@ -1119,6 +1119,11 @@ struct hsb_demag_plan_s {
     float2* tw4c;       // four-step twiddles of the y columns (length L1, or 1024 for yc2k)
     int zdirect;        // the y/z kernel convolves z directly: kern4 rows d < N0 hold k_zdirect
     int tensor;         // HSB_DEMAG_ARNE (0) or HSB_DEMAG_NEWELL (1)
+    // Grids whose open axes do not pad to a power of two run embedded in the next power-of-two
+    // grid (vacuum around them): `inner` is that grid's plan, mpad / hpad its m and H.
+    hsb_demag_plan_s* inner;
+    float* mpad;
+    float* hpad;
     float2* tw4z;       // and of the z transform (length L0)
 };
 
@@ -1430,11 +1435,46 @@ HSB_EXPORT int hsb_demag_plan_create_tensor(const int* size, const double* cells
             return HSB_ERR_INVALID;
         }
         P->L[a] = (size[a] > 1 && pbc[a] == 0) ? 2 * size[a] : size[a];
-        if (!is_pow2(P->L[a])) {
-            hsb_set_error("hsb_demag_plan_create: padded size %d on axis %d is not a power of two", P->L[a], a);
+        if (!is_pow2(P->L[a]) && pbc[a] != 0) {
+            hsb_set_error("hsb_demag_plan_create: periodic axis %d of %d cells is not a power of two", a, size[a]);
             free(P);
             return HSB_ERR_UNSUPPORTED;
         }
+    }
+    if (!is_pow2(P->L[0]) || !is_pow2(P->L[1]) || !is_pow2(P->L[2])) {
+        // Open axes whose padded size 2N is not a power of two: the convolution runs on the grid
+        // of next_pow2(N) cells along them, the N cells at its origin and vacuum (m = 0)
+        // beyond.  The reference pads to 2N (engine/zeropad.go:12-22); any padding of at
+        // least 2N - 1 gives the same linear convolution, and Kernel_Arne's entries for the
+        // offsets |d| <= N - 1 that reach the N cells do not depend on the padded size.
+        int in[3];
+        for (int a = 0; a < 3; a++) {
+            in[a] = size[a];
+            if (pbc[a] == 0 && size[a] > 1)
+                while (!is_pow2(in[a])) in[a]++;
+        }
+        int rc = hsb_demag_plan_create_tensor(in, cellsize, pbc, accuracy, tensor, stream, &P->inner);
+        if (rc != HSB_OK) {
+            free(P);
+            return rc;
+        }
+        const long ninner = 3L * in[0] * in[1] * in[2];
+        if (cudaMalloc(&P->mpad, sizeof(float) * ninner) != cudaSuccess ||
+            cudaMalloc(&P->hpad, sizeof(float) * ninner) != cudaSuccess) {
+            hsb_set_error("hsb_demag_plan_create: cudaMalloc of the embedding buffers failed");
+            hsb_demag_plan_destroy(P);
+            return HSB_ERR_NOMEM;
+        }
+        // zero once: the vacuum cells of mpad are never written
+        if (cudaMemset(P->mpad, 0, sizeof(float) * ninner) != cudaSuccess) {
+            hsb_set_error("hsb_demag_plan_create: cudaMemset failed");
+            hsb_demag_plan_destroy(P);
+            return HSB_ERR_CUDA;
+        }
+        for (int a = 0; a < 3; a++) P->L[a] = P->inner->L[a];
+        P->C2 = P->inner->C2;
+        *out = P;
+        return HSB_OK;
     }
     if (P->L[2] < 2 || P->L[0] > 4096 || P->L[1] > 4096 || P->L[2] > 8192) {
         hsb_set_error("hsb_demag_plan_create: padded size (%d,%d,%d) outside 2..4096 (a2 >= 2)", P->L[0], P->L[1], P->L[2]);
@@ -1573,6 +1613,9 @@ HSB_EXPORT int hsb_demag_plan_create_tensor(const int* size, const double* cells
 
 HSB_EXPORT int hsb_demag_plan_destroy(hsb_demag_plan P) {
     if (!P) return HSB_OK;
+    if (P->inner) hsb_demag_plan_destroy(P->inner);
+    cudaFree(P->mpad);
+    cudaFree(P->hpad);
     cudaFree(P->kern);
     cudaFree(P->kern4);
     cudaFree(P->tw4x);
@@ -1586,11 +1629,15 @@ HSB_EXPORT int hsb_demag_plan_destroy(hsb_demag_plan P) {
     return HSB_OK;
 }
 
-int hsb_demag_nlaunch(hsb_demag_plan P) { return P ? ((P->yz4 || P->fused) ? 3 : 5) : 0; }
+int hsb_demag_nlaunch(hsb_demag_plan P) {
+    if (P && P->inner) return hsb_demag_nlaunch(P->inner) + 2;
+    return P ? ((P->yz4 || P->fused) ? 3 : 5) : 0;
+}
 
 HSB_EXPORT int hsb_demag_plan_info(hsb_demag_plan P, int* logic, int* fused, double* max_imag) {
     if (!P) return HSB_ERR_INVALID;
     if (logic) for (int a = 0; a < 3; a++) logic[a] = P->L[a];
+    if (P->inner) P = P->inner;
     if (fused) *fused = P->fused;
     if (max_imag) *max_imag = P->kern_max_imag;
     return HSB_OK;
@@ -1598,12 +1645,75 @@ HSB_EXPORT int hsb_demag_plan_info(hsb_demag_plan P, int* logic, int* fused, dou
 
 // Launch the convolution: H (A/m, FP32 SoA [3][N0][N1][N2]) = Ms0 * K (*) (m * mask).
 long hsb_demag_x1_bytes(hsb_demag_plan P) {
-    if (!P || !P->xfwd4 || !P->yz4 || !P->xinv4) return 0;
+    if (!P || P->inner || !P->xfwd4 || !P->yz4 || !P->xinv4) return 0;
     return 3L * P->N[0] * P->C2 * P->N[1] * (long)sizeof(float2);
+}
+
+// Embedding of an N-cell grid in the plan's power-of-two grid of M cells (M >= N per axis): m
+// (times the optional Ms mask) into the first N cells of each axis; the other cells were zeroed
+// at plan creation and stay zero.  Reads m[(*msel) ^ minv] as the x kernels do.
+__global__ void k_demag_embed(const float* __restrict__ m0, const float* __restrict__ m1, const int* msel, int minv,
+                              const float* __restrict__ mask, int N0, int N1, int N2, int M0, int M1, int M2,
+                              float* __restrict__ mpad, const int* active) {
+    if (active && !*active) return;
+    const float* m = (msel && ((*msel) ^ minv)) ? m1 : m0;
+    const long n = (long)N0 * N1 * N2, npad = (long)M0 * M1 * M2;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < 3 * n; q += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(q / n);
+        const long i = q - c * n;
+        const int i2 = (int)(i % N2);
+        const long r = i / N2;
+        const int i1 = (int)(r % N1);
+        const int i0 = (int)(r / N1);
+        const float v = m[q];
+        mpad[c * npad + ((long)i0 * M1 + i1) * M2 + i2] = mask ? v * mask[i] : v;
+    }
+}
+
+// The field of the N cells back out of the embedding grid, into h[(*hsel) ^ hinv].
+__global__ void k_demag_extract(const float* __restrict__ hpad, float* h0, float* h1, const int* hsel, int hinv,
+                                int N0, int N1, int N2, int M0, int M1, int M2, const int* active) {
+    if (active && !*active) return;
+    float* h = (hsel && ((*hsel) ^ hinv)) ? h1 : h0;
+    const long n = (long)N0 * N1 * N2, npad = (long)M0 * M1 * M2;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < 3 * n; q += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(q / n);
+        const long i = q - c * n;
+        const int i2 = (int)(i % N2);
+        const long r = i / N2;
+        const int i1 = (int)(r % N1);
+        const int i0 = (int)(r / N1);
+        h[q] = hpad[c * npad + ((long)i0 * M1 + i1) * M2 + i2];
+    }
 }
 
 int hsb_demag_launch(hsb_demag_plan P, const HsbDemagIO& io, const float* mask, float ms0,
                      cudaStream_t st, const int* active, const HsbDemagBatch* batch) {
+    if (P->inner) {
+        if (batch) {
+            hsb_set_error("hsb_demag_launch: batches need padded sizes that are powers of two");
+            return HSB_ERR_UNSUPPORTED;
+        }
+        const hsb_demag_plan_s* Q = P->inner;
+        const long n3 = 3L * P->N[0] * P->N[1] * P->N[2];
+        const int grid = hsb_grid_1d(n3, 256);
+        k_demag_embed<<<grid, 256, 0, st>>>(io.m[0], io.m[1], io.msel, io.minv, mask, P->N[0], P->N[1], P->N[2],
+                                            Q->N[0], Q->N[1], Q->N[2], P->mpad, active);
+        HsbDemagIO inner = {};
+        inner.m[0] = inner.m[1] = P->mpad;
+        inner.h[0] = inner.h[1] = P->hpad;
+        inner.ev = io.ev;
+        int rc = hsb_demag_launch(P->inner, inner, nullptr, ms0, st, active, nullptr);
+        if (rc != HSB_OK) return rc;
+        k_demag_extract<<<grid, 256, 0, st>>>(P->hpad, io.h[0], io.h[1], io.hsel, io.hinv, P->N[0], P->N[1],
+                                              P->N[2], Q->N[0], Q->N[1], Q->N[2], active);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            hsb_set_error("hsb_demag_launch: %s", cudaGetErrorString(e));
+            return HSB_ERR_CUDA;
+        }
+        return HSB_OK;
+    }
     const int N0 = P->N[0], N1 = P->N[1], N2 = P->N[2];
     const int L0 = P->L[0], L1 = P->L[1], L2 = P->L[2];
     const int C2 = P->C2;
@@ -1735,6 +1845,7 @@ HSB_EXPORT int hsb_demag_profile(hsb_demag_plan P, const float* m, const float* 
 
 HSB_EXPORT int hsb_demag_kernel_copy(hsb_demag_plan P, float* host_out, long count) {
     if (!P || !host_out) return HSB_ERR_INVALID;
+    if (P->inner) P = P->inner;
     const long kcount = (long)P->C2 * (P->L[1] / 2 + 1) * (P->L[0] / 2 + 1) * 6;
     if (count < kcount) {
         hsb_set_error("hsb_demag_kernel_copy: need %ld floats", kcount);

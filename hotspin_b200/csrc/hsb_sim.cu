@@ -1820,6 +1820,13 @@ static int batch_check_class(const hsb_sim_desc& d, int32_t nslot, const char* w
                       d.size[2]);
         return HSB_ERR_UNSUPPORTED;
     }
+    for (int a = 0; a < 3; a++) {
+        const int n = d.size[a];
+        if (d.demag && (n & (n - 1)) != 0) {
+            hsb_set_error("%s: batches with demag need sizes that are powers of two, got %d on axis %d", who, n, a);
+            return HSB_ERR_UNSUPPORTED;
+        }
+    }
     return HSB_OK;
 }
 

@@ -93,9 +93,11 @@ def test_limits_are_checked_before_any_device_work():
     assert rc == 1 and b"llb" in msg
     lib = _lib.load()
     plan = ctypes.c_void_p()
-    size = (ctypes.c_int * 3)(3, 8, 8)          # padded z length 6
+    # an open axis whose padding is not a power of two runs embedded in a larger grid; a
+    # periodic one cannot (its transform length is the grid's own) and is refused
+    size = (ctypes.c_int * 3)(3, 8, 8)
     cs = (ctypes.c_double * 3)(1e-9, 1e-9, 1e-9)
-    pbc = (ctypes.c_int * 3)(0, 0, 0)
+    pbc = (ctypes.c_int * 3)(1, 0, 0)
     assert lib.hsb_demag_plan_create(size, cs, pbc, 6, None, ctypes.byref(plan)) == 4
     assert b"power of two" in lib.hsb_last_error()
 
@@ -111,6 +113,9 @@ def test_batches_refuse_what_they_do_not_support():
     assert b"batches" in lib.hsb_last_error()
     d = _desc(size=(1, 8, 8), solver="dp45")
     assert lib.hsb_batch_footprint(ctypes.byref(d), 0, ctypes.byref(nbytes)) == 1
+    d = _desc(size=(1, 12, 8), solver="dp45", demag=True)  # demag classes: powers of two only
+    assert lib.hsb_batch_footprint(ctypes.byref(d), 4, ctypes.byref(nbytes)) == 4
+    assert b"powers of two" in lib.hsb_last_error()
 
 
 def test_dropins_export_every_name_the_go_sequence_replay_binds():

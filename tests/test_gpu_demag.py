@@ -103,3 +103,31 @@ def test_demag_golden_64cube(cuda):
 def test_unsupported_size_is_rejected(cuda):
     with pytest.raises(_lib.HsbError):
         demag_plan((3, 5, 6), (1e-9,) * 3, (1, 1, 1))
+
+
+@pytest.mark.parametrize("size,cs,pbc", [((3, 12, 20), (2e-9, 3e-9, 4e-9), (0, 0, 0)),
+                                         ((1, 25, 100), (3e-9, 5e-9, 5e-9), (0, 0, 0)),
+                                         ((4, 12, 16), (2e-9, 2e-9, 2e-9), (2, 0, 0))])
+def test_demag_on_grids_that_do_not_pad_to_powers_of_two(cuda, size, cs, pbc):
+    """Open axes whose padded size 2N is not a power of two (the reference's cuFFT takes any
+    size): the plan embeds the grid in the next power-of-two grid, and the field equals the
+    oracle's convolution padded to 2N as the reference pads it."""
+    rng = np.random.default_rng(8)
+    m = rng.normal(size=(3,) + size)
+    m /= np.sqrt((m * m).sum(0))
+    mask = rng.uniform(0.2, 1.0, size=size)
+    logic = demag.pad_size(size, pbc)
+    Kf = demag.kernel_spectrum(native.kernel_arne(logic, cs, pbc))
+    want = demag.demag_field(m, mask, 8e5, Kf, logic) / demag.MU0
+    plan = demag_plan(size, cs, pbc)
+    try:
+        dm = dev(cuda, m, np.float32)
+        dk = dev(cuda, mask, np.float32)
+        H = cuda.empty_like(dm)
+        _lib.check(_lib.load().hsb_demag_field(plan, ptr(dm), ptr(dk), 8e5, ptr(H), None))
+        assert rel_err(host(cuda, H), want) < 2e-5
+        _lib.check(_lib.load().hsb_demag_field(plan, ptr(dm), None, 8e5, ptr(H), None))
+        want2 = demag.demag_field(m, None, 8e5, Kf, logic) / demag.MU0
+        assert rel_err(host(cuda, H), want2) < 2e-5
+    finally:
+        _lib.load().hsb_demag_plan_destroy(plan)
