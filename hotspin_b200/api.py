@@ -10,7 +10,8 @@ everything is converted to program order (z, y, x) exactly as ``engine/api.go:41
 ``common/index.go:68-113`` do.
 
 Supported modules: exchange6, demag, zeeman, anisotropy/uniaxial, llbar, llbar/torque,
-llbar/damping/nonconservative/00/local, normalizer, mfa/longfield, mfa/msat0,
+llbar/damping/nonconservative/00/local, llbar/damping/nonconservative/02/local (setv('μ∥',
+...)), llbar/damping/conservative/02/local (setv('μ⊥', ...)), normalizer, mfa/longfield, mfa/msat0,
 temperature/brown, temperature/ETM, temperature/PTM, temperature/E-P, temperature/Drude,
 temperature/ETM/diffusion, solver/euler, solver/heun, solver/rk12 (errors per step set with
 setv('m_maxerror' / 'Te_maxerror' / 'Tp_maxerror', ...)), solver/am12 ('<q>_maxabserror',
@@ -28,7 +29,8 @@ MUB = 9.27400968202020202e-24
 
 SUPPORTED = {
     "exchange6", "demag", "zeeman", "anisotropy/uniaxial", "llbar", "llbar/torque",
-    "llbar/damping/nonconservative/00/local", "normalizer", "mfa/longfield", "mfa/msat0",
+    "llbar/damping/nonconservative/00/local", "llbar/damping/nonconservative/02/local",
+    "llbar/damping/conservative/02/local", "normalizer", "mfa/longfield", "mfa/msat0",
     "temperature/brown", "temperature/ETM", "temperature/PTM", "temperature/E-P",
     "temperature/Drude", "temperature/ETM/diffusion", "solver/euler", "solver/heun",
     "solver/rk12", "solver/am12", "solver/bdf-euler", "solver/rk4", "solver/rk45", "micromag/energy",
@@ -197,7 +199,9 @@ class Engine:
                  thermal="temperature/brown" in mods, seed=int(g("Therm_seed", 0)), cutoff_dt=g("cutoff_dt"),
                  ttm="temperature/ETM" in mods, solver=solver, dt=g("dt", 1e-15), rtol=g("m_maxrelerror", 1e-5),
                  mindt=g("mindt", 1e-22), maxdt=g("maxdt", 1e-12), maxerr=maxerr, maxrelerr=maxrelerr,
-                 max_iter=max_iter)
+                 max_iter=max_iter,
+                 mu_par=g("μ∥", (0.0, 0.0, 0.0)) if "llbar/damping/nonconservative/02/local" in mods else (0, 0, 0),
+                 mu_perp=g("μ⊥", (0.0, 0.0, 0.0)) if "llbar/damping/conservative/02/local" in mods else (0, 0, 0))
         if d["ttm"]:
             d.update(gamma_e=g("γ") * g("n") / 6.02214129272727272e23 if "temperature/Drude" in mods else 0.0,
                      c_l=g("Cp"), g_ep=g("Ge-p"), k_e=g("Ke") if "temperature/ETM/diffusion" in mods else 0.0)

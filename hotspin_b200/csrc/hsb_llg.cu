@@ -185,6 +185,7 @@ __device__ __forceinline__ void rhs_cell(const HsbPhys& P, const float* __restri
         k[0] = g * (-H[1] * y[2] + H[2] * y[1]) + r * g * P.lam[0] * H[0];
         k[1] = g * (-H[2] * y[0] + H[0] * y[2]) + r * g * P.lam[1] * H[1];
         k[2] = g * (-H[0] * y[1] + H[1] * y[0]) + r * g * P.lam[2] * H[2];
+        if (P.llbar02 && !torque_only) hsb_llbar02(y, H, g, P.mu_par, P.mu_perp, k);
     }
     // ---- two-temperature model
     if (CH >= 5) {
@@ -1211,15 +1212,16 @@ static void launch_vec(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, c
 // True when stage launches of this simulation run the load-first kernel, which is the one
 // that can keep the step's thermal field (StageArgs.hth_mode).
 bool hsb_stage_keeps_thermal(const HsbPhys& P, int variant) {
-    return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask && stage_variant(variant) != 0;
+    return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask && !P.llbar02 && stage_variant(variant) != 0;
 }
 
-// True when the stage launches of this geometry can take a variant (no masks, a2 % 4 == 0).
-bool hsb_stage_tunable(const HsbPhys& P) { return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask; }
+// True when the stage launches of this geometry can take a variant (no masks, no second-order
+// relaxation terms, a2 % 4 == 0); otherwise every stage runs the generic per-cell kernel.
+bool hsb_stage_tunable(const HsbPhys& P) { return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask && !P.llbar02; }
 
 int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st, int variant) {
     const int threads = 256;
-    if (P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask) {
+    if (hsb_stage_tunable(P)) {
         BatchArgs nb = {0, nullptr, 1};
         if (P.nch == 5) launch_vec<5, false>(P, A, sd, nb, 1, st, variant);
         else launch_vec<3, false>(P, A, sd, nb, 1, st, variant);
@@ -1258,7 +1260,7 @@ int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st) {
 // P carries the class-wide geometry (size, channels; masks are not supported in batches).
 int hsb_launch_stage_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
                              cudaStream_t st, int variant) {
-    if (P.N2 % 4 != 0 || P.msat_mask || P.lex_mask) return HSB_ERR_UNSUPPORTED;
+    if (P.N2 % 4 != 0 || P.msat_mask || P.lex_mask || P.llbar02) return HSB_ERR_UNSUPPORTED;
     if (P.nch == 5) launch_vec<5, true>(P, A, sd, Bt, Bt.nslot, st, variant);
     else launch_vec<3, true>(P, A, sd, Bt, Bt.nslot, st, variant);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;

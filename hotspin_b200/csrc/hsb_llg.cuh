@@ -49,6 +49,10 @@ struct HsbPhys {
     float cs1, cs2;
     int normalize;       // renormalise m at stage formation (LLG mode); used by batched launches
     float ms0;           // Ms0 (A/m), the demag scale of this simulation
+    // second-order local relaxation terms of the LLBar equation (0 = not loaded):
+    // llbar/damping/nonconservative/02/local (mu_par) and conservative/02/local (mu_perp)
+    int llbar02;
+    float mu_par[3], mu_perp[3];
     // division of a cell index (< 2^31) by N2 and by N1 as a multiply-high and shift
     // (round-up reciprocal, Granlund & Montgomery 1994): q = umulhi(x, mul) >> shr
     unsigned div2_mul, div2_shr, div1_mul, div1_shr;
@@ -586,5 +590,23 @@ __host__ __device__ inline void hsb_imp_rule(HsbSolverDev& sd, const ImpLimits& 
             break;
         default: break;
     }
+}
+
+// The LLBar equation's second-order local relaxation terms at one cell, added to k (the
+// torque and zero-order relaxation already in it), for m and the cell's effective field H:
+//   llbar-local02nc.cu:11-73:  gamma diag(mu_par) (m . H) m
+//   llbar-local02c.cu:11-69:   gamma cross(diag(mu_perp) cross(m, H), m) with the reference's
+//                              cross(a, b) = b x a (common_func.h:52-55): gamma m x (mu_perp (H x m))
+// Host and device share this code.
+__host__ __device__ inline void hsb_llbar02(const float* m, const float* H, float g, const float* mu_par,
+                                            const float* mu_perp, float* k) {
+    const float mH = m[0] * H[0] + m[1] * H[1] + m[2] * H[2];
+    // a = mu_perp (H x m)
+    const float a0 = mu_perp[0] * (H[1] * m[2] - H[2] * m[1]);
+    const float a1 = mu_perp[1] * (H[2] * m[0] - H[0] * m[2]);
+    const float a2 = mu_perp[2] * (H[0] * m[1] - H[1] * m[0]);
+    k[0] += g * (mu_par[0] * mH * m[0] + (m[1] * a2 - m[2] * a1));
+    k[1] += g * (mu_par[1] * mH * m[1] + (m[2] * a0 - m[0] * a2));
+    k[2] += g * (mu_par[2] * mH * m[2] + (m[0] * a1 - m[1] * a0));
 }
 

@@ -65,7 +65,15 @@ struct hsb_sim_desc {
     double maxrelerr[3];         // am12: maxRelError (m, Te, Tl)
     int32_t max_iter;            // bdf-euler: sweeps per equation
     int32_t demag_tensor;        // 0 Kernel_Arne, 1 Newell
+    double mu_par[3];            // llbar/damping/nonconservative/02/local (0: not loaded)
+    double mu_perp[3];           // llbar/damping/conservative/02/local (0: not loaded)
 };
+
+static bool has_llbar02(const hsb_sim_desc& d) {
+    for (int a = 0; a < 3; a++)
+        if (d.mu_par[a] != 0.0 || d.mu_perp[a] != 0.0) return true;
+    return false;
+}
 
 enum { SOLVER_EULER = 0, SOLVER_HEUN = 1, SOLVER_RK4 = 2, SOLVER_DP45 = 3, SOLVER_RK12 = 4, SOLVER_AM12 = 5,
        SOLVER_BDF_EULER = 6 };
@@ -997,6 +1005,11 @@ static void phys_from_desc(const hsb_sim_desc& d, int nch, long ncell, HsbPhys& 
     P.cs2 = (float)d.cellsize[2];
     P.normalize = d.normalize;
     P.ms0 = (float)d.msat0T0;
+    P.llbar02 = has_llbar02(d) ? 1 : 0;
+    for (int a = 0; a < 3; a++) {
+        P.mu_par[a] = (float)d.mu_par[a];
+        P.mu_perp[a] = (float)d.mu_perp[a];
+    }
     hsb_fastdiv_init((unsigned)P.N2, &P.div2_mul, &P.div2_shr);
     hsb_fastdiv_init((unsigned)P.N1, &P.div1_mul, &P.div1_shr);
 }
@@ -1820,6 +1833,10 @@ static int batch_check_class(const hsb_sim_desc& d, int32_t nslot, const char* w
                       d.size[2]);
         return HSB_ERR_UNSUPPORTED;
     }
+    if (has_llbar02(d)) {
+        hsb_set_error("%s: the second-order relaxation terms run on the single-simulation handle only", who);
+        return HSB_ERR_UNSUPPORTED;
+    }
     for (int a = 0; a < 3; a++) {
         const int n = d.size[a];
         if (d.demag && (n & (n - 1)) != 0) {
@@ -1973,6 +1990,10 @@ HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* d
             hsb_set_error("hsb_batch_admit: grid size / boundaries differ from the class");
             return HSB_ERR_INVALID;
         }
+    }
+    if (has_llbar02(d)) {
+        hsb_set_error("hsb_batch_admit: the second-order relaxation terms run on the single-simulation handle only");
+        return HSB_ERR_UNSUPPORTED;
     }
     if (d.solver != c.solver || d.ttm != c.ttm || d.demag != c.demag || (d.thermal && !c.thermal) ||
         d.demag_tensor != c.demag_tensor ||

@@ -120,6 +120,14 @@ typedef struct hsb_sim_desc {
     double maxrelerr[3];
     int32_t max_iter;
     int32_t demag_tensor;   /* HSB_DEMAG_ARNE (default, the reference's) or HSB_DEMAG_NEWELL */
+    /* Second-order local relaxation terms of the LLBar equation, diagonal tensors in program
+     * components (0 = module not loaded): mu_par = mu_par of
+     * llbar/damping/nonconservative/02/local, gamma diag(mu_par) (m . H) m
+     * (llbar-local02nc.cu:11-73); mu_perp = mu_perp of llbar/damping/conservative/02/local,
+     * gamma m x (diag(mu_perp) (H x m)) (llbar-local02c.cu:11-69).  Uniform values only; the
+     * single-simulation handle runs them (batches refuse them). */
+    double mu_par[3];
+    double mu_perp[3];
 } hsb_sim_desc;
 
 typedef struct hsb_sim_s* hsb_sim;

@@ -64,6 +64,8 @@ class Spec:
     bext_table: object = None        # (t, Bx, By, Bz) rows (tesla): pointwise applied field instead of b_ext
     msat_mask: Optional[np.ndarray] = None
     lex_mask: Optional[np.ndarray] = None
+    mu_par: tuple = (0.0, 0.0, 0.0)  # llbar/damping/nonconservative/02/local (program components)
+    mu_perp: tuple = (0.0, 0.0, 0.0)  # llbar/damping/conservative/02/local
 
 
 def laser_profile(spec):
@@ -177,6 +179,10 @@ class Model:
         H = self.heff(yy, t)
         dm = F.llbar_torque(m, H, s.msat_mask, s.gamma_ll)
         dm = dm + F.llbar_local00nc(H, s.msat_mask, None, s.alpha, s.gamma_ll)
+        if any(v != 0.0 for v in s.mu_par):
+            dm = dm + F.llbar_local02nc(m, H, s.msat_mask, None, s.mu_par, s.gamma_ll)
+        if any(v != 0.0 for v in s.mu_perp):
+            dm = dm + F.llbar_local02c(m, H, s.msat_mask, None, s.mu_perp, s.gamma_ll)
         out = {"m": dm}
         if s.ttm:
             Te, Tl = y["Te"], y["Tl"]

@@ -151,3 +151,10 @@ extern "C" void arne_kernel_host(const int* L, const int* pbc, const double* cs,
         for (int d = s; d < 3; d++) Kc[(long)full[s][d] * ncell + c] = acc[d];
     }
 }
+
+// ---- the LLBar second-order local relaxation terms of one cell (hsb_llbar02 in hsb_llg.cuh)
+extern "C" void llbar02_host(const float* m, const float* H, float g, const float* mu_par, const float* mu_perp,
+                             float* k) {
+    k[0] = k[1] = k[2] = 0.f;
+    hsb_llbar02(m, H, g, mu_par, mu_perp, k);
+}

@@ -339,3 +339,25 @@ def test_bdf_euler_too_few_sweeps_stops_like_the_reference(rules):
         Integrator(model, y0, "bdf_euler", 5e-14, max_iter=1, max_iter_err=1e-12).step()
     _, status = emulate_bdf(rules, model, y0, 5e-14, 1, 1e-12, 1)
     assert status == 4
+
+
+def test_second_order_relaxation_terms_match_oracle(rules):
+    """hsb_llbar02 (the fused kernel's llbar/damping/{nonconservative,conservative}/02/local)
+    against the oracle's restatement of llbar-local02nc.cu and llbar-local02c.cu."""
+    from oracle import fields as F
+    f = rules.llbar02_host
+    P3 = ctypes.c_float * 3
+    f.argtypes = [ctypes.POINTER(ctypes.c_float)] * 2 + [ctypes.c_float] + [ctypes.POINTER(ctypes.c_float)] * 3
+    f.restype = None
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        m = rng.normal(size=3)
+        m /= np.linalg.norm(m)
+        H = rng.normal(size=3) * 1e5
+        mu_par, mu_perp = rng.uniform(0, 0.01, 3), rng.uniform(0, 0.01, 3)
+        g = 2.2e5
+        k = P3()
+        f(P3(*m), P3(*H), g, P3(*mu_par), P3(*mu_perp), k)
+        want = (F.llbar_local02nc(m[:, None], H[:, None], None, None, mu_par, g) +
+                F.llbar_local02c(m[:, None], H[:, None], None, None, mu_perp, g))[:, 0]
+        assert np.abs(np.array(list(k)) - want).max() <= 1e-5 * np.abs(want).max()

@@ -344,3 +344,22 @@ def test_pointwise_applied_field(cuda):
     assert np.abs(m - it.y["m"]).max() < 1e-5
     with pytest.raises(_lib.HsbError, match="batches"):
         Batch(2, **dict(desc, size=(2, 16, 32)), solver="dp45", dt=1e-15)
+
+
+@pytest.mark.parametrize("kw", [LLG, LLB], ids=["llg", "llb"])
+def test_second_order_relaxation_terms(cuda, kw):
+    """llbar/damping/nonconservative/02/local and conservative/02/local on the handle (the
+    generic stage kernel runs them): right-hand side and 20 RK4 steps against the oracle."""
+    kw = dict(kw, thermal=False, mu_par=(0.02, 0.015, 0.01), mu_perp=(0.005, 0.01, 0.02))
+    spec, desc = pair(**kw)
+    y = state(kw, seed=23)
+    want = Model(spec).rhs(0.0, y)
+    it = Integrator(Model(spec), y, "rk4", 1e-14)
+    it.run_steps(20)
+    with Simulation(**desc, solver="rk4", dt=1e-14) as sim:
+        sim.set("m", y["m"])
+        k = sim.get("k")
+        sim.step(20)
+        m = sim.get("m")
+    assert rel_err(k[:3], want["m"]) < 3e-5
+    assert np.abs(m - it.y["m"]).max() < 1e-5
