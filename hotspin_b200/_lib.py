@@ -40,7 +40,7 @@ class SimDesc(ctypes.Structure):
         ("mindt", c_dbl), ("maxdt", c_dbl), ("laser_table", ctypes.POINTER(c_dbl)), ("laser_npts", c_i32),
         ("bext_table", ctypes.POINTER(c_dbl)), ("bext_npts", c_i32), ("maxerr", c_dbl * 3),
         ("maxrelerr", c_dbl * 3), ("max_iter", c_i32), ("demag_tensor", c_i32),
-        ("mu_par", c_dbl * 3), ("mu_perp", c_dbl * 3),
+        ("mu_par", c_dbl * 3), ("mu_perp", c_dbl * 3), ("alpha_e", c_dbl * 3),
     ]
 
 

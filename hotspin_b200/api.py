@@ -11,7 +11,8 @@ everything is converted to program order (z, y, x) exactly as ``engine/api.go:41
 
 Supported modules: exchange6, demag, zeeman, anisotropy/uniaxial, llbar, llbar/torque,
 llbar/damping/nonconservative/00/local, llbar/damping/nonconservative/02/local (setv('μ∥',
-...)), llbar/damping/conservative/02/local (setv('μ⊥', ...)), normalizer, mfa/longfield, mfa/msat0,
+...)), llbar/damping/conservative/02/local (setv('μ⊥', ...)),
+llbar/damping/nonconservative/00/nonlocal (setv('αₑ', ...)), normalizer, mfa/longfield, mfa/msat0,
 temperature/brown, temperature/ETM, temperature/PTM, temperature/E-P, temperature/Drude,
 temperature/ETM/diffusion, solver/euler, solver/heun, solver/rk12 (errors per step set with
 setv('m_maxerror' / 'Te_maxerror' / 'Tp_maxerror', ...)), solver/am12 ('<q>_maxabserror',
@@ -30,7 +31,8 @@ MUB = 9.27400968202020202e-24
 SUPPORTED = {
     "exchange6", "demag", "zeeman", "anisotropy/uniaxial", "llbar", "llbar/torque",
     "llbar/damping/nonconservative/00/local", "llbar/damping/nonconservative/02/local",
-    "llbar/damping/conservative/02/local", "normalizer", "mfa/longfield", "mfa/msat0",
+    "llbar/damping/conservative/02/local", "llbar/damping/nonconservative/00/nonlocal", "normalizer",
+    "mfa/longfield", "mfa/msat0",
     "temperature/brown", "temperature/ETM", "temperature/PTM", "temperature/E-P",
     "temperature/Drude", "temperature/ETM/diffusion", "solver/euler", "solver/heun",
     "solver/rk12", "solver/am12", "solver/bdf-euler", "solver/rk4", "solver/rk45", "micromag/energy",
@@ -201,7 +203,8 @@ class Engine:
                  mindt=g("mindt", 1e-22), maxdt=g("maxdt", 1e-12), maxerr=maxerr, maxrelerr=maxrelerr,
                  max_iter=max_iter,
                  mu_par=g("μ∥", (0.0, 0.0, 0.0)) if "llbar/damping/nonconservative/02/local" in mods else (0, 0, 0),
-                 mu_perp=g("μ⊥", (0.0, 0.0, 0.0)) if "llbar/damping/conservative/02/local" in mods else (0, 0, 0))
+                 mu_perp=g("μ⊥", (0.0, 0.0, 0.0)) if "llbar/damping/conservative/02/local" in mods else (0, 0, 0),
+                 alpha_e=g("αₑ", (0.0, 0.0, 0.0)) if "llbar/damping/nonconservative/00/nonlocal" in mods else (0, 0, 0))
         if d["ttm"]:
             d.update(gamma_e=g("γ") * g("n") / 6.02214129272727272e23 if "temperature/Drude" in mods else 0.0,
                      c_l=g("Cp"), g_ep=g("Ge-p"), k_e=g("Ke") if "temperature/ETM/diffusion" in mods else 0.0)

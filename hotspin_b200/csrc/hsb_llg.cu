@@ -97,7 +97,8 @@ template <int CH>
 __device__ __forceinline__ void rhs_cell(const HsbPhys& P, const float* __restrict__ ys,
                                          const float* __restrict__ hd, const float* __restrict__ yth,
                                          double t, double dt, long long step, int a0, int a1, int a2,
-                                         long i, float* y, float* k, bool torque_only = false) {
+                                         long i, float* y, float* k, bool torque_only = false,
+                                         float* hout = nullptr) {
     const long n = P.ncell;
     const long s1 = P.N2, s0 = (long)P.N1 * P.N2;
     load_ch<CH>(ys, n, i, y);
@@ -176,6 +177,11 @@ __device__ __forceinline__ void rhs_cell(const HsbPhys& P, const float* __restri
             for (int c = 0; c < 3; c++) H[c] += amp * sqrtf(P.lam[c]) * g[c];
         }
     }
+    if (hout) {       // first pass of the non-local relaxation: the effective field only
+#pragma unroll
+        for (int c = 0; c < 3; c++) hout[c * n + i] = H[c];
+        return;
+    }
     // ---- LLBar torque cross(H, m) = m x H + zero-order local relaxation (zero in vacuum)
     if (ms == 0.f) {
         k[0] = k[1] = k[2] = 0.f;
@@ -186,6 +192,26 @@ __device__ __forceinline__ void rhs_cell(const HsbPhys& P, const float* __restri
         k[1] = g * (-H[2] * y[0] + H[0] * y[2]) + r * g * P.lam[1] * H[1];
         k[2] = g * (-H[0] * y[1] + H[1] * y[0]) + r * g * P.lam[2] * H[2];
         if (P.llbar02 && !torque_only) hsb_llbar02(y, H, g, P.mu_par, P.mu_perp, k);
+        // zero-order non-local relaxation -gamma alpha_e lap(H) with the stored fields of the
+        // neighbours (llbar-nonlocal00nc.cu:11-205 with a uniform alpha_e: the harmonic means of
+        // the cell's and each neighbour's alpha_e are alpha_e itself; clamp / wrap boundaries)
+        if (P.nonlocal && !torque_only) {
+            const int lo[3] = {nb_lo(a0, P.N0, P.pbc0), nb_lo(a1, P.N1, P.pbc1), nb_lo(a2, P.N2, P.pbc2)};
+            const int hi[3] = {nb_hi(a0, P.N0, P.pbc0), nb_hi(a1, P.N1, P.pbc1), nb_hi(a2, P.N2, P.pbc2)};
+            const int me[3] = {a0, a1, a2};
+            const long st[3] = {s0, s1, 1};
+            float lap[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const long im = i + (long)(lo[d] - me[d]) * st[d];
+                const long ip = i + (long)(hi[d] - me[d]) * st[d];
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    lap[c] += P.inv_cs2[d] * ((P.hbuf[c * n + im] + P.hbuf[c * n + ip]) - (H[c] + H[c]));
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) k[c] -= g * P.lam_e[c] * lap[c];
+        }
     }
     // ---- two-temperature model
     if (CH >= 5) {
@@ -277,7 +303,8 @@ __global__ void __launch_bounds__(256) k_stage(const HsbPhys P, const StageArgs 
         const int a1 = (int)(r % P.N1);
         const int a0 = (int)(r / P.N1);
         float y[CH], k[CH];
-        rhs_cell<CH>(P, ys, hd, yth, ts, dt, step, a0, a1, a2, i, y, k, A.torque_only != 0);
+        rhs_cell<CH>(P, ys, hd, yth, ts, dt, step, a0, a1, a2, i, y, k, A.torque_only != 0, A.heff_out);
+        if (A.heff_out) continue;
         if (kout) {
 #pragma unroll
             for (int c = 0; c < CH; c++) {
@@ -1209,34 +1236,45 @@ static void launch_vec(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, c
     }
 }
 
+bool hsb_stage_tunable(const HsbPhys& P);
+
 // True when stage launches of this simulation run the load-first kernel, which is the one
 // that can keep the step's thermal field (StageArgs.hth_mode).
 bool hsb_stage_keeps_thermal(const HsbPhys& P, int variant) {
-    return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask && !P.llbar02 && stage_variant(variant) != 0;
+    return hsb_stage_tunable(P) && stage_variant(variant) != 0;
 }
 
 // True when the stage launches of this geometry can take a variant (no masks, no second-order
 // relaxation terms, a2 % 4 == 0); otherwise every stage runs the generic per-cell kernel.
-bool hsb_stage_tunable(const HsbPhys& P) { return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask && !P.llbar02; }
+bool hsb_stage_tunable(const HsbPhys& P) {
+    return P.N2 % 4 == 0 && !P.msat_mask && !P.lex_mask && !P.llbar02 && !P.nonlocal;
+}
+
+int hsb_launch_stage_generic(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st);
 
 int hsb_launch_stage(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st, int variant) {
-    const int threads = 256;
     if (hsb_stage_tunable(P)) {
         BatchArgs nb = {0, nullptr, 1};
         if (P.nch == 5) launch_vec<5, false>(P, A, sd, nb, 1, st, variant);
         else launch_vec<3, false>(P, A, sd, nb, 1, st, variant);
         return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
     }
-    const int grid = hsb_grid_1d(P.ncell, threads, 8);
-    if (P.nch == 5) k_stage<5><<<grid, threads, 0, st>>>(P, A, sd);
-    else k_stage<3><<<grid, threads, 0, st>>>(P, A, sd);
-    return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
+    return hsb_launch_stage_generic(P, A, sd, st);
 }
 
-// The generic per-cell kernel whatever the geometry (state queries such as the torque).
+// The generic per-cell kernel whatever the geometry (state queries such as the torque).  With
+// the non-local relaxation term a first launch of the same kernel stores every cell's effective
+// field, which the second reads at the neighbours.
 int hsb_launch_stage_generic(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, cudaStream_t st) {
     const int threads = 256;
     const int grid = hsb_grid_1d(P.ncell, threads, 8);
+    if (P.nonlocal && !A.torque_only) {
+        if (!P.hbuf) return HSB_ERR_INVALID;
+        StageArgs Hp = A;
+        Hp.heff_out = P.hbuf;
+        if (P.nch == 5) k_stage<5><<<grid, threads, 0, st>>>(P, Hp, sd);
+        else k_stage<3><<<grid, threads, 0, st>>>(P, Hp, sd);
+    }
     if (P.nch == 5) k_stage<5><<<grid, threads, 0, st>>>(P, A, sd);
     else k_stage<3><<<grid, threads, 0, st>>>(P, A, sd);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;
@@ -1260,7 +1298,7 @@ int hsb_launch_dp45_control(HsbSolverDev* sd, cudaStream_t st) {
 // P carries the class-wide geometry (size, channels; masks are not supported in batches).
 int hsb_launch_stage_batched(const HsbPhys& P, const StageArgs& A, HsbSolverDev* sd, const BatchArgs& Bt,
                              cudaStream_t st, int variant) {
-    if (P.N2 % 4 != 0 || P.msat_mask || P.lex_mask || P.llbar02) return HSB_ERR_UNSUPPORTED;
+    if (P.N2 % 4 != 0 || P.msat_mask || P.lex_mask || P.llbar02 || P.nonlocal) return HSB_ERR_UNSUPPORTED;
     if (P.nch == 5) launch_vec<5, true>(P, A, sd, Bt, Bt.nslot, st, variant);
     else launch_vec<3, true>(P, A, sd, Bt, Bt.nslot, st, variant);
     return cudaGetLastError() == cudaSuccess ? HSB_OK : HSB_ERR_CUDA;

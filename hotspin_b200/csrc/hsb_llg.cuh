@@ -53,6 +53,13 @@ struct HsbPhys {
     // llbar/damping/nonconservative/02/local (mu_par) and conservative/02/local (mu_perp)
     int llbar02;
     float mu_par[3], mu_perp[3];
+    // zero-order non-local relaxation (llbar/damping/nonconservative/00/nonlocal, alpha_e):
+    // -gamma diag(alpha_e) lap(H_eff); the effective field of every cell is stored in hbuf by
+    // a first pass of the generic stage kernel so the second can take the neighbours' values
+    int nonlocal;
+    float lam_e[3];
+    float inv_cs2[3];    // 1 / cs_d^2 (1/m^2)
+    float* hbuf;         // [3][ncell]
     // division of a cell index (< 2^31) by N2 and by N1 as a multiply-high and shift
     // (round-up reciprocal, Granlund & Montgomery 1994): q = umulhi(x, mul) >> shr
     unsigned div2_mul, div2_shr, div1_mul, div1_shr;
@@ -286,6 +293,7 @@ struct StageArgs {
     int hth_mode;
     PtrSel hth;              // [3][ncell]
     int torque_only;         // generic kernel only: k = gamma (m x H), without the relaxation term
+    float* heff_out;         // generic kernel only: store H_eff of ys here and compute nothing else
     // error mode: 0 = the DP45 norm (m: |e| / rtol, T: |e| / (rtol max(|T0|, |T|)), one
     // maximum); 1 = per-equation absolute errors dt |e| into HsbSolverDev.err_eq (rk12)
     int err_abs;

@@ -67,12 +67,16 @@ struct hsb_sim_desc {
     int32_t demag_tensor;        // 0 Kernel_Arne, 1 Newell
     double mu_par[3];            // llbar/damping/nonconservative/02/local (0: not loaded)
     double mu_perp[3];           // llbar/damping/conservative/02/local (0: not loaded)
+    double alpha_e[3];           // llbar/damping/nonconservative/00/nonlocal (0: not loaded)
 };
 
 static bool has_llbar02(const hsb_sim_desc& d) {
     for (int a = 0; a < 3; a++)
         if (d.mu_par[a] != 0.0 || d.mu_perp[a] != 0.0) return true;
     return false;
+}
+static bool has_nonlocal(const hsb_sim_desc& d) {
+    return d.alpha_e[0] != 0.0 || d.alpha_e[1] != 0.0 || d.alpha_e[2] != 0.0;
 }
 
 enum { SOLVER_EULER = 0, SOLVER_HEUN = 1, SOLVER_RK4 = 2, SOLVER_DP45 = 3, SOLVER_RK12 = 4, SOLVER_AM12 = 5,
@@ -158,6 +162,7 @@ struct hsb_sim_s {
     long long launch_total;       // kernels enqueued for stepping since creation
     double rk12_maxerr[3];        // rk12: per-step error limits (m, Te, Tl; +inf = uncontrolled)
     ImpLimits imp;                // am12 / bdf-euler limits
+    float* hbuf;                  // non-local relaxation: effective field of every cell [3][n]
     float* ckpt;                  // checkpoint: the state channels [nch][n] (device)
     HsbSolverDev* ckpt_sd;        // checkpoint: the solver word (device)
 };
@@ -1006,9 +1011,12 @@ static void phys_from_desc(const hsb_sim_desc& d, int nch, long ncell, HsbPhys& 
     P.normalize = d.normalize;
     P.ms0 = (float)d.msat0T0;
     P.llbar02 = has_llbar02(d) ? 1 : 0;
+    P.nonlocal = has_nonlocal(d) ? 1 : 0;
     for (int a = 0; a < 3; a++) {
         P.mu_par[a] = (float)d.mu_par[a];
         P.mu_perp[a] = (float)d.mu_perp[a];
+        P.lam_e[a] = (float)d.alpha_e[a];
+        P.inv_cs2[a] = (float)(1.0 / (d.cellsize[a] * d.cellsize[a]));
     }
     hsb_fastdiv_init((unsigned)P.N2, &P.div2_mul, &P.div2_shr);
     hsb_fastdiv_init((unsigned)P.N1, &P.div1_mul, &P.div1_shr);
@@ -1022,6 +1030,7 @@ static void fill_phys(hsb_sim_s* S) {
     S->P.bext_npts = S->bext_tab ? S->d.bext_npts : 0;
     S->P.msat_mask = S->msat_mask;
     S->P.lex_mask = S->lex_mask;
+    S->P.hbuf = S->hbuf;
 }
 
 // Offsets (floats) of one slot's buffers in its arena.
@@ -1096,6 +1105,7 @@ static void free_sim(hsb_sim_s* S) {
     cudaFree(S->stage_d);
     cudaFree(S->ckpt);
     cudaFree(S->ckpt_sd);
+    cudaFree(S->hbuf);
     if (S->sd_host) cudaFreeHost(S->sd_host);
     if (S->stage_pin) cudaFreeHost(S->stage_pin);
     if (S->red_host) cudaFreeHost(S->red_host);
@@ -1324,6 +1334,7 @@ HSB_EXPORT int hsb_sim_create(const hsb_sim_desc* desc, hsb_sim_s** out) {
     }
     const SlotLayout L = slot_layout(d, n);
     STRY(cudaMalloc(&S->arena, sizeof(float) * L.total));
+    if (has_nonlocal(d)) STRY(cudaMalloc(&S->hbuf, sizeof(float) * 3 * n));
     STRY(cudaMemsetAsync(S->arena, 0, sizeof(float) * L.total, S->st));
     point_slot0(S, L);
     STRY(cudaMalloc(&S->sd, sizeof(HsbSolverDev)));
@@ -1833,8 +1844,9 @@ static int batch_check_class(const hsb_sim_desc& d, int32_t nslot, const char* w
                       d.size[2]);
         return HSB_ERR_UNSUPPORTED;
     }
-    if (has_llbar02(d)) {
-        hsb_set_error("%s: the second-order relaxation terms run on the single-simulation handle only", who);
+    if (has_llbar02(d) || has_nonlocal(d)) {
+        hsb_set_error("%s: the second-order and non-local relaxation terms run on the single-simulation handle only",
+                      who);
         return HSB_ERR_UNSUPPORTED;
     }
     for (int a = 0; a < 3; a++) {
@@ -1991,8 +2003,9 @@ HSB_EXPORT int hsb_batch_admit(hsb_sim_s* B, int32_t slot, const hsb_sim_desc* d
             return HSB_ERR_INVALID;
         }
     }
-    if (has_llbar02(d)) {
-        hsb_set_error("hsb_batch_admit: the second-order relaxation terms run on the single-simulation handle only");
+    if (has_llbar02(d) || has_nonlocal(d)) {
+        hsb_set_error("hsb_batch_admit: the second-order and non-local relaxation terms run on the single-simulation "
+                      "handle only");
         return HSB_ERR_UNSUPPORTED;
     }
     if (d.solver != c.solver || d.ttm != c.ttm || d.demag != c.demag || (d.thermal && !c.thermal) ||

@@ -128,6 +128,10 @@ typedef struct hsb_sim_desc {
      * single-simulation handle runs them (batches refuse them). */
     double mu_par[3];
     double mu_perp[3];
+    /* alpha_e of llbar/damping/nonconservative/00/nonlocal (llbar-nonlocal00nc.cu:11-205):
+     * -gamma diag(alpha_e) lap(H_eff), uniform, program components (0 = not loaded); the
+     * single-simulation handle runs it with one extra pass per right-hand side. */
+    double alpha_e[3];
 } hsb_sim_desc;
 
 typedef struct hsb_sim_s* hsb_sim;

@@ -66,6 +66,7 @@ class Spec:
     lex_mask: Optional[np.ndarray] = None
     mu_par: tuple = (0.0, 0.0, 0.0)  # llbar/damping/nonconservative/02/local (program components)
     mu_perp: tuple = (0.0, 0.0, 0.0)  # llbar/damping/conservative/02/local
+    alpha_e: tuple = (0.0, 0.0, 0.0)  # llbar/damping/nonconservative/00/nonlocal
 
 
 def laser_profile(spec):
@@ -183,6 +184,8 @@ class Model:
             dm = dm + F.llbar_local02nc(m, H, s.msat_mask, None, s.mu_par, s.gamma_ll)
         if any(v != 0.0 for v in s.mu_perp):
             dm = dm + F.llbar_local02c(m, H, s.msat_mask, None, s.mu_perp, s.gamma_ll)
+        if any(v != 0.0 for v in s.alpha_e):
+            dm = dm + s.gamma_ll * F.llbar_nonlocal00nc(H, s.msat_mask, None, s.alpha_e, s.cellsize, s.pbc)
         out = {"m": dm}
         if s.ttm:
             Te, Tl = y["Te"], y["Tl"]

@@ -363,3 +363,23 @@ def test_second_order_relaxation_terms(cuda, kw):
         m = sim.get("m")
     assert rel_err(k[:3], want["m"]) < 3e-5
     assert np.abs(m - it.y["m"]).max() < 1e-5
+
+
+@pytest.mark.parametrize("pbc", [(0, 0, 0), (0, 2, 3)])
+def test_nonlocal_relaxation_term(cuda, pbc):
+    """llbar/damping/nonconservative/00/nonlocal on the handle (two passes of the generic stage
+    kernel: effective fields stored, then their Laplacian): right-hand side and 20 RK4 steps
+    against the oracle's restatement of llbar-nonlocal00nc.cu."""
+    kw = dict(LLG, pbc=pbc, thermal=False, alpha_e=(2e-19, 3e-19, 1e-19))
+    spec, desc = pair(**kw)
+    y = state(kw, seed=29)
+    want = Model(spec).rhs(0.0, y)
+    it = Integrator(Model(spec), y, "rk4", 1e-14)
+    it.run_steps(20)
+    with Simulation(**desc, solver="rk4", dt=1e-14) as sim:
+        sim.set("m", y["m"])
+        k = sim.get("k")
+        sim.step(20)
+        m = sim.get("m")
+    assert rel_err(k[:3], want["m"]) < 3e-5
+    assert np.abs(m - it.y["m"]).max() < 1e-5
