@@ -61,6 +61,7 @@ _SIGS = {
     "partialMaxAbsAsync": [P, P, I, I, I, P],
     "partialMaxDiffAsync": [P, P, P, I, I, I, P],
     "madd2Async": [P, P, D, P, D, P, I],
+    "addMaddAsync": [P, P, P, P, D, P, I],
     "normalizeAsync": [P, P, P, P, I],
 }
 
@@ -378,6 +379,115 @@ class RefSim:
             self.rejects += 1
             tr += 1
         self._normalize(self.y)          # the next update of m renormalises it
+        self.t = t0 + dt
+        self.steps += 1
+
+    def _am_norm(self, a, b, scale, abs_err, rel_err):
+        """solve_am01.go's error of one equation on the reference's reductions: per component,
+        MaxDiff(a_p, b_p) / (maxAbsError + MaxAbs(scale_p) maxRelError), root mean square."""
+        t = 0.0
+        for p_ in range(a.shape[0]):
+            d = self._maxdiff(a[p_], b[p_])
+            mx = self._maxabs(scale[p_])
+            v = d / (abs_err + mx * rel_err) if (abs_err + mx * rel_err) != 0 else math.inf
+            t += v * v
+        return math.sqrt(t) / math.sqrt(a.shape[0])
+
+    def step_am12(self, abs_err, rel_err):
+        """One step of hotspin's adaptive Adams-Moulton 1-2 solver (solve_am01.go:45-318) on the
+        reference kernels: inputs updated (m renormalised), y0 and dy0 kept; per try the
+        explicit Euler start (Madd), the implicit Euler predictor and the trapezoidal corrector
+        solved by fixed-point sweeps (Madd / AddMadd, MaxDiff / MaxAbs per component), the
+        step error of corrector against predictor and the new dt.  The decisions follow the Go
+        code as the oracle restates them (oracle.solvers.am_iter_rule); abs_err / rel_err:
+        {"m": .., "Te": .., "Tl": ..}.  Without a thermal field."""
+        from .solvers import am_iter_rule
+        L, p, s = self.lib, self.p, self.sh
+        assert not self.kw.get("thermal")
+        nn = self.nch * self.n
+        torch = self.torch
+        keys = [("m", slice(0, 3))] + ([("Te", slice(3, 4)), ("Tl", slice(4, 5))] if self.ttm else [])
+        ab = [abs_err[k] for k, _ in keys]
+        rl = [rel_err[k] for k, _ in keys]
+        if not hasattr(self, "y0b"):
+            self.y0b = torch.zeros_like(self.y)
+            self.y1b = torch.zeros_like(self.y)
+        t0 = self.t
+        self._normalize(self.y)
+        dy0, dybuf, dy = self.k[0], self.k[1], self.k[2]
+        self.rhs(t0, self.y, dy0)
+        self.y0b.copy_(self.y)
+        self.sync()
+        tries, restrict, s_alpha = 0, False, [0.0] * len(keys)
+        while True:
+            dt = self.dt
+            L.maddAsync(p(self.y), p(self.y0b), p(dy0), D(dt), s, I(nn))
+            self.sync()
+            self._normalize(self.y)
+            self.rhs(t0 + dt, self.y, dy)
+            dybuf.copy_(dy)
+            self.sync()
+            failed = False
+            for phase in (0, 1):
+                er = [0.1] * len(keys)
+                it = 0
+                while True:
+                    terrs = []
+                    for (k, sl) in keys:
+                        if phase == 0:
+                            L.maddAsync(p(self.ys[sl]), p(self.y0b[sl]), p(dy[sl]), D(dt), s,
+                                        I(self.n * (sl.stop - sl.start)))
+                        else:
+                            L.addMaddAsync(p(self.ys[sl]), p(self.y0b[sl]), p(dy[sl]), p(dy0[sl]), D(0.5 * dt), s,
+                                           I(self.n * (sl.stop - sl.start)))
+                        self.sync()
+                        i = [kk for kk, _ in keys].index(k)
+                        terrs.append(self._am_norm(self.y[sl], self.ys[sl], self.ys[sl], ab[i], rl[i]))
+                        self.y[sl].copy_(self.ys[sl])
+                    er, alp, err, alpha = am_iter_rule(er, terrs)
+                    if phase == 0:
+                        s_alpha = alp
+                    it += 1
+                    if err <= 0.1:
+                        break
+                    if alpha >= 1.0 or it > 5:
+                        failed = True
+                        break
+                    self._normalize(self.y)
+                    self.rhs(t0 + dt, self.y, dy)
+                if failed:
+                    if tries == 9:
+                        raise RuntimeError("The BDF iterator cannot converge")
+                    self.dt = dt * math.sqrt(0.6 / alpha) if alpha > 0.6 else 0.5 * dt
+                    restrict = restrict or phase == 0
+                    self.attempts += 1
+                    break
+                if phase == 0:
+                    self.y1b.copy_(self.y)
+                    dy.copy_(dybuf)
+                    self.sync()
+            if failed:
+                continue
+            bad = False
+            ndts = []
+            for i, (k, sl) in enumerate(keys):
+                terr = self._am_norm(self.y[sl], self.y1b[sl], self.y1b[sl], ab[i], rl[i])
+                bad = bad or terr > 1.0
+                hr = dt * math.sqrt(0.8 / terr) if terr > 0 else math.inf
+                nd = hr
+                if restrict:
+                    nd = min(hr, dt * math.sqrt(0.6 / s_alpha[i]) if s_alpha[i] > 0 else math.inf)
+                    restrict = False
+                ndts.append(min(max(nd, self.mindt), self.maxdt))
+            self.attempts += 1
+            self.dt = min(ndts)
+            if not bad or self.dt == self.mindt:
+                break
+            if tries > 10:
+                raise RuntimeError("The solver cannot converge after 10 badsteps")
+            self.rejects += 1
+            tries += 1
+        self._normalize(self.y)
         self.t = t0 + dt
         self.steps += 1
 

@@ -119,3 +119,25 @@ def test_am12_batch_slot_matches_plain_handle(cuda):
         m, st = sim.get("m"), sim.status()
     assert sb["steps"] == st["steps"]
     assert float(np.abs(mb - m).max()) <= 1e-6
+
+
+def test_am12_matches_reference_kernels(cuda):
+    """The reference's own kernels (oracle/_ref) stepped by the replay of solve_am01.go."""
+    from oracle import replay
+    if not replay.available():
+        pytest.skip("oracle/_ref/libhotspin.so not built (needs the reference sources)")
+    kw = dict(LLG, size=(1, 16, 32))
+    y0 = _start(kw)
+    ref = replay.RefSim(kw, dt=1e-17, mindt=1e-22, maxdt=1e-12)
+    ref.set("m", y0["m"])
+    for _ in range(30):
+        ref.step_am12({"m": 1e-5}, {"m": 1e-5})
+    with Simulation(**kw, solver="am12", dt=1e-17, mindt=1e-22, maxdt=1e-12, maxerr=(1e-5, 0.0, 0.0),
+                    maxrelerr=(1e-5, 0.0, 0.0)) as sim:
+        sim.set("m", y0["m"])
+        sim.step(30)
+        st = sim.status()
+        m = sim.get("m")
+    assert st["t"] == pytest.approx(ref.t, rel=1e-6)
+    assert st["rejects"] == ref.rejects
+    assert float(np.abs(m - ref.get("m")).max()) < 1e-5
