@@ -64,53 +64,10 @@ __global__ void __launch_bounds__(256) k_imp_sweep(const __grid_constant__ HsbPh
 #pragma unroll
     for (int c = 0; c < CH; c++) dmax[c] = smax[c] = 0.f;
     bool bad = false;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        if (mode == IMP_AM_ERR) {
-#pragma unroll
-            for (int c = 0; c < CH; c++) {
-                const float a = uc[c * n + i], b = up[c * n + i];
-                dmax[c] = fmaxf(dmax[c], fabsf(a - b));
-                smax[c] = fmaxf(smax[c], fabsf(b));
-                bad |= !isfinite(a - b);
-            }
-            continue;
-        }
-        float nv[CH];
-#pragma unroll
-        for (int c = 0; c < CH; c++) {
-            if (c < c0 || c >= c1) continue;
-            const float b = __ldg(y0 + c * n + i);
-            if (mode == IMP_AM_CORR) nv[c] = b + (0.5f * fdt) * (dy[c * n + i] + k0[c * n + i]);
-            else if (mode == IMP_AM_PRED) nv[c] = b + fdt * dy[c * n + i];
-            else nv[c] = b + fdt * k0[c * n + i];
-            bad |= !isfinite(nv[c]);
-        }
-        if (mode != IMP_BDF_EULER) {
-#pragma unroll
-            for (int c = 0; c < CH; c++) {
-                if (c < c0 || c >= c1) continue;
-                const float pv = prev_raw[c * n + i];
-                dmax[c] = fmaxf(dmax[c], fabsf(pv - nv[c]));
-                smax[c] = fmaxf(smax[c], mode == IMP_BDF_SWEEP ? fabsf(pv + nv[c]) : fabsf(nv[c]));
-            }
-        }
-        if (mode == IMP_AM_PRED || mode == IMP_AM_CORR) {
-            float* u = (mode == IMP_AM_PRED) ? up : uc;
-#pragma unroll
-            for (int c = 0; c < CH; c++) u[c * n + i] = nv[c];
-        }
-        // the reference renormalises m when it next updates it (before the next right-hand side)
-        if (normalize && c0 == 0) {
-            const float l2 = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
-            const float inv = (l2 == 0.f) ? 0.f : rsqrtf(l2);
-            nv[0] *= inv;
-            nv[1] *= inv;
-            nv[2] *= inv;
-        }
-#pragma unroll
-        for (int c = 0; c < CH; c++)
-            if (c >= c0 && c < c1) w[c * n + i] = nv[c];
-    }
+    float* u = (mode == IMP_AM_PRED) ? up : (mode == IMP_AM_CORR ? uc : nullptr);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        hsb_imp_sweep_cell<CH>(mode, i, n, fdt, c0, c1, normalize, y0, w, prev_raw, dy, k0, u, up, uc, dmax, smax,
+                               bad);
     if (mode != IMP_BDF_EULER) {
 #pragma unroll
         for (int c = 0; c < CH; c++) {

@@ -618,3 +618,56 @@ __host__ __device__ inline void hsb_llbar02(const float* m, const float* H, floa
     k[2] += g * (mu_par[2] * mH * m[2] + (m[0] * a1 - m[1] * a0));
 }
 
+// One cell of a fixed-point sweep (k_imp_sweep; host builds drive it cell by cell): forms the
+// new iterate of the channels [c0, c1) from y0 and the derivative, folds max|prev - new| and the
+// error scale (|new|, or |prev + new| for bdf-euler) into dmax / smax, writes the raw iterate to
+// u (am12 predictor / corrector) and the iterate, m renormalised when `normalize`, to w; the
+// am12 step-error mode compares uc with up (scale |up|) and writes nothing.
+template <int CH>
+__host__ __device__ inline void hsb_imp_sweep_cell(int mode, long i, long n, float fdt, int c0, int c1,
+                                                   int normalize, const float* y0, float* w, const float* prev,
+                                                   const float* dy, const float* k0, float* u, const float* up,
+                                                   const float* uc, float* dmax, float* smax, bool& bad) {
+    if (mode == IMP_AM_ERR) {
+        for (int c = 0; c < CH; c++) {
+            const float a = uc[c * n + i], b = up[c * n + i];
+            dmax[c] = fmaxf(dmax[c], fabsf(a - b));
+            smax[c] = fmaxf(smax[c], fabsf(b));
+            bad |= !isfinite(a - b);
+        }
+        return;
+    }
+    float nv[CH];
+    for (int c = 0; c < CH; c++) {
+        nv[c] = 0.f;
+        if (c < c0 || c >= c1) continue;
+        const float b = y0[c * n + i];
+        if (mode == IMP_AM_CORR) nv[c] = b + (0.5f * fdt) * (dy[c * n + i] + k0[c * n + i]);
+        else if (mode == IMP_AM_PRED) nv[c] = b + fdt * dy[c * n + i];
+        else nv[c] = b + fdt * k0[c * n + i];
+        bad |= !isfinite(nv[c]);
+    }
+    if (mode != IMP_BDF_EULER) {
+        for (int c = c0; c < c1; c++) {
+            const float pv = prev[c * n + i];
+            dmax[c] = fmaxf(dmax[c], fabsf(pv - nv[c]));
+            smax[c] = fmaxf(smax[c], mode == IMP_BDF_SWEEP ? fabsf(pv + nv[c]) : fabsf(nv[c]));
+        }
+    }
+    if (u)
+        for (int c = 0; c < CH; c++) u[c * n + i] = nv[c];
+    // the reference renormalises m when it next updates it (before the next right-hand side)
+    if (normalize && c0 == 0) {
+        const float l2 = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
+#ifdef __CUDA_ARCH__
+        const float inv = (l2 == 0.f) ? 0.f : rsqrtf(l2);
+#else
+        const float inv = (l2 == 0.f) ? 0.f : 1.0f / sqrtf(l2);
+#endif
+        nv[0] *= inv;
+        nv[1] *= inv;
+        nv[2] *= inv;
+    }
+    for (int c = c0; c < c1; c++) w[c * n + i] = nv[c];
+}
+
