@@ -24,6 +24,10 @@ __device__ __forceinline__ float* imp_resolve(const PtrSel& s, const HsbSolverDe
     return p ? p + off : nullptr;
 }
 
+__device__ __forceinline__ double* imp_slot64(double* p, long off) {
+    return p ? (double*)((float*)p + off) : nullptr;
+}
+
 __device__ __forceinline__ void imp_fold_max(float v, unsigned int* word) {
     v = warp_max_f(v);
     if ((threadIdx.x & 31) == 0 && v > 0.f) atomicMax(word, __float_as_uint(v));
@@ -38,22 +42,25 @@ __global__ void __launch_bounds__(256) k_imp_sweep(const __grid_constant__ HsbPh
     const int mode = A.mode;
     bool run;
     if (mode == IMP_AM_ERR) run = sd->active && !(sd->it_flags & 4);
-    else if (mode == IMP_BDF_EULER) run = sd->active != 0;
+    else if (mode == IMP_BDF_EULER || mode == IMP_AM_EULER) run = sd->active != 0;
     else run = sd->active && sd->it_active;
     if (!run) return;
     const HsbPhys& P = BATCH ? Bt.phys[slot] : P0;
     const long off = BATCH ? (long)slot * Bt.stride : 0;
     const int normalize = BATCH ? (A.normalize && P.normalize) : A.normalize;
     const long n = P.ncell;
-    const float fdt = (float)sd->dt;
+    const double dt = sd->dt;
     const float* y0 = imp_resolve(A.y0, sd, off);
     float* w = imp_resolve(A.w, sd, off);
-    float* up = A.up ? A.up + off : nullptr;
-    float* uc = A.uc ? A.uc + off : nullptr;
     const float* k0 = A.k0 ? A.k0 + off : nullptr;
     const float* dy = (sd->dysel ? A.k2 : A.k1);
     if (dy) dy += off;
-    const float* prev_raw = (mode == IMP_AM_CORR && sd->prevsel) ? up : w;
+    // the FP64 iterates lie in the slot's arena (the slot stride, in floats, keeps 256-byte alignment)
+    double* w64 = imp_slot64(A.w64, off);
+    double* up64 = imp_slot64(A.up64, off);
+    double* uc64 = imp_slot64(A.uc64, off);
+    const double* prev64 = (mode == IMP_AM_CORR && sd->prevsel) ? up64 : w64;
+    double* u64 = (mode == IMP_AM_PRED) ? up64 : (mode == IMP_AM_CORR ? uc64 : nullptr);
     // channels this launch touches
     int c0 = 0, c1 = CH;
     if (mode == IMP_BDF_EULER || mode == IMP_BDF_SWEEP) {
@@ -64,11 +71,10 @@ __global__ void __launch_bounds__(256) k_imp_sweep(const __grid_constant__ HsbPh
 #pragma unroll
     for (int c = 0; c < CH; c++) dmax[c] = smax[c] = 0.f;
     bool bad = false;
-    float* u = (mode == IMP_AM_PRED) ? up : (mode == IMP_AM_CORR ? uc : nullptr);
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-        hsb_imp_sweep_cell<CH>(mode, i, n, fdt, c0, c1, normalize, y0, w, prev_raw, dy, k0, u, up, uc, dmax, smax,
-                               bad);
-    if (mode != IMP_BDF_EULER) {
+        hsb_imp_sweep_cell<CH>(mode, i, n, dt, c0, c1, normalize, y0, w, w, dy, k0, w64, prev64, u64, up64, uc64,
+                               dmax, smax, bad);
+    if (mode != IMP_BDF_EULER && mode != IMP_AM_EULER) {
 #pragma unroll
         for (int c = 0; c < CH; c++) {
             imp_fold_max(dmax[c], &sd->red[c]);

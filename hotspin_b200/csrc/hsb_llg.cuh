@@ -309,7 +309,7 @@ __host__ __device__ inline bool hsb_gate(const HsbSolverDev* sd, int gate_word) 
 }
 
 // ------------------------------------------------------------------ am12 / bdf-euler sweeps
-enum { IMP_AM_PRED = 0, IMP_AM_CORR = 1, IMP_AM_ERR = 2, IMP_BDF_EULER = 3, IMP_BDF_SWEEP = 4 };
+enum { IMP_AM_PRED = 0, IMP_AM_CORR = 1, IMP_AM_ERR = 2, IMP_BDF_EULER = 3, IMP_BDF_SWEEP = 4, IMP_AM_EULER = 5 };
 enum {
     IMP_RULE_AM_BEGIN = 0, IMP_RULE_AM_ITER_PRED = 1, IMP_RULE_AM_ITER_CORR = 2, IMP_RULE_AM_PRED_END = 3,
     IMP_RULE_AM_CORR_END = 4, IMP_RULE_AM_FINAL = 5, IMP_RULE_BDF_BEGIN = 6, IMP_RULE_BDF_ITER = 7,
@@ -321,11 +321,15 @@ enum {
 struct ImpArgs {
     PtrSel y0;         // state at the start of the step (y[cur])
     PtrSel w;          // renormalised iterate / working state (y[next])
-    float* up;         // am12: raw predictor iterate
-    float* uc;         // am12: raw corrector iterate
     float* k0;         // am12: f(y0); bdf-euler: the latest derivative
     float* k1;         // am12: derivative at the explicit Euler point
     float* k2;         // am12: derivative of the latest iterate
+    // am12: FP64 renormalised iterate and raw predictor / corrector iterates, which the sweeps
+    // compare (the FP32 w, rounded from w64, feeds the right-hand side); slot 0's, the others
+    // one slot stride of floats further
+    double* w64;
+    double* up64;
+    double* uc64;
     int mode;          // IMP_AM_* / IMP_BDF_*
     int normalize;     // renormalise m where it is written to w (LLG mode)
     int eq;            // bdf-euler: equation (0 m, 1 Te, 2 Tl)
@@ -618,45 +622,79 @@ __host__ __device__ inline void hsb_llbar02(const float* m, const float* H, floa
     k[2] += g * (mu_par[2] * mH * m[2] + (m[0] * a1 - m[1] * a0));
 }
 
-// One cell of a fixed-point sweep (k_imp_sweep; host builds drive it cell by cell): forms the
-// new iterate of the channels [c0, c1) from y0 and the derivative, folds max|prev - new| and the
-// error scale (|new|, or |prev + new| for bdf-euler) into dmax / smax, writes the raw iterate to
-// u (am12 predictor / corrector) and the iterate, m renormalised when `normalize`, to w; the
-// am12 step-error mode compares uc with up (scale |up|) and writes nothing.
+// One cell of a fixed-point sweep (k_imp_sweep; host builds drive it cell by cell).
+// am12 (modes IMP_AM_*): the iterate is formed in FP64 from the FP32 state y0 and derivatives,
+// compared in FP64 with the previous iterate's FP64 copy (w64, or the raw predictor up64 in the
+// corrector's first sweep), so the sweep errors carry no FP32 rounding of the iterates; the raw
+// iterate goes to up64 / uc64, the renormalised one (m, when `normalize`) to w64 and, rounded,
+// to w for the next right-hand side.  IMP_AM_EULER forms the explicit Euler point that way; the
+// step-error mode compares uc64 with up64 (scale |up64|) and writes nothing.  bdf-euler
+// (IMP_BDF_*): FP32 throughout on the channels [c0, c1) of one equation, scale |prev + new|.
+// dmax / smax fold max|prev - new| and the error scale per channel.
 template <int CH>
-__host__ __device__ inline void hsb_imp_sweep_cell(int mode, long i, long n, float fdt, int c0, int c1,
+__host__ __device__ inline void hsb_imp_sweep_cell(int mode, long i, long n, double dt, int c0, int c1,
                                                    int normalize, const float* y0, float* w, const float* prev,
-                                                   const float* dy, const float* k0, float* u, const float* up,
-                                                   const float* uc, float* dmax, float* smax, bool& bad) {
+                                                   const float* dy, const float* k0, double* w64,
+                                                   const double* prev64, double* u64, const double* up64,
+                                                   const double* uc64, float* dmax, float* smax, bool& bad) {
     if (mode == IMP_AM_ERR) {
         for (int c = 0; c < CH; c++) {
-            const float a = uc[c * n + i], b = up[c * n + i];
-            dmax[c] = fmaxf(dmax[c], fabsf(a - b));
-            smax[c] = fmaxf(smax[c], fabsf(b));
+            const double a = uc64[c * n + i], b = up64[c * n + i];
+            dmax[c] = fmaxf(dmax[c], (float)fabs(a - b));
+            smax[c] = fmaxf(smax[c], (float)fabs(b));
             bad |= !isfinite(a - b);
         }
         return;
     }
+    if (mode == IMP_AM_PRED || mode == IMP_AM_CORR || mode == IMP_AM_EULER) {
+        double nv[CH];
+        for (int c = 0; c < CH; c++) {
+            const double b = (double)y0[c * n + i];
+            if (mode == IMP_AM_CORR)
+                nv[c] = b + (0.5 * dt) * ((double)dy[c * n + i] + (double)k0[c * n + i]);
+            else if (mode == IMP_AM_PRED)
+                nv[c] = b + dt * (double)dy[c * n + i];
+            else
+                nv[c] = b + dt * (double)k0[c * n + i];
+            bad |= !isfinite(nv[c]);
+        }
+        if (mode != IMP_AM_EULER) {
+            for (int c = 0; c < CH; c++) {
+                const double pv = prev64[c * n + i];
+                dmax[c] = fmaxf(dmax[c], (float)fabs(pv - nv[c]));
+                smax[c] = fmaxf(smax[c], (float)fabs(nv[c]));
+            }
+            for (int c = 0; c < CH; c++) u64[c * n + i] = nv[c];
+        }
+        // the reference renormalises m when it next updates it (before the next right-hand side)
+        if (normalize) {
+            const double l2 = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
+            const double inv = (l2 == 0.0) ? 0.0 : 1.0 / sqrt(l2);
+            nv[0] *= inv;
+            nv[1] *= inv;
+            nv[2] *= inv;
+        }
+        for (int c = 0; c < CH; c++) {
+            w64[c * n + i] = nv[c];
+            w[c * n + i] = (float)nv[c];
+        }
+        return;
+    }
+    const float fdt = (float)dt;
     float nv[CH];
     for (int c = 0; c < CH; c++) {
         nv[c] = 0.f;
         if (c < c0 || c >= c1) continue;
-        const float b = y0[c * n + i];
-        if (mode == IMP_AM_CORR) nv[c] = b + (0.5f * fdt) * (dy[c * n + i] + k0[c * n + i]);
-        else if (mode == IMP_AM_PRED) nv[c] = b + fdt * dy[c * n + i];
-        else nv[c] = b + fdt * k0[c * n + i];
+        nv[c] = y0[c * n + i] + fdt * k0[c * n + i];
         bad |= !isfinite(nv[c]);
     }
-    if (mode != IMP_BDF_EULER) {
+    if (mode == IMP_BDF_SWEEP) {
         for (int c = c0; c < c1; c++) {
             const float pv = prev[c * n + i];
             dmax[c] = fmaxf(dmax[c], fabsf(pv - nv[c]));
-            smax[c] = fmaxf(smax[c], mode == IMP_BDF_SWEEP ? fabsf(pv + nv[c]) : fabsf(nv[c]));
+            smax[c] = fmaxf(smax[c], fabsf(pv + nv[c]));
         }
     }
-    if (u)
-        for (int c = 0; c < CH; c++) u[c * n + i] = nv[c];
-    // the reference renormalises m when it next updates it (before the next right-hand side)
     if (normalize && c0 == 0) {
         const float l2 = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
 #ifdef __CUDA_ARCH__
@@ -670,4 +708,3 @@ __host__ __device__ inline void hsb_imp_sweep_cell(int mode, long i, long n, flo
     }
     for (int c = c0; c < c1; c++) w[c * n + i] = nv[c];
 }
-

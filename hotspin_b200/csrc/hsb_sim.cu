@@ -133,6 +133,7 @@ struct hsb_sim_s {
     bool launched;
     float* y[2];        // state double buffer
     float* ystage[2];   // stage points (ping-pong: a kernel never reads and writes one)
+    double* y64[3];     // am12: FP64 iterates (renormalised, raw predictor, raw corrector)
     float* k[8];        // stage derivatives
     float* hd;          // demag field of the stage point
     float* hd01[2];     // demag field of y[0], y[1] (DP45 with a thermal field)
@@ -438,8 +439,9 @@ static int L_sweep(hsb_sim_s* S, int mode, int eq = 0) {
     memset(&A, 0, sizeof(A));
     A.y0 = pair(S->y[0], S->y[1], SEL_CUR);
     A.w = pair(S->y[0], S->y[1], SEL_NEXT);
-    A.up = S->ystage[0];
-    A.uc = S->ystage[1];
+    A.w64 = S->y64[0];
+    A.up64 = S->y64[1];
+    A.uc64 = S->y64[2];
     A.k0 = S->k[0];
     A.k1 = S->k[1];
     A.k2 = S->k[2];
@@ -691,18 +693,15 @@ static int enqueue_attempt(hsb_sim_s* S) {
             const int* itg = &S->sd->it_active;
             RC(timed(S, PROF_OTHER, [&] { return L_rule(S, IMP_RULE_AM_BEGIN); }));
             RC(run_demag(S, nullptr, 0, hd, -1));
-            StageArgs A = empty_args();          // dy0 = f(t0, y0) and the explicit Euler point
+            StageArgs A = empty_args();          // dy0 = f(t0, y0)
             A.ys = YC;
             A.hd = fixed(hd);
             A.ytherm = YC;
             A.kout = fixed(S->k[0]);
             A.kself_w = 1.0f;
-            A.ynext = YN;
-            A.ybase = YC;
-            A.cself = 1.0f;
-            A.normalize = norm;
             thermal_keep(S, A, true);
             RC(timed(S, PROF_STAGE, [&] { return L_stage(S, A); }));
+            RC(timed(S, PROF_OTHER, [&] { return L_sweep(S, IMP_AM_EULER); }));  // the explicit Euler point
             StageArgs R = empty_args();          // f(t0 + dt, iterate)
             R.ys = YN;
             R.hd = fixed(hd);
@@ -1035,7 +1034,7 @@ static void fill_phys(hsb_sim_s* S) {
 
 // Offsets (floats) of one slot's buffers in its arena.
 struct SlotLayout {
-    long y, ystage, k, hd, hd01, hth, total;
+    long y, ystage, k, hd, hd01, hth, d64, total;
     int nk;
 };
 static SlotLayout slot_layout(const hsb_sim_desc& d, long n) {
@@ -1065,6 +1064,11 @@ static SlotLayout slot_layout(const hsb_sim_desc& d, long n) {
         L.hth = o;
         o += al(3 * n);
     }
+    L.d64 = -1;
+    if (d.solver == SOLVER_AM12) {  // FP64 iterates w64, up64, uc64 (2 floats per double)
+        L.d64 = o;
+        o += al(3 * 2 * ny);
+    }
     L.total = o;
     return L;
 }
@@ -1081,6 +1085,7 @@ static void point_slot0(hsb_sim_s* S, const SlotLayout& L) {
     S->hd01[0] = L.hd01 >= 0 ? a + L.hd01 : nullptr;
     S->hd01[1] = L.hd01 >= 0 ? S->hd01[0] + 3 * S->n : nullptr;
     S->hth = L.hth >= 0 ? a + L.hth : nullptr;
+    for (int j = 0; j < 3; j++) S->y64[j] = L.d64 >= 0 ? (double*)(a + L.d64) + j * ny : nullptr;
     S->slot_stride = L.total;
 }
 

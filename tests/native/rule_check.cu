@@ -160,14 +160,19 @@ extern "C" void llbar02_host(const float* m, const float* H, float g, const floa
 }
 
 // ---- one fixed-point sweep over all cells with the kernel's own cell code (hsb_imp_sweep_cell)
-extern "C" void imp_sweep_host(int ch, int mode, long n, float fdt, int c0, int c1, int normalize, const float* y0,
-                               float* w, const float* prev, const float* dy, const float* k0, float* u,
-                               const float* up, const float* uc, float* dmax, float* smax, int* bad) {
+extern "C" void imp_sweep_host(int ch, int mode, long n, double dt, int c0, int c1, int normalize, const float* y0,
+                               float* w, const float* prev, const float* dy, const float* k0, double* w64,
+                               const double* prev64, double* u64, const double* up64, const double* uc64, float* dmax,
+                               float* smax, int* bad) {
     bool b = false;
     for (int c = 0; c < 5; c++) dmax[c] = smax[c] = 0.f;
     for (long i = 0; i < n; i++) {
-        if (ch == 5) hsb_imp_sweep_cell<5>(mode, i, n, fdt, c0, c1, normalize, y0, w, prev, dy, k0, u, up, uc, dmax, smax, b);
-        else hsb_imp_sweep_cell<3>(mode, i, n, fdt, c0, c1, normalize, y0, w, prev, dy, k0, u, up, uc, dmax, smax, b);
+        if (ch == 5)
+            hsb_imp_sweep_cell<5>(mode, i, n, dt, c0, c1, normalize, y0, w, prev, dy, k0, w64, prev64, u64, up64, uc64,
+                                  dmax, smax, b);
+        else
+            hsb_imp_sweep_cell<3>(mode, i, n, dt, c0, c1, normalize, y0, w, prev, dy, k0, w64, prev64, u64, up64, uc64,
+                                  dmax, smax, b);
     }
     *bad = b ? 1 : 0;
 }

@@ -108,7 +108,7 @@ def test_rk12_oracle_run_keeps_the_reference_retry_count():
 # launch sequence in FP64 with the oracle's right-hand side and the host-built rules, and check
 # that it takes the same steps as the oracle's restatement of the reference solvers.
 
-AM_PRED, AM_CORR, AM_ERR, BDF_EULER, BDF_SWEEP = range(5)
+AM_PRED, AM_CORR, AM_ERR, BDF_EULER, BDF_SWEEP, AM_EULER = range(6)
 R_AM_BEGIN, R_AM_ITER_PRED, R_AM_ITER_CORR, R_AM_PRED_END, R_AM_CORR_END, R_AM_FINAL, R_BDF_BEGIN, R_BDF_ITER, \
     R_BDF_CLEAR = range(9)
 CHANNELS = {"m": (0, 3), "Te": (3, 1), "Tl": (4, 1)}
@@ -366,25 +366,28 @@ def test_second_order_relaxation_terms_match_oracle(rules):
 def _f32_sweeper(lib):
     f = lib.imp_sweep_host
     fp = ctypes.POINTER(ctypes.c_float)
-    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                  fp, fp, fp, fp, fp, fp, fp, fp, fp, fp, ctypes.POINTER(ctypes.c_int)]
+    dp = ctypes.POINTER(ctypes.c_double)
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                  fp, fp, fp, fp, fp, dp, dp, dp, dp, dp, fp, fp, ctypes.POINTER(ctypes.c_int)]
     f.restype = None
-    P = lambda a: a.ctypes.data_as(fp) if a is not None else None
+    P = lambda a: None if a is None else a.ctypes.data_as(dp if a.dtype == np.float64 else fp)
 
-    def sweep(mode, ch, fdt, c0, c1, normalize, y0, w, prev, dy, k0, u, up, uc):
+    def sweep(mode, ch, dt, c0, c1, normalize, y0, w, prev, dy, k0, w64=None, prev64=None, u64=None, up64=None,
+              uc64=None):
         dmax = np.zeros(5, np.float32)
         smax = np.zeros(5, np.float32)
         bad = ctypes.c_int()
-        f(ch, mode, y0.shape[1], fdt, c0, c1, normalize, P(y0), P(w), P(prev), P(dy), P(k0), P(u), P(up), P(uc),
-          P(dmax), P(smax), ctypes.byref(bad))
+        f(ch, mode, y0.shape[1], dt, c0, c1, normalize, P(y0), P(w), P(prev), P(dy), P(k0), P(w64), P(prev64), P(u64),
+          P(up64), P(uc64), P(dmax), P(smax), ctypes.byref(bad))
         return dmax, smax, bad.value
     return sweep
 
 
 def emulate_am12_kernel(lib, model, y0, dt, nsteps, mindt, maxdt, abs_err, rel_err, t_stop=0.0):
-    """enqueue_attempt's SOLVER_AM12 sequence with the sweep kernel's own cell code on FP32
-    buffers (channels x cells, as on the device); the right-hand sides are the oracle's, rounded
-    to FP32 as the stage kernels store them."""
+    """enqueue_attempt's SOLVER_AM12 sequence with the sweep kernel's own cell code on the
+    device's buffers (channels x cells): FP32 state, derivatives and right-hand-side iterate,
+    FP64 iterates compared by the sweeps; the right-hand sides are the oracle's, rounded to FP32
+    as the stage kernels store them."""
     sweep = _f32_sweeper(lib)
     keys = [k for k in ("m", "Te", "Tl") if k in y0]
     ch = 5 if len(keys) == 3 else 3
@@ -408,7 +411,8 @@ def emulate_am12_kernel(lib, model, y0, dt, nsteps, mindt, maxdt, abs_err, rel_e
                   t_stop=t_stop)
     R = lambda which: sd.rule(which, ab, rl, neq=neq)
     Y = pack(y0)
-    W, up, uc = np.zeros_like(Y), np.zeros_like(Y), np.zeros_like(Y)
+    W = np.zeros_like(Y)
+    w64, up64, uc64 = (np.zeros(Y.shape, np.float64) for _ in range(3))
     trace = []
 
     def fold(dmax, smax):
@@ -416,30 +420,27 @@ def emulate_am12_kernel(lib, model, y0, dt, nsteps, mindt, maxdt, abs_err, rel_e
             sd.fold(c, dmax[c])
             sd.fold(5 + c, smax[c])
     while sd["active"]:
-        t0, h = sd["t"], sd["dt"]
+        t0 = sd["t"]
         R(R_AM_BEGIN)
         k0 = f(t0, Y)
-        W = Y + np.float32(h) * k0
-        if norm:
-            W[:3] /= np.sqrt((W[:3] ** 2).sum(0))
-        k1 = f(t0 + h, W)
+        sweep(AM_EULER, ch, sd["dt"], 0, ch, norm, Y, W, W, None, k0, w64)
+        k1 = f(t0 + sd["dt"], W)
         k2 = np.zeros_like(k1)
         for phase in (0, 1):
             for j in range(6):
                 if sd["active"] and sd["it_active"]:
                     mode = AM_PRED if phase == 0 else AM_CORR
                     dy = k2 if sd["dysel"] else k1
-                    prev = up if (phase == 1 and sd["prevsel"]) else W
-                    prev = prev.copy()
-                    d, s_, _ = sweep(mode, ch, np.float32(sd["dt"]), 0, ch, norm, Y, W, prev, dy, k0,
-                                     up if phase == 0 else uc, up, uc)
+                    prev64 = up64 if (phase == 1 and sd["prevsel"]) else w64
+                    d, s_, _ = sweep(mode, ch, sd["dt"], 0, ch, norm, Y, W, W, dy, k0, w64, prev64,
+                                     up64 if phase == 0 else uc64)
                     fold(d, s_)
                 R(R_AM_ITER_PRED if phase == 0 else R_AM_ITER_CORR)
                 if j < 5 and sd["active"] and sd["it_active"]:
                     k2 = f(t0 + sd["dt"], W)
             R(R_AM_PRED_END if phase == 0 else R_AM_CORR_END)
         if sd["active"] and not int(sd["it_flags"]) & 4:
-            d, s_, _ = sweep(AM_ERR, ch, np.float32(sd["dt"]), 0, ch, norm, Y, W, W, k1, k0, None, up, uc)
+            d, s_, _ = sweep(AM_ERR, ch, sd["dt"], 0, ch, norm, Y, W, W, k1, k0, up64=up64, uc64=uc64)
             fold(d, s_)
         steps = sd["step"]
         R(R_AM_FINAL)
@@ -451,14 +452,15 @@ def emulate_am12_kernel(lib, model, y0, dt, nsteps, mindt, maxdt, abs_err, rel_e
     return out
 
 
-@pytest.mark.parametrize("case,tol", [("llg", (1e-4, 1e-3)), ("ttm", (1e-4, 1e-3)), ("ttm", (1e-5, 1e-5))])
+@pytest.mark.parametrize("case,tol", [("llg", (1e-4, 1e-3)), ("llg", (1e-5, 1e-5)), ("ttm", (1e-4, 1e-3)),
+                                      ("ttm", (1e-5, 1e-5))])
 def test_am12_with_the_sweep_kernels_cell_code(rules, case, tol):
-    """The same launch sequence with the sweep kernel's own per-cell code on FP32 buffers, to the
-    same end time as the oracle: as many steps and the state within 1e-5.  (For an LLG film at
-    tolerances below the reference's defaults, 1e-4 absolute and 1e-3 relative, the iterates'
-    FP32 rounding starts to set am12's step control: at 1e-5 / 1e-5 the FP32 sequence takes 6 %
-    fewer steps than the FP64 one over 50 fs and ends 2e-5 away; the two-temperature case keeps
-    the same steps.)"""
+    """The same launch sequence with the sweep kernel's own per-cell code on the device's buffers
+    (FP32 state and derivatives, FP64 iterates), to the same end time as the oracle: the same
+    number of steps, and the state within the FP32 rounding that the steps accumulate.  Below the
+    reference's default tolerances (1e-5 / 1e-5 for an LLG film, about 1400 steps) the sweeps'
+    comparisons of FP64 iterates keep the oracle's step sequence, which comparisons of FP32
+    iterates (rounding about 6e-8 of |m|) did not."""
     from oracle.solvers import Integrator
     model, y0 = _am_case() if case == "llg" else _ttm_case()
     keys = list(y0)
@@ -469,9 +471,9 @@ def test_am12_with_the_sweep_kernels_cell_code(rules, case, tol):
     it.run_until(t_end)
     Y, trace, status = emulate_am12_kernel(rules, model, y0, 1e-16, -1, 1e-22, 1e-12, abs_err, rel_err, t_stop=t_end)
     assert status == 0
-    assert abs(len(trace) - it.step_count) <= 1
+    assert len(trace) == it.step_count
     assert trace[-1][0] == pytest.approx(t_end, rel=1e-9)
     want = _fix(it.y, model.s.normalize)
-    assert np.abs(Y["m"] - want["m"]).max() < 1e-5
+    assert np.abs(Y["m"] - want["m"]).max() < (5e-6 if len(trace) > 1000 else 1e-6)
     if "Te" in keys:
-        assert np.abs(Y["Te"] - want["Te"]).max() < 1e-5 * np.abs(want["Te"]).max()
+        assert np.abs(Y["Te"] - want["Te"]).max() < 1e-6 * np.abs(want["Te"]).max()
