@@ -63,6 +63,38 @@ int main(void) {
     assert crc == 0xB90956C775A41001      # CRC-64/GO-ISO check value of "123456789"
 
 
+def test_every_descriptor_field_at_the_same_offset(tmp_path):
+    """Every field of hsb_sim_desc sits at the same offset in the public header, in the Python
+    mirror and in the library's own copy of the struct (hsb_sim.cu, compiled here as host C++)."""
+    import os
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    names = [f[0] for f in _lib.SimDesc._fields_]
+    body = open(os.path.join(root, "hotspin_b200", "csrc", "hsb_sim.cu")).read()
+    mirror = re.search(r"struct hsb_sim_desc \{.*?\n\};", body, re.S).group(0)
+    prints = "".join('    printf("%%s %%zu %%zu\\n", "%s", offsetof(hsb_sim_desc, %s), offsetof(lib::hsb_sim_desc, %s));\n'
+                     % (n, n, n) for n in names)
+    src = tmp_path / "layout.cpp"
+    src.write_text("#include <stddef.h>\n#include <stdint.h>\n#include <stdio.h>\n#include \"hotspin_b200.h\"\n"
+                   "namespace lib {\n" + mirror + "\n}\nint main() {\n" + prints +
+                   '    printf("sizeof %zu %zu\\n", sizeof(hsb_sim_desc), sizeof(lib::hsb_sim_desc));\n    return 0;\n}\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines()
+    rows = {l.split()[0]: tuple(int(x) for x in l.split()[1:]) for l in out}
+    D = _lib.SimDesc
+    assert rows["sizeof"] == (ctypes.sizeof(D), ctypes.sizeof(D))
+    bad = [(n, rows[n], getattr(D, n).offset) for n in names if rows[n] != (getattr(D, n).offset,) * 2]
+    assert not bad, bad
+    # and no field of the header is missing from the Python mirror
+    hdr = open(os.path.join(root, "include", "hotspin_b200.h")).read()
+    pub = re.search(r"typedef struct hsb_sim_desc \{(.*?)\n\} hsb_sim_desc;", hdr, re.S)
+    if pub:
+        decl = re.sub(r"/\*.*?\*/|//[^\n]*", "", pub.group(1), flags=re.S)
+        fields = set(re.findall(r"(\w+)\s*(?:\[\d+\])?\s*[;,]", decl))
+        assert fields <= set(names), sorted(fields - set(names))
+
+
 def _desc(**kw):
     from hotspin_b200.sim import make_desc
     base = dict(size=(1, 8, 8), cellsize=(1e-9,) * 3, msat0T0=8e5, lex=5e-9, solver="rk4", dt=1e-14)
