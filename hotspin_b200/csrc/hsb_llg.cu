@@ -1074,8 +1074,8 @@ __global__ void __launch_bounds__(256) k_combine(const __grid_constant__ HsbPhys
     }
 }
 
-// Dormand-Prince step-size control, one thread (see the controller rule in the header of
-// include/hotspin_b200.h).  Consumes the attempt's error maximum.
+// Dormand-Prince step-size control, one thread per slot (hsb_dp45_rule in hsb_llg.cuh).
+// Consumes the attempt's error maximum.
 __global__ void k_dp45_control(HsbSolverDev* sd0, int nslot) {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= nslot) return;
@@ -1085,39 +1085,7 @@ __global__ void k_dp45_control(HsbSolverDev* sd0, int nslot) {
     const unsigned int nf = sd->nonfinite;
     sd->err_acc = 0u;
     sd->nonfinite = 0u;
-    const double h = sd->dt;
-    double err = (double)ef;
-    bool finite = (nf == 0u) && isfinite(err);
-    bool accept = finite && (err <= 1.0 || h <= sd->mindt);
-    double fac;
-    if (!finite) fac = 0.2;
-    else if (err == 0.0) fac = 5.0;
-    else fac = 0.9 * pow(err, -0.2);
-    fac = fmin(fmax(fac, 0.2), accept ? 5.0 : 1.0);
-    double nd = fmin(fmax(h * fac, sd->mindt), sd->maxdt);
-    sd->err = finite ? err : INFINITY;
-    sd->attempts += 1;
-    if (!finite && h <= sd->mindt) sd->status |= 1;
-    // a step taken at the floor without meeting the tolerance (accepted because dt cannot
-    // shrink further; hotspin's rk12 accepts such steps the same way, solve_rk12.go:196-198)
-    if (finite && err > 1.0 && h <= sd->mindt) sd->status |= 2;
-    if (accept) {
-        sd->t += h;
-        sd->step += 1;
-        sd->cur = 1 - sd->cur;
-        sd->kslot = 1 - sd->kslot;
-    } else {
-        sd->rejects += 1;
-        if (h <= sd->mindt) sd->status |= 2;
-    }
-    if (sd->t_stop > 0.0) {
-        const double rem = sd->t_stop - sd->t;
-        if (rem <= 1e-6 * nd || rem <= 0.0) sd->active = 0;
-        else if (nd > rem) nd = rem;
-    }
-    if (sd->step_stop >= 0 && sd->step >= sd->step_stop) sd->active = 0;
-    if (sd->status & 1) sd->active = 0;
-    sd->dt = nd;
+    hsb_dp45_rule(*sd, ef, nf != 0u);
 }
 
 // hotspin's adaptive Heun (rk12) step control, one thread per slot: consumes the attempt's

@@ -187,6 +187,49 @@ struct HsbSolverDev {
                            // scale per channel (5..9: |new|, |predictor| or |prev + new|)
 };
 
+// Dormand-Prince step-size rule (the controller described in include/hotspin_b200.h), applied
+// to one solver word after an attempt: err = the attempt's error norm (max over the cells of
+// |e| / (rtol scale)), nonfinite its non-finite flag.  Accept at err <= 1 or at the dt floor;
+// factor 0.9 err^(-1/5) clamped to [0.2, 5] (to [0.2, 1] after a rejection), 0.2 for a
+// non-finite attempt (status bit 1 at the floor), 5 for err = 0; dt_new clamped to
+// [mindt, maxdt] and to the time left before t_stop.  Status bit 2: an attempt at the floor
+// that did not meet the tolerance.
+__host__ __device__ inline void hsb_dp45_rule(HsbSolverDev& sd, float ef, bool nonfinite) {
+    const double h = sd.dt;
+    const double err = (double)ef;
+    const bool finite = !nonfinite && isfinite(err);
+    const bool accept = finite && (err <= 1.0 || h <= sd.mindt);
+    double fac;
+    if (!finite) fac = 0.2;
+    else if (err == 0.0) fac = 5.0;
+    else fac = 0.9 * pow(err, -0.2);
+    fac = fmin(fmax(fac, 0.2), accept ? 5.0 : 1.0);
+    double nd = fmin(fmax(h * fac, sd.mindt), sd.maxdt);
+    sd.err = finite ? err : INFINITY;
+    sd.attempts += 1;
+    if (!finite && h <= sd.mindt) sd.status |= 1;
+    // a step taken at the floor without meeting the tolerance (accepted because dt cannot
+    // shrink further; hotspin's rk12 accepts such steps the same way, solve_rk12.go:196-198)
+    if (finite && err > 1.0 && h <= sd.mindt) sd.status |= 2;
+    if (accept) {
+        sd.t += h;
+        sd.step += 1;
+        sd.cur = 1 - sd.cur;
+        sd.kslot = 1 - sd.kslot;
+    } else {
+        sd.rejects += 1;
+        if (h <= sd.mindt) sd.status |= 2;
+    }
+    if (sd.t_stop > 0.0) {
+        const double rem = sd.t_stop - sd.t;
+        if (rem <= 1e-6 * nd || rem <= 0.0) sd.active = 0;
+        else if (nd > rem) nd = rem;
+    }
+    if (sd.step_stop >= 0 && sd.step >= sd.step_stop) sd.active = 0;
+    if (sd.status & 1) sd.active = 0;
+    sd.dt = nd;
+}
+
 // Step-size rule of hotspin's adaptive Heun solver (solve_rk12.go:91-214), applied to one
 // solver word after an attempt.  err[q] = dt max_i |k1_i - k0_i| over the cells and
 // components of equation q (m, Te, Tl in this order; neq of them), maxerr[q] its

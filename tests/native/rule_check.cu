@@ -39,7 +39,10 @@ extern "C" void hsd_free(HsbSolverDev* p) { delete p; }
 #define HSD_FIELDS(X)                                                                           \
     X(t) X(dt) X(step) X(attempts) X(rejects) X(cur) X(active) X(status) X(err) X(mindt) X(maxdt) \
     X(t_stop) X(step_stop) X(tries) X(it_active) X(it_count) X(it_flags) X(aborts) X(dysel)        \
-    X(prevsel) X(eq) X(rhs_due) X(alpha_max) X(nonfinite)
+    X(prevsel) X(eq) X(rhs_due) X(alpha_max) X(nonfinite) X(kslot)
+
+// hsb_dp45_rule (the DP45 controller kernel's rule) on a host solver word.
+extern "C" void dp45_rule_host(HsbSolverDev* p, float err, int nonfinite) { hsb_dp45_rule(*p, err, nonfinite != 0); }
 
 extern "C" double hsd_get(const HsbSolverDev* p, const char* name) {
     const std::string n(name);

@@ -101,6 +101,65 @@ def test_rk12_oracle_run_keeps_the_reference_retry_count():
     assert it.bad_steps == 11
 
 
+def _dp45_host(lib):
+    f = lib.dp45_rule_host
+    f.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_int]
+    f.restype = None
+    return f
+
+
+def test_dp45_rule_matches_oracle_controller(rules):
+    """hsb_dp45_rule (the device's DP45 controller) against the oracle's _dp45 step control on
+    random, boundary and non-finite errors: accept / reject, the next dt, the counters, the
+    t_stop clamp and the status bits."""
+    f = _dp45_host(rules)
+    rng = np.random.default_rng(11)
+    errs = list(np.exp(rng.uniform(np.log(1e-12), np.log(1e6), 400))) + [0.0, 1.0, np.nextafter(1.0, 2.0), 1e-30,
+                                                                        3.0e38, float("inf"), float("nan")]
+    for k, e in enumerate(errs):
+        e32 = float(np.float32(e))
+        dt = float(np.exp(rng.uniform(np.log(1e-18), np.log(1e-12))))
+        mindt = dt if k % 7 == 0 else 1e-22          # every 7th attempt at the floor
+        maxdt = float(dt * rng.uniform(0.5, 20.0))
+        t0 = float(rng.uniform(0.0, 1e-11))
+        t_stop = t0 + dt * float(rng.choice([0.5, 1.0, 1.3, 3.0, 100.0])) if k % 3 == 0 else 0.0
+        sd = HostWord(rules, t=t0, dt=dt, mindt=mindt, maxdt=maxdt, t_stop=t_stop, step_stop=-1, active=1)
+        f(sd.p, e32, 0)
+        # the oracle's rule (oracle/solvers.py _dp45) and the device's t_stop / status handling
+        finite = np.isfinite(e32)
+        accept = finite and (e32 <= 1.0 or dt <= mindt)
+        fac = 0.2 if not finite else (5.0 if e32 == 0.0 else 0.9 * e32 ** -0.2)
+        fac = min(max(fac, 0.2), 5.0 if accept else 1.0)
+        nd = min(max(dt * fac, mindt), maxdt)
+        t1 = t0 + dt if accept else t0
+        active = 1
+        if t_stop > 0.0:
+            rem = t_stop - t1
+            if rem <= 1e-6 * nd or rem <= 0.0:
+                active = 0
+            elif nd > rem:
+                nd = rem
+        floor = dt <= mindt
+        status = (1 if floor and not finite else 0) | (2 if floor and (not accept or e32 > 1.0) else 0)
+        if status & 1:
+            active = 0
+        assert sd["step"] == (1 if accept else 0), (e32, dt, mindt)
+        assert sd["rejects"] == (0 if accept else 1)
+        assert sd["cur"] == (1 if accept else 0) and sd["kslot"] == (1 if accept else 0)
+        assert sd["t"] == t1
+        assert sd["dt"] == pytest.approx(nd, rel=1e-14)
+        assert sd["active"] == active
+        assert int(sd["status"]) == status, (e32, dt, mindt, int(sd["status"]), status)
+        if finite:
+            assert sd["err"] == e32
+        sd.close()
+    # the non-finite flag of the attempt rejects whatever the error says
+    sd = HostWord(rules, t=0.0, dt=1e-15, mindt=1e-22, maxdt=1e-12, step_stop=-1, active=1)
+    f(sd.p, 0.5, 1)
+    assert sd["step"] == 0 and sd["dt"] == pytest.approx(2e-16, rel=1e-14) and int(sd["status"]) == 0
+    sd.close()
+
+
 # ---------------------------------------------------------------- implicit solvers, emulated
 # The device runs am12 / bdf-euler as a fixed sequence of gated launches (hsb_sim.cu
 # enqueue_attempt): sweeps (k_imp_sweep) fold per-channel maxima into the solver word and the
