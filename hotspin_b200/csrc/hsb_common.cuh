@@ -70,20 +70,30 @@ __device__ __forceinline__ float warp_max_f(float v) {
     return v;
 }
 
+// Read-only loads and fast FP32 division: the device intrinsics, plain forms in host builds
+// of the shared per-cell code.
+#ifdef __CUDA_ARCH__
+#define HSB_LDG(p) __ldg(p)
+#define HSB_FDIV(a, b) __fdividef(a, b)
+#else
+#define HSB_LDG(p) (*(p))
+#define HSB_FDIV(a, b) ((a) / (b))
+#endif
+
 // Harmonic mean 2ab/(a+b), 0 when a+b == 0 (the reference's avgGeomZero).
 template <typename T>
-__device__ __forceinline__ T harm0(T a, T b) {
+__host__ __device__ __forceinline__ T harm0(T a, T b) {
     T s = a + b;
     return (s == T(0)) ? T(0) : T(2) * a * b / s;
 }
 
 // Neighbour index along an axis: wrap when periodic, clamp otherwise.
-__device__ __forceinline__ int nb_lo(int i, int n, int wrap) {
+__host__ __device__ __forceinline__ int nb_lo(int i, int n, int wrap) {
     int j = i - 1;
     if (j < 0) j = wrap ? n - 1 : 0;
     return j;
 }
-__device__ __forceinline__ int nb_hi(int i, int n, int wrap) {
+__host__ __device__ __forceinline__ int nb_hi(int i, int n, int wrap) {
     int j = i + 1;
     if (j >= n) j = wrap ? 0 : n - 1;
     return j;

@@ -70,7 +70,7 @@ struct HsbPhys {
 // a (time, factor) table as hotspin's pointwise quantities evaluate theirs
 // (engine/update_pointwiseof.go:31-98); zero outside the table's time range.  Uniform over a
 // launch: every thread finds the same table interval.
-__device__ __forceinline__ float hsb_laser_power(const HsbPhys& P, double t) {
+__host__ __device__ __forceinline__ float hsb_laser_power(const HsbPhys& P, double t) {
     if (P.laser_p0 == 0.f) return 0.f;
     if (P.laser_npts >= 2) {
         const double2* tab = P.laser_tab;
@@ -92,7 +92,7 @@ __device__ __forceinline__ float hsb_laser_power(const HsbPhys& P, double t) {
 // Applied field H_ext (A/m) at time t: the constant bext, or the piecewise-linear interpolation
 // of the (time, B) table divided by mu0 (a pointwise quantity as in
 // engine/update_pointwiseof.go:31-98), zero outside the table's time range.
-__device__ __forceinline__ void hsb_bext(const HsbPhys& P, double t, float* h) {
+__host__ __device__ __forceinline__ void hsb_bext(const HsbPhys& P, double t, float* h) {
     if (P.bext_npts >= 2) {
         const double* tab = P.bext_tab;
         int lo = 0, hi = P.bext_npts - 1;

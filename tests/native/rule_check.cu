@@ -1,7 +1,9 @@
 // Host build of the device step-control rules (test support, compiled by the CPU tests with
 // nvcc as host code): the same inline functions the controller kernels run, driven from
 // Python through ctypes so the rules can be checked against the oracle without a GPU.
+#include "hsb_desc.h"
 #include "hsb_llg.cuh"
+#include "hsb_rhs.cuh"
 
 // One rk12 attempt on a fresh solver word.  out: dt_new, accepted (0/1), status, tries,
 // active, err.
@@ -178,4 +180,40 @@ extern "C" void imp_sweep_host(int ch, int mode, long n, double dt, int c0, int 
                                   dmax, smax, b);
     }
     *bad = b ? 1 : 0;
+}
+
+// The generic stage kernel's per-cell right-hand side (rhs_cell) over every cell of a grid,
+// with the physics the library derives from the descriptor (phys_from_desc).  Buffers are
+// FP32 [channel][cell] as on the device: ys the state, hd the demag field (A/m, or null), yth
+// the state whose Te sets the thermal amplitude; masks and tables optional (host copies).
+// With the non-local relaxation term a first pass stores every cell's effective field in
+// hbuf ([3][cell]), as the kernel's first launch does.  k: [channel][cell].
+extern "C" void rhs_host(const hsb_sim_desc* d, const float* ys, const float* hd, const float* yth, double t,
+                         double dt, long long step, const float* msat_mask, const float* lex_mask, float* hbuf,
+                         float* k) {
+    const int nch = d->ttm ? 5 : 3;
+    const long n = (long)d->size[0] * d->size[1] * d->size[2];
+    HsbPhys P;
+    phys_from_desc(*d, nch, n, P);
+    P.msat_mask = msat_mask;
+    P.lex_mask = lex_mask;
+    P.laser_tab = (const double2*)d->laser_table;
+    P.laser_npts = d->laser_table ? d->laser_npts : 0;
+    P.bext_tab = d->bext_table;
+    P.bext_npts = d->bext_table ? d->bext_npts : 0;
+    P.hbuf = hbuf;
+    for (int pass = P.nonlocal ? 0 : 1; pass < 2; pass++) {
+        for (long i = 0; i < n; i++) {
+            const int a2 = (int)(i % P.N2);
+            const long r = i / P.N2;
+            const int a1 = (int)(r % P.N1);
+            const int a0 = (int)(r / P.N1);
+            float y[5], kk[5];
+            float* hout = pass == 0 ? hbuf : nullptr;
+            if (nch == 5) rhs_cell<5>(P, ys, hd, yth, t, dt, step, a0, a1, a2, i, y, kk, false, hout);
+            else rhs_cell<3>(P, ys, hd, yth, t, dt, step, a0, a1, a2, i, y, kk, false, hout);
+            if (pass == 1)
+                for (int c = 0; c < nch; c++) k[c * n + i] = kk[c];
+        }
+    }
 }

@@ -65,12 +65,12 @@ int main(void) {
 
 def test_every_descriptor_field_at_the_same_offset(tmp_path):
     """Every field of hsb_sim_desc sits at the same offset in the public header, in the Python
-    mirror and in the library's own copy of the struct (hsb_sim.cu, compiled here as host C++)."""
+    mirror and in the library's own copy of the struct (hsb_desc.h, compiled here as host C++)."""
     import os
     import re
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     names = [f[0] for f in _lib.SimDesc._fields_]
-    body = open(os.path.join(root, "hotspin_b200", "csrc", "hsb_sim.cu")).read()
+    body = open(os.path.join(root, "hotspin_b200", "csrc", "hsb_desc.h")).read()
     mirror = re.search(r"struct hsb_sim_desc \{.*?\n\};", body, re.S).group(0)
     prints = "".join('    printf("%%s %%zu %%zu\\n", "%s", offsetof(hsb_sim_desc, %s), offsetof(lib::hsb_sim_desc, %s));\n'
                      % (n, n, n) for n in names)
