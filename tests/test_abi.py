@@ -23,6 +23,62 @@ def test_every_declared_symbol_is_exported():
     assert names <= exported, sorted(names - exported)
 
 
+def test_python_signatures_match_the_header_prototypes():
+    """Every ctypes signature the bindings set (hotspin_b200/_lib.py) has the header
+    prototype's parameter count, and each parameter and result the C type's width and kind."""
+    import os
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = "".join(open(os.path.join(root, "include", f)).read() for f in sorted(os.listdir(os.path.join(root, "include"))))
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"//[^\n]*", "", src)
+    handles = ("hsb_sim", "hsb_batch", "hsb_demag_plan")
+
+    def ctype_of(decl):
+        d = re.sub(r"\bconst\b", "", decl).strip()
+        d = re.sub(r"\s+\w+$", "", d) if not d.endswith("*") else d   # drop the parameter name
+        d = d.replace(" ", "")
+        if d in handles or d == "void*":
+            return ctypes.c_void_p
+        if d.endswith("*"):
+            base = d[:-1]
+            if base == "char":
+                return ctypes.c_char_p
+            if base in handles:
+                return ctypes.POINTER(ctypes.c_void_p)
+            return ctypes.POINTER(ctype_of(base + " x"))
+        return {"int": ctypes.c_int, "int32_t": ctypes.c_int32, "int64_t": ctypes.c_int64, "long": ctypes.c_long,
+                "double": ctypes.c_double, "float": ctypes.c_float, "uint64_t": ctypes.c_uint64,
+                "hsb_sim_desc": _lib.SimDesc}[d]
+
+    def same(a, b):
+        if a is None or b is None:
+            return a is b
+        if b is ctypes.c_void_p and (a is ctypes.c_void_p or a.__name__.startswith("LP_")):
+            return True       # device addresses and opaque buffers are bound as void*
+        if hasattr(a, "_type_") and hasattr(b, "_type_") and a.__name__.startswith("LP_"):
+            return b.__name__.startswith("LP_") and same(a._type_, b._type_)
+        return ctypes.sizeof(a) == ctypes.sizeof(b) and a._type_ == b._type_ if hasattr(a, "_type_") and \
+            isinstance(a._type_, str) and hasattr(b, "_type_") and isinstance(b._type_, str) else a is b
+
+    bad = []
+    for name, (res, args) in _lib._SIGS.items():
+        m = re.search(r"([\w\s\*]+?)\b" + name + r"\s*\(([^)]*)\)\s*;", src)
+        assert m, "no prototype for " + name
+        params = [p.strip() for p in m.group(2).split(",") if p.strip() and p.strip() != "void"]
+        ret = m.group(1).strip().split("\n")[-1].strip()
+        want_res = None if ret == "void" else ctype_of(ret + (" x" if not ret.endswith("*") else ""))
+        if len(params) != len(args):
+            bad.append((name, "parameter count", len(params), len(args)))
+            continue
+        if not same(want_res, res):
+            bad.append((name, "result", ret, res))
+        for p, a in zip(params, args):
+            if not same(ctype_of(p), a):
+                bad.append((name, p, a))
+    assert not bad, bad
+
+
 def test_errors_are_reported_not_aborted():
     lib = _lib.load()
     h = ctypes.c_void_p()
