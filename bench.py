@@ -12,6 +12,7 @@ accepted DP45 step of the whole grid; value = cells x accepted steps / device ti
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 """
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -51,7 +52,6 @@ def workload():
 
 def equilibrium_lib(kw, T=300.0):
     """m_e(T) from the product library's FP64 mean-field table."""
-    import ctypes
     from hotspin_b200 import _lib
     me = ctypes.c_double()
     _lib.check(_lib.load().hsb_mfa_equilibrium(T, kw["tc"], kw["spin_j"], ctypes.byref(me)), "m_e")
@@ -328,7 +328,7 @@ def run_ours(args):
     same = all(r["attempts"] == reps[0]["attempts"] and r["t_ps"] == reps[0]["t_ps"] for r in reps)
     value = whole_job_value(world, ncell, args.steps, ms)
     # ---- live per-kernel timing of one attempt (eager launches between CUDA events)
-    prof = (ctypes_double * 7)()
+    prof = (ctypes.c_double * 7)()
     _lib.check(sim._lib.hsb_sim_profile(sim._h, 3, prof), "profile")
     cats = {"stage": prof[0], "xfwd": prof[1], "yz": prof[2], "xinv": prof[3], "other": prof[4]}
     ab = algorithmic_bytes(kw)
@@ -535,14 +535,6 @@ def profile_demag(size):
     torch.cuda.synchronize()
     print("demag", tuple(size), "ms x-fwd / y-z / x-inv", [round(x, 5) for x in ms])
     lib.hsb_demag_plan_destroy(plan)
-
-
-def ctypes_int():
-    import ctypes
-    return ctypes.c_int()
-
-
-ctypes_double = __import__("ctypes").c_double
 
 
 def main():
