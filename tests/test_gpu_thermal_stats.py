@@ -10,8 +10,12 @@
    within 3 sigma, xi = Ms V B / (kB T_eff).  hotspin's noise (variance
    2 kB T lambda / (mu0 Ms V gamma_LL dt), mod_brown.go:125-145) drives the Landau-Lifshitz
    form of the LLBar equation, whose stationary temperature is T (1 + lambda^2) when gamma_LL
-   is the bare gyromagnetic ratio: T_eff below.  Snapshots are two relaxation times apart, so
-   spins and snapshots are independent samples.
+   is the bare gyromagnetic ratio: T_eff below.  Snapshots are three relaxation times apart
+   (correlation below e^-3), so spins and snapshots are close to independent samples.  The
+   same Heun scheme on macrospins in NumPy (65536 spins, lambda 0.1, 300 K) gives <cos theta>
+   at 1.7 and 0.3 sigma from L(xi / (1 + lambda^2)) at dt = 2e-14 and 4e-14 s and 8 sigma away
+   from L(xi): the T (1 + lambda^2) temperature is the scheme's, and its time-step bias is
+   below the sampling error.
 """
 import numpy as np
 import pytest
@@ -98,8 +102,8 @@ def test_equilibrium_is_boltzmann_3sigma(cuda, T):
         m = np.zeros((3,) + size)
         m[0] = 1.0
         sim.set("m", m)
-        per = int(round(2 * tau / dt))
-        sim.step(3 * per)                           # six relaxation times to equilibrium
+        per = int(round(3 * tau / dt))
+        sim.step(3 * per)                           # nine relaxation times to equilibrium
         for _ in range(10):
             sim.step(per)
             samples.append(sim.get("m")[0].ravel())
