@@ -17,7 +17,7 @@
 
 // cos(2 pi k / 64) through quarter-wave symmetry of cos(2 pi k / 64), k = 0..16
 // (mathematical constants).
-__device__ __forceinline__ constexpr double c64q(int k) {
+__host__ __device__ __forceinline__ constexpr double c64q(int k) {
     return k == 0 ? 1.0
          : k == 1 ? 0.9951847266721969
          : k == 2 ? 0.9807852804032304
@@ -36,13 +36,13 @@ __device__ __forceinline__ constexpr double c64q(int k) {
          : k == 15 ? 0.09801714032956077
          : 0.0;
 }
-__device__ __forceinline__ constexpr double c64cos(int k) {
+__host__ __device__ __forceinline__ constexpr double c64cos(int k) {
     return (k & 63) <= 16 ? c64q(k & 63)
          : (k & 63) <= 32 ? -c64q(32 - (k & 63))
          : (k & 63) <= 48 ? -c64q((k & 63) - 32)
          : c64q(64 - (k & 63));
 }
-__device__ __forceinline__ constexpr double c64sin(int k) { return c64cos(k - 16); }
+__host__ __device__ __forceinline__ constexpr double c64sin(int k) { return c64cos(k - 16); }
 
 // In-register radix-2 DIT FFT of R = 1..64 points on v[0..R), bit-reversed input order
 // handled by the unrolled permutation; every twiddle is a compile-time constant.
@@ -50,7 +50,7 @@ __device__ __forceinline__ constexpr double c64sin(int k) { return c64cos(k - 16
 // copies.  HOUT: only the lower half of the output is wanted — the last stage skips the
 // upper outputs (left unspecified).
 template <int R, int DIR, bool ZIN = false, bool HOUT = false>
-__device__ __forceinline__ void fft_reg64(float2* v) {
+__host__ __device__ __forceinline__ void fft_reg64(float2* v) {
     constexpr int B = ilog2c(R);
 #pragma unroll
     for (int i = 0; i < R; i++) {
@@ -110,6 +110,47 @@ template <int L> struct Slot {
     static constexpr int S = (T % 2 == 0) ? T + 1 : T;
 };
 
+// The two halves of the four-step transform of one sequence, split at its shared-memory
+// exchange (host builds run every lane's first half, then every lane's second half).
+// First: the A-point FFT in registers, the twiddles, the A x B intermediate to the slot.
+template <int L, int DIR, bool ZIN = false, bool SMTW = false>
+__host__ __device__ __forceinline__ void fft4_first(float2 (&v)[Split<L>::A], float2* slot, int lane,
+                                                    const float2* __restrict__ tw4) {
+    constexpr int A = Split<L>::A, B = Split<L>::B;
+    // n = B n1 + n2 >= L/2 exactly when n1 >= A/2
+    fft_reg64<A, DIR, ZIN>(v);
+    if (B > 1) {
+#pragma unroll
+        for (int k1 = 1; k1 < A; k1++) {
+#ifdef __CUDA_ARCH__
+            float2 w = SMTW ? tw4[k1 * B + lane] : __ldg(&tw4[k1 * B + lane]);
+#else
+            float2 w = tw4[k1 * B + lane];
+#endif
+            if (DIR > 0) w.y = -w.y;
+            const float2 a = v[k1];
+            v[k1] = make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < A; k1++) slot[lane * (A + 1) + k1] = v[k1];
+    }
+}
+
+// Second: lane t reads the A/B columns k1 = t + B i back and runs their B-point FFTs.
+template <int L, int DIR, bool HOUT = false>
+__host__ __device__ __forceinline__ void fft4_second(float2 (&v)[Split<L>::A], const float2* slot, int lane) {
+    constexpr int A = Split<L>::A, B = Split<L>::B;
+    if (B > 1) {
+#pragma unroll
+        for (int i = 0; i < A / B; i++) {
+#pragma unroll
+            for (int n2 = 0; n2 < B; n2++) v[i * B + n2] = slot[n2 * (A + 1) + lane + B * i];
+            // X index (lane + B i) + A k2 >= L/2 exactly when k2 >= B/2
+            fft_reg64<B, DIR, false, HOUT>(v + i * B);
+        }
+    }
+}
+
 // Four-step transform of one sequence (see header).  `lane` in [0, B); all B lanes of
 // the sequence, and every existing lane of the warp (`wmask`), must call it.
 // `tw4`: the A x B twiddle matrix of length L, in global memory, or in shared memory
@@ -118,33 +159,16 @@ template <int L> struct Slot {
 template <int L, int DIR, bool ZIN = false, bool HOUT = false, bool SMTW = false>
 __device__ __forceinline__ void fft4(float2 (&v)[Split<L>::A], float2* slot, int lane,
                                      const float2* __restrict__ tw4, unsigned wmask = 0xffffffffu) {
-    constexpr int A = Split<L>::A, B = Split<L>::B;
-    // n = B n1 + n2 >= L/2 exactly when n1 >= A/2
-    fft_reg64<A, DIR, ZIN>(v);
-    if (B > 1) {
-#pragma unroll
-        for (int k1 = 1; k1 < A; k1++) {
-            float2 w = SMTW ? tw4[k1 * B + lane] : __ldg(&tw4[k1 * B + lane]);
-            if (DIR > 0) w.y = -w.y;
-            const float2 a = v[k1];
-            v[k1] = make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
-        }
-#pragma unroll
-        for (int k1 = 0; k1 < A; k1++) slot[lane * (A + 1) + k1] = v[k1];
+    fft4_first<L, DIR, ZIN, SMTW>(v, slot, lane, tw4);
+    if (Split<L>::B > 1) {
         __syncwarp(wmask);
-#pragma unroll
-        for (int i = 0; i < A / B; i++) {
-#pragma unroll
-            for (int n2 = 0; n2 < B; n2++) v[i * B + n2] = slot[n2 * (A + 1) + lane + B * i];
-            // X index (lane + B i) + A k2 >= L/2 exactly when k2 >= B/2
-            fft_reg64<B, DIR, false, HOUT>(v + i * B);
-        }
+        fft4_second<L, DIR, HOUT>(v, slot, lane);
         __syncwarp(wmask);
     }
 }
 
 // Index of output element j of lane `lane`: X index (lane + B i) + A k2 with j = i B + k2.
 template <int L>
-__device__ __forceinline__ constexpr int fft4_out_index(int lane, int j) {
+__host__ __device__ __forceinline__ constexpr int fft4_out_index(int lane, int j) {
     return (lane + Split<L>::B * (j / Split<L>::B)) + Split<L>::A * (j % Split<L>::B);
 }

@@ -2,6 +2,7 @@
 // nvcc as host code): the same inline functions the controller kernels run, driven from
 // Python through ctypes so the rules can be checked against the oracle without a GPU.
 #include "hsb_desc.h"
+#include "hsb_fft4.cuh"
 #include "hsb_llg.cuh"
 #include "hsb_rhs.cuh"
 
@@ -215,5 +216,61 @@ extern "C" void rhs_host(const hsb_sim_desc* d, const float* ys, const float* hd
             if (pass == 1)
                 for (int c = 0; c < nch; c++) k[c * n + i] = kk[c];
         }
+    }
+}
+
+// The four-step register FFT of one sequence (fft4 in hsb_fft4.cuh) with its lanes run one
+// after the other: every lane's first half (A-point FFT, twiddles, write to the shared slot),
+// then every lane's second half (read back, B-point FFTs), as the warp does between its
+// __syncwarp calls.  x and X interleaved (re, im), L points; tw4 the A x B twiddle matrix.
+template <int L, int DIR, bool ZIN, bool HOUT>
+static void fft4_run(const float* x, const float* tw, float* X) {
+    constexpr int A = Split<L>::A, B = Split<L>::B;
+    static float2 v[B][A];
+    static float2 slot[Slot<L>::S];
+    const float2* tw4 = (const float2*)tw;
+    for (int t = 0; t < B; t++)
+        for (int n1 = 0; n1 < A; n1++) v[t][n1] = make_float2(x[2 * (B * n1 + t)], x[2 * (B * n1 + t) + 1]);
+    for (int t = 0; t < B; t++) fft4_first<L, DIR, ZIN>(v[t], slot, t, tw4);
+    for (int t = 0; t < B; t++) fft4_second<L, DIR, HOUT>(v[t], slot, t);
+    for (int t = 0; t < B; t++)
+        for (int j = 0; j < A; j++) {
+            const int k = fft4_out_index<L>(t, j);
+            X[2 * k] = v[t][j].x;
+            X[2 * k + 1] = v[t][j].y;
+        }
+}
+
+template <int L>
+static void fft4_dispatch(int dir, int zin, int hout, const float* x, const float* tw, float* X) {
+    const int c = (dir > 0 ? 4 : 0) + (zin ? 2 : 0) + (hout ? 1 : 0);
+    switch (c) {
+        case 0: fft4_run<L, -1, false, false>(x, tw, X); break;
+        case 1: fft4_run<L, -1, false, true>(x, tw, X); break;
+        case 2: fft4_run<L, -1, true, false>(x, tw, X); break;
+        case 3: fft4_run<L, -1, true, true>(x, tw, X); break;
+        case 4: fft4_run<L, 1, false, false>(x, tw, X); break;
+        case 5: fft4_run<L, 1, false, true>(x, tw, X); break;
+        case 6: fft4_run<L, 1, true, false>(x, tw, X); break;
+        default: fft4_run<L, 1, true, true>(x, tw, X); break;
+    }
+}
+
+// Split<L>::B of a length (0 when fft4 has no such length).
+extern "C" int fft4_lanes(int L) {
+    switch (L) {
+#define FB(N) case N: return Split<N>::B;
+        FB(2) FB(4) FB(8) FB(16) FB(32) FB(64) FB(128) FB(256) FB(512) FB(1024) FB(2048)
+#undef FB
+        default: return 0;
+    }
+}
+
+extern "C" int fft4_host(int L, int dir, int zin, int hout, const float* x, const float* tw, float* X) {
+    switch (L) {
+#define FD(N) case N: fft4_dispatch<N>(dir, zin, hout, x, tw, X); return 0;
+        FD(2) FD(4) FD(8) FD(16) FD(32) FD(64) FD(128) FD(256) FD(512) FD(1024) FD(2048)
+#undef FD
+        default: return 1;
     }
 }
