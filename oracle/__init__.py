@@ -14,7 +14,7 @@ golden dumps (``tests/test-exchange/hex_ref*.dump``, ``tests/test-demag/B_ref*.d
 subsampled copies of those goldens live in ``tests/golden/`` together with the script
 that extracted them.  Other terms (long field, thermal scaling, heat stencils, solvers)
 have no reference golden and are pinned by the reference's kernels rebuilt from source
-(``oracle/_ref``), run on the GPU box.
+(``oracle/_ref``), run on a B200 by the GPU tests.
 
 Conventions (reference ``engine/api.go:41-62``, ``common/index.go:68-113``): arrays are in
 the reference's *program order* -- shape ``(N0, N1, N2)`` with N2 the fastest index, which

@@ -1,7 +1,7 @@
 """Newell demag tensor (FP64 / extended precision) -- TEST INFRASTRUCTURE ONLY.
 
 The reference computes only Kernel_Arne (modules/kernel_magnetostatic.go:25-241); the Newell
-tensor is the option its north star names for large grids.  This is the oracle for the
+tensor is the closed-form alternative offered for large grids.  This is the oracle for the
 device version (hotspin_b200/csrc/hsb_newell.cuh):
 
 * exact: Newell, Williams and Dunlop, J. Geophys. Res. 98 (1993) 9551, the cell-averaged

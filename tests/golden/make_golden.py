@@ -14,7 +14,7 @@ against the FULL golden dumps, and writes
   (all three components, float32 as stored), so tests can compare without the reference;
 * ``golden_report.json`` -- the oracle-vs-golden errors measured on the full dumps.
 
-The GPU box has no reference checkout; tests use only these two files.
+Machines without a reference checkout run the tests on these two files alone.
 """
 import json
 import math
