@@ -8,19 +8,57 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 
+def pytest_addoption(parser):
+    parser.addoption("--emulate-cuda", action="store_true",
+                     help="run the gpu tests on the library's kernels built for the CPU emulation of CUDA "
+                          "(tests/emu); tests that need torch device memory or the reference's CUDA "
+                          "library are skipped")
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: longer CPU test")
+    config.addinivalue_line("markers", "torch_device: needs torch device memory (not emulated)")
+    if config.getoption("--emulate-cuda"):
+        use_emulated_library()
+
+
+def use_emulated_library():
+    """Bind tests/emu's build of the library (same C ABI and signatures) as the handle the
+    package's bindings use in this test process, in place of libhsb200.so."""
+    import ctypes
+    from tests.emu import build as emu_build
+    from hotspin_b200 import _lib
+    lib = ctypes.CDLL(emu_build.build())
+    for name, (res, args) in _lib._SIGS.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib._lib = lib
+    import oracle.replay
+    oracle.replay.available = lambda: False      # the reference's library needs a real GPU
 
 
 @pytest.fixture(scope="session")
-def cuda():
-    """torch with a CUDA device; the gpu-marked tests use it for device buffers only."""
+def cuda(request):
+    """torch with a CUDA device; the gpu-marked tests use it for device buffers only.  Under
+    --emulate-cuda there is no device: None (tests needing torch device memory skip)."""
+    if request.config.getoption("--emulate-cuda"):
+        return None
     import torch
     if not torch.cuda.is_available():
         pytest.fail("gpu test selected but no CUDA device is visible")
     torch.cuda.init()
     return torch
+
+
+def pytest_collection_modifyitems(config, items):
+    if not config.getoption("--emulate-cuda"):
+        return
+    skip = pytest.mark.skip(reason="needs torch device memory (not available under --emulate-cuda)")
+    for it in items:
+        if "torch_device" in it.keywords:
+            it.add_marker(skip)
 
 
 @pytest.fixture(scope="session")
