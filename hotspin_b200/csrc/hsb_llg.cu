@@ -914,9 +914,10 @@ __global__ void k_fixed_advance(HsbSolverDev* sd0, int nslot) {
     sd->step += 1;
     sd->cur = 1 - sd->cur;
     sd->attempts += 1;
-    if (sd->nonfinite) {
+    if (sd->nonfinite) {     // consumed, as the adaptive controllers consume it
         sd->status |= 1;
         sd->active = 0;
+        sd->nonfinite = 0u;
     }
     if (sd->step_stop >= 0 && sd->step >= sd->step_stop) sd->active = 0;
     if (sd->t_stop > 0.0 && sd->t_stop - sd->t <= 1e-6 * sd->dt) sd->active = 0;

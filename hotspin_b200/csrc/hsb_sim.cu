@@ -1343,8 +1343,9 @@ HSB_EXPORT int hsb_sim_set(hsb_sim_s* S, const char* name, const double* host, i
     k_d2f<<<hsb_grid_1d(count, 256), 256, 0, S->st>>>(S->stage_d, y + (long)first * S->n, count);
     HSB_CUDA_TRY(cudaGetLastError());
     S->initialized = false;
-    if (S->sd_host->status) {       // the flags described the state just replaced
+    if (S->sd_host->status || S->sd_host->nonfinite) {   // the flags described the state just replaced
         S->sd_host->status = 0;
+        S->sd_host->nonfinite = 0u;
         RC(set_sd_fields(S));
     }
     HSB_CUDA_TRY(cudaStreamSynchronize(S->st));
@@ -1423,8 +1424,9 @@ HSB_EXPORT int hsb_sim_set_device(hsb_sim_s* S, const char* name, const double* 
     k_d2f<<<hsb_grid_1d(count, 256), 256, 0, S->st>>>(dev, y + (long)first * S->n, count);
     HSB_CUDA_TRY(cudaGetLastError());
     S->initialized = false;
-    if (S->sd_host->status) {
+    if (S->sd_host->status || S->sd_host->nonfinite) {
         S->sd_host->status = 0;
+        S->sd_host->nonfinite = 0u;
         RC(set_sd_fields(S));
     }
     HSB_CUDA_TRY(cudaStreamSynchronize(S->st));

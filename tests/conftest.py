@@ -11,14 +11,12 @@ if ROOT not in sys.path:
 def pytest_addoption(parser):
     parser.addoption("--emulate-cuda", action="store_true",
                      help="run the gpu tests on the library's kernels built for the CPU emulation of CUDA "
-                          "(tests/emu); tests that need torch device memory or the reference's CUDA "
-                          "library are skipped")
+                          "(tests/emu); tests of the reference's CUDA library are skipped")
 
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: longer CPU test")
-    config.addinivalue_line("markers", "torch_device: needs torch device memory (not emulated)")
     if config.getoption("--emulate-cuda"):
         use_emulated_library()
 
@@ -37,28 +35,40 @@ def use_emulated_library():
     _lib._lib = lib
     import oracle.replay
     oracle.replay.available = lambda: False      # the reference's library needs a real GPU
+    _torch_device_memory_on_the_host()
+
+
+def _torch_device_memory_on_the_host():
+    """Under the emulation every device pointer is a host pointer: torch's "cuda" tensors of
+    the tests become CPU tensors (Tensor.cuda() returns the tensor, device="cuda" means the
+    CPU, synchronisation is a no-op)."""
+    import torch
+    torch.Tensor.cuda = lambda self, *a, **k: self
+    torch.cuda.synchronize = lambda *a, **k: None
+    for name in ("full", "zeros", "empty", "ones", "tensor", "randn", "rand", "arange", "zeros_like",
+                 "empty_like", "full_like", "ones_like"):
+        f = getattr(torch, name)
+
+        def on_host(*a, _f=f, **k):
+            if str(k.get("device", "")).startswith("cuda"):
+                k["device"] = "cpu"
+            return _f(*a, **k)
+        setattr(torch, name, on_host)
 
 
 @pytest.fixture(scope="session")
 def cuda(request):
     """torch with a CUDA device; the gpu-marked tests use it for device buffers only.  Under
-    --emulate-cuda there is no device: None (tests needing torch device memory skip)."""
-    if request.config.getoption("--emulate-cuda"):
-        return None
+    --emulate-cuda, torch with its "cuda" tensors in host memory."""
     import torch
+    if request.config.getoption("--emulate-cuda"):
+        return torch
     if not torch.cuda.is_available():
         pytest.fail("gpu test selected but no CUDA device is visible")
     torch.cuda.init()
     return torch
 
 
-def pytest_collection_modifyitems(config, items):
-    if not config.getoption("--emulate-cuda"):
-        return
-    skip = pytest.mark.skip(reason="needs torch device memory (not available under --emulate-cuda)")
-    for it in items:
-        if "torch_device" in it.keywords:
-            it.add_marker(skip)
 
 
 @pytest.fixture(scope="session")
