@@ -27,7 +27,9 @@ def use_emulated_library():
     import ctypes
     from tests.emu import build as emu_build
     from hotspin_b200 import _lib
-    lib = ctypes.CDLL(emu_build.build())
+    # HSBEMU_ASAN=1 (with the process started under LD_PRELOAD of libasan): the AddressSanitizer
+    # build, which reports any out-of-bounds access of a kernel to host memory
+    lib = ctypes.CDLL(emu_build.build(asan=os.environ.get("HSBEMU_ASAN") == "1"))
     for name, (res, args) in _lib._SIGS.items():
         f = getattr(lib, name)
         f.restype = res
@@ -40,10 +42,10 @@ def use_emulated_library():
 
 def _torch_device_memory_on_the_host():
     """Under the emulation every device pointer is a host pointer: torch's "cuda" tensors of
-    the tests become CPU tensors (Tensor.cuda() returns the tensor, device="cuda" means the
-    CPU, synchronisation is a no-op)."""
+    the tests become CPU tensors (Tensor.cuda() returns a copy, as the transfer does,
+    device="cuda" means the CPU, synchronisation is a no-op)."""
     import torch
-    torch.Tensor.cuda = lambda self, *a, **k: self
+    torch.Tensor.cuda = lambda self, *a, **k: self.clone()
     torch.cuda.synchronize = lambda *a, **k: None
     for name in ("full", "zeros", "empty", "ones", "tensor", "randn", "rand", "arange", "zeros_like",
                  "empty_like", "full_like", "ones_like"):

@@ -77,16 +77,26 @@ def rewrite(text):
     return "".join(out)
 
 
+def _newest_input():
+    files = [os.path.join(SRC, f) for f in os.listdir(SRC)] + [os.path.join(HERE, f) for f in os.listdir(HERE)]
+    files += [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
+    return max(os.path.getmtime(f) for f in files if os.path.isfile(f))
+
+
 def build(asan=False, verbose=False):
+    """Build (or reuse, when nothing it is made from changed) the emulation library."""
     os.makedirs(OUT, exist_ok=True)
     tag = "_asan" if asan else ""
-    gen = os.path.join(OUT, "src")
+    lib = os.path.join(OUT, "libhsb200_emu%s.so" % tag)
+    if os.path.exists(lib) and os.path.getmtime(lib) >= _newest_input():
+        return lib
+    gen = os.path.join(OUT, "src" + tag)
     os.makedirs(gen, exist_ok=True)
     flags = ["-std=c++17", "-O1", "-g", "-fPIC", "-fvisibility=hidden", "-Wno-unknown-pragmas",
              "-I" + HERE, "-I" + SRC, "-I" + os.path.join(ROOT, "include")]
     if asan:
         flags += ["-fsanitize=address", "-fno-omit-frame-pointer"]
-    objs = []
+    jobs = []
     for f in sorted(os.listdir(SRC)):
         if not f.endswith(".cu"):
             continue
@@ -95,24 +105,29 @@ def build(asan=False, verbose=False):
             text = rewrite(fh.read())
         with open(dst, "w") as fh:
             fh.write("#line 1 \"%s\"\n" % os.path.join(SRC, f) + text)
-        obj = os.path.join(OUT, f[:-3] + tag + ".o")
-        objs.append(obj)
-        cmd = ["g++"] + flags + ["-c", dst, "-o", obj]
+        jobs.append((f, dst, os.path.join(gen, f[:-3] + ".o")))
+    jobs.append(("emu_runtime.cpp", os.path.join(HERE, "emu_runtime.cpp"), os.path.join(gen, "emu_runtime.o")))
+
+    def compile_one(job):
+        name, src, obj = job
+        cmd = ["g++"] + flags + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         p = subprocess.run(cmd, capture_output=True, text=True)
-        if p.returncode:
-            raise RuntimeError("emulation build of %s failed:\n%s" % (f, p.stderr[-6000:]))
-    rt = os.path.join(OUT, "emu_runtime" + tag + ".o")
-    p = subprocess.run(["g++"] + flags + ["-c", os.path.join(HERE, "emu_runtime.cpp"), "-o", rt],
-                       capture_output=True, text=True)
-    if p.returncode:
-        raise RuntimeError("emulation runtime build failed:\n" + p.stderr[-6000:])
-    lib = os.path.join(OUT, "libhsb200_emu%s.so" % tag)
-    cmd = ["g++", "-shared", "-o", lib] + objs + [rt] + (["-fsanitize=address"] if asan else [])
+        return None if p.returncode == 0 else "emulation build of %s failed:\n%s" % (name, p.stderr[-6000:])
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 2)) as ex:
+        errs = [e for e in ex.map(compile_one, jobs) if e]
+    if errs:
+        raise RuntimeError("\n".join(errs))
+    objs = [j[2] for j in jobs[:-1]]
+    rt = jobs[-1][2]
+    tmp = lib + ".tmp%d" % os.getpid()
+    cmd = ["g++", "-shared", "-o", tmp] + objs + [rt] + (["-fsanitize=address"] if asan else [])
     p = subprocess.run(cmd, capture_output=True, text=True)
     if p.returncode:
         raise RuntimeError("emulation link failed:\n" + p.stderr[-6000:])
+    os.replace(tmp, lib)      # processes already holding the old file keep it
     return lib
 
 
