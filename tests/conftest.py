@@ -46,7 +46,22 @@ def _torch_device_memory_on_the_host():
     device="cuda" means the CPU, synchronisation is a no-op)."""
     import torch
     torch.Tensor.cuda = lambda self, *a, **k: self.clone()
+    to = torch.Tensor.to
+
+    def to_host(self, *a, **k):
+        a = tuple("cpu" if str(x).startswith("cuda") else x for x in a)
+        if str(k.get("device", "")).startswith("cuda"):
+            k["device"] = "cpu"
+        return to(self, *a, **k)
+    torch.Tensor.to = to_host
     torch.cuda.synchronize = lambda *a, **k: None
+
+    class _Stream:
+        cuda_stream = 0
+
+        def synchronize(self):
+            pass
+    torch.cuda.current_stream = lambda *a, **k: _Stream()
     for name in ("full", "zeros", "empty", "ones", "tensor", "randn", "rand", "arange", "zeros_like",
                  "empty_like", "full_like", "ones_like"):
         f = getattr(torch, name)

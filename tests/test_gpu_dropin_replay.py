@@ -20,7 +20,10 @@ from tests.gpu_util import rel_err
 
 pytestmark = pytest.mark.gpu
 
-HSB = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "hotspin_b200", "libhsb200.so")
+def _hsb():
+    """The product library this process binds (libhsb200.so)."""
+    from hotspin_b200 import _lib
+    return _lib.load()._name
 KW = dict(size=(2, 32, 64), cellsize=(4e-9, 4e-9, 4e-9), msat0T0=8e5,
           lex=float(np.sqrt(2 * 1.3e-11 / (F.MU0 * 8e5 ** 2))), gamma_ll=2.2e5, alpha=(0.02, 0.03, 0.04),
           ku=3e4, anis_u=(0.2, 0.3, 1.0), b_ext=(0.01, -0.02, 0.015), demag=True, llb=True, tc=630.0, spin_j=0.5,
@@ -39,7 +42,7 @@ def test_dropins_give_the_reference_rhs_under_the_go_sequence(cuda):
     y = _state(KW["size"])
     want = Model(Spec(**KW)).rhs(0.7e-13, y)
     outs = {}
-    libs = {"hsb": HSB}
+    libs = {"hsb": _hsb()}
     if replay.available():
         libs["ref"] = None
     for name, path in libs.items():
@@ -66,7 +69,7 @@ def test_dropins_step_like_the_reference_library(cuda, solver):
     m = rng.normal(size=(3,) + kw["size"])
     m /= np.sqrt((m * m).sum(0))
     res = {}
-    for name, path in (("ref", None), ("hsb", HSB)):
+    for name, path in (("ref", None), ("hsb", _hsb())):
         sim = replay.RefSim(kw, dt=1e-15, rtol=1e-4, lib_path=path)
         sim.set("m", m)
         cuda.cuda.synchronize()
