@@ -62,7 +62,32 @@ def _torch_device_memory_on_the_host():
         def synchronize(self):
             pass
     torch.cuda.current_stream = lambda *a, **k: _Stream()
-    for name in ("full", "zeros", "empty", "ones", "tensor", "randn", "rand", "arange", "zeros_like",
+    torch.cuda.ExternalStream = lambda *a, **k: _Stream()
+    torch.cuda.set_device = lambda *a, **k: None
+
+    class _Event:            # host clock: every emulated launch has finished when it returns
+        def __init__(self, enable_timing=False, **k):
+            self.t = None
+
+        def record(self, stream=None):
+            import time
+            self.t = time.perf_counter()
+
+        def synchronize(self):
+            pass
+
+        def elapsed_time(self, other):
+            return (other.t - self.t) * 1e3
+    torch.cuda.Event = _Event
+    empty = torch.empty
+
+    def empty_unpinned(*a, **k):
+        k.pop("pin_memory", None)            # page-locking needs the CUDA driver
+        if str(k.get("device", "")).startswith("cuda"):
+            k["device"] = "cpu"
+        return empty(*a, **k)
+    torch.empty = empty_unpinned
+    for name in ("full", "zeros", "ones", "tensor", "randn", "rand", "arange", "zeros_like",
                  "empty_like", "full_like", "ones_like"):
         f = getattr(torch, name)
 
