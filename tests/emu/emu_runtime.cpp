@@ -183,7 +183,9 @@ void run_grid(const hsbemu::Cfg& c, const std::function<void()>& body) {
     gridDim = c.grid;
     g_body = &body;
     g_in_kernel = true;
-    g_dyn.assign(c.smem + 16, 0xFF);   // uninitialised shared memory reads as NaN / all ones
+    // exactly the launch's dynamic shared memory (an AddressSanitizer build reports any access
+    // past it); uninitialised shared memory reads as NaN / all ones
+    g_dyn.assign(c.smem ? c.smem : 1, 0xFF);
     for (unsigned z = 0; z < c.grid.z; z++)
         for (unsigned y = 0; y < c.grid.y; y++)
             for (unsigned x = 0; x < c.grid.x; x++) {
