@@ -12,16 +12,20 @@ def pytest_addoption(parser):
     parser.addoption("--emulate-cuda", action="store_true",
                      help="run the gpu tests on the library's kernels built for the CPU emulation of CUDA "
                           "(tests/emu); tests of the reference's CUDA library are skipped")
+    parser.addoption("--replay-dropins", action="store_true",
+                     help="with --emulate-cuda: let the replay of hotspin's call sequence (oracle/replay.py) "
+                          "drive the product's FP64 drop-ins in place of the reference's library, to check "
+                          "the replay's solver logic and the tests built on it (not the reference's kernels)")
 
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: longer CPU test")
     if config.getoption("--emulate-cuda"):
-        use_emulated_library()
+        use_emulated_library(config.getoption("--replay-dropins"))
 
 
-def use_emulated_library():
+def use_emulated_library(replay_dropins=False):
     """Bind tests/emu's build of the library (same C ABI and signatures) as the handle the
     package's bindings use in this test process, in place of libhsb200.so."""
     import ctypes
@@ -36,7 +40,11 @@ def use_emulated_library():
         f.argtypes = args
     _lib._lib = lib
     import oracle.replay
-    oracle.replay.available = lambda: False      # the reference's library needs a real GPU
+    if replay_dropins:                           # the drop-ins stand in for the reference's library
+        oracle.replay.REF_LIB = lib._name
+        oracle.replay.available = lambda: True
+    else:
+        oracle.replay.available = lambda: False  # the reference's library needs a real GPU
     _torch_device_memory_on_the_host()
 
 

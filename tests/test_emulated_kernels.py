@@ -35,6 +35,28 @@ SELECTION = [
 ]
 
 
+REPLAY_SELECTION = [
+    "tests/test_gpu_reference_replay.py",
+    "tests/test_gpu_rk12.py::test_rk12_matches_reference_kernels",
+    "tests/test_gpu_implicit.py::test_am12_matches_reference_kernels",
+]
+
+
+def test_replay_logic_with_the_dropins_in_place_of_the_reference_library():
+    """oracle/replay.py's restatement of hotspin's solver loops (dp45, rk12, am12) and the
+    tests built on it, with the product's FP64 drop-ins standing in for the reference's library
+    (both export the same functions): a check of the replay's logic, not of the reference's
+    kernels, which need a GPU."""
+    if not shutil.which("g++"):
+        pytest.skip("g++ is not available")
+    cmd = [sys.executable, "-m", "pytest", "-m", "gpu", "--emulate-cuda", "--replay-dropins", "-q",
+           "-p", "no:cacheprovider"] + REPLAY_SELECTION
+    p = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=1800)
+    tail = "\n".join(p.stdout.splitlines()[-30:])
+    assert p.returncode == 0, tail
+    assert " passed" in tail and "failed" not in tail and "skipped" not in tail, tail
+
+
 def test_selected_gpu_tests_pass_on_the_emulated_kernels():
     if not shutil.which("g++"):
         pytest.skip("g++ is not available")
