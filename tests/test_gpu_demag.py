@@ -24,6 +24,7 @@ GEOMS = [
     ((32, 8, 16), (2e-9, 3e-9, 2e-9), (1, 0, 0)),                  # multipass, periodic z (L0 = N0 = 32)
     ((4, 8, 16), (1e-9, 2e-9, 3e-9), (2, 0, 3)),                   # periodic axes
     ((1, 1, 64), (2e-9, 2e-9, 2e-9), (0, 0, 0)),                   # a single row
+    ((1, 8, 2048), (2e-9, 2e-9, 2e-9), (0, 0, 0)),                 # x length 4096 (2048-point rows)
 ]
 
 
