@@ -42,6 +42,17 @@ REPLAY_SELECTION = [
 ]
 
 
+def _run(args):
+    """A child pytest on the emulated library (built here first, so its workers reuse it)."""
+    from tests.emu import build as emu_build
+    emu_build.build()
+    import importlib.util
+    workers = ["-n", str(min(4, os.cpu_count() or 1))] if importlib.util.find_spec("xdist") else []
+    cmd = [sys.executable, "-m", "pytest", "-m", "gpu", "--emulate-cuda", "-q", "-p", "no:cacheprovider"] + workers + args
+    p = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=1800)
+    return p, "\n".join(p.stdout.splitlines()[-30:])
+
+
 def test_replay_logic_with_the_dropins_in_place_of_the_reference_library():
     """oracle/replay.py's restatement of hotspin's solver loops (dp45, rk12, am12) and the
     tests built on it, with the product's FP64 drop-ins standing in for the reference's library
@@ -49,10 +60,7 @@ def test_replay_logic_with_the_dropins_in_place_of_the_reference_library():
     kernels, which need a GPU."""
     if not shutil.which("g++"):
         pytest.skip("g++ is not available")
-    cmd = [sys.executable, "-m", "pytest", "-m", "gpu", "--emulate-cuda", "--replay-dropins", "-q",
-           "-p", "no:cacheprovider"] + REPLAY_SELECTION
-    p = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=1800)
-    tail = "\n".join(p.stdout.splitlines()[-30:])
+    p, tail = _run(["--replay-dropins"] + REPLAY_SELECTION)
     assert p.returncode == 0, tail
     assert " passed" in tail and "failed" not in tail and "skipped" not in tail, tail
 
@@ -60,8 +68,6 @@ def test_replay_logic_with_the_dropins_in_place_of_the_reference_library():
 def test_selected_gpu_tests_pass_on_the_emulated_kernels():
     if not shutil.which("g++"):
         pytest.skip("g++ is not available")
-    cmd = [sys.executable, "-m", "pytest", "-m", "gpu", "--emulate-cuda", "-q", "-p", "no:cacheprovider"] + SELECTION
-    p = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=1800)
-    tail = "\n".join(p.stdout.splitlines()[-30:])
+    p, tail = _run(SELECTION)
     assert p.returncode == 0, tail
     assert " passed" in tail and "failed" not in tail, tail
