@@ -70,7 +70,10 @@ type HsbDesc struct {
 	MaxErr     [3]float64 // rk12 maxError / am12 maxAbsError / bdf-euler maxIterError (m, Te, Tl)
 	MaxRelErr  [3]float64 // am12 maxRelError
 	MaxIter    int
-	Newell     bool // the FP64 Newell tensor instead of Kernel_Arne
+	Newell     bool       // the FP64 Newell tensor instead of Kernel_Arne
+	MuPar      [3]float64 // llbar/damping/nonconservative/02/local (0: not loaded)
+	MuPerp     [3]float64 // llbar/damping/conservative/02/local (0: not loaded)
+	AlphaE     [3]float64 // llbar/damping/nonconservative/00/nonlocal (0: not loaded)
 }
 
 func b2i(b bool) C.int32_t {
@@ -91,6 +94,9 @@ func (d *HsbDesc) c() C.hsb_sim_desc {
 		c.b_ext[i] = C.double(d.BExt[i])
 		c.maxerr[i] = C.double(d.MaxErr[i])
 		c.maxrelerr[i] = C.double(d.MaxRelErr[i])
+		c.mu_par[i] = C.double(d.MuPar[i])
+		c.mu_perp[i] = C.double(d.MuPerp[i])
+		c.alpha_e[i] = C.double(d.AlphaE[i])
 	}
 	c.msat0T0, c.lex, c.gamma_ll, c.ku = C.double(d.Msat0T0), C.double(d.Lex), C.double(d.GammaLL), C.double(d.Ku)
 	c.demag, c.normalize, c.llb = b2i(d.Demag), b2i(d.Normalize), b2i(d.LLB)
