@@ -77,6 +77,15 @@ func (s *B200Solver) desc(e *Engine) gpu.HsbDesc {
 	if e.HasModule("llbar/damping/nonconservative/00/local") {
 		d.Alpha = vec3Or(e, "α", [3]float64{})
 	}
+	if e.HasModule("llbar/damping/nonconservative/02/local") {
+		d.MuPar = vec3Or(e, "μ∥", [3]float64{})
+	}
+	if e.HasModule("llbar/damping/conservative/02/local") {
+		d.MuPerp = vec3Or(e, "μ⊥", [3]float64{})
+	}
+	if e.HasModule("llbar/damping/nonconservative/00/nonlocal") {
+		d.AlphaE = vec3Or(e, "αₑ", [3]float64{})
+	}
 	if e.HasModule("anisotropy/uniaxial") {
 		d.Ku = scalarOr(e, "Ku", 0)
 		d.AnisU = vec3Or(e, "anisU", [3]float64{0, 0, 1})
