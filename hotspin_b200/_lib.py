@@ -97,6 +97,10 @@ _SIGS = {
     "hsb_demag_plan_info": (c_int, [c_vp, c_ip, c_ip, c_dp]),
     "hsb_demag_field": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_vp, c_vp]),
     "hsb_demag_kernel_copy": (c_int, [c_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_long]),
+    "hsb_fft_plan_create": (c_int, [c_ip, c_ip, c_vp, ctypes.POINTER(c_vp)]),
+    "hsb_fft_forward": (c_int, [c_vp, c_vp, c_vp]),
+    "hsb_fft_inverse": (c_int, [c_vp, c_vp, c_vp]),
+    "hsb_fft_plan_destroy": (c_int, [c_vp]),
 }
 
 

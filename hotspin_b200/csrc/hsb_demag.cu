@@ -26,6 +26,7 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -1852,5 +1853,212 @@ HSB_EXPORT int hsb_demag_kernel_copy(hsb_demag_plan P, float* host_out, long cou
         return HSB_ERR_INVALID;
     }
     HSB_CUDA_TRY(cudaMemcpy(host_out, P->kern, sizeof(float) * kcount, cudaMemcpyDeviceToHost));
+    return HSB_OK;
+}
+
+// ==================================================================================== FFT plan
+// FP64 3-D real FFT with the semantics of hotspin's FFTPlanX (gpu/fftplanX.go:76-104), the
+// FFTInterface a hotspin build selects with -fft (gpu/fftinterface.go:16-42):
+//   forward: the data block (N0, N1, N2) zero-padded to the logic size (L0, L1, L2), then the
+//            unnormalised real-to-complex transform, output (L0, L1, L2/2 + 1) complex
+//            (cuFFT's packed layout: L2 + 2 doubles per row);
+//   inverse: the unnormalised complex-to-real transform of such a spectrum, cropped to the
+//            data block.
+// Three passes of the column transform k_fft_cols (FP64 Stockham, any power of two up to
+// 4096) with a transpose between them, each axis contiguous in turn; the real axis runs as a
+// complex transform of the real row (forward) or of the row's Hermitian extension (inverse).
+#define RC_OK(x)                  \
+    do {                          \
+        const int rc_ = (x);      \
+        if (rc_ != HSB_OK) return rc_; \
+    } while (0)
+
+HSB_EXPORT int hsb_fft_plan_destroy(struct hsb_fft_plan_s* P);
+
+struct hsb_fft_plan_s {
+    int N[3], L[3], C2, twL;
+    double2* tw;
+    double2* s0;        // scratch, max(C2 L1 L0, N0 N1 L2) complex each
+    double2* s1;
+    cudaStream_t st;
+};
+
+// in (N0, N1, N2) real -> s (N0 N1 N2) complex
+__global__ void k_fftp_complexify(const double* __restrict__ in, double2* __restrict__ s, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        s[i] = make_double2(in[i], 0.0);
+}
+
+// out[(a * B + b) * C + c] = in[(a * C + c) * B + b]: swap the two fastest axes (B <-> C) of
+// `na` blocks
+__global__ void k_fftp_swap(const double2* __restrict__ in, double2* __restrict__ out, long na, int B, int C) {
+    const long n = na * B * C;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long r = i / C;
+        const int b = (int)(r % B);
+        const long a = r / B;
+        out[i] = in[(a * C + c) * B + b];
+    }
+}
+
+// out[(b * C + c) * A + a] = in[(a * B + b) * C + c]: the slowest axis (A) moved to the fastest
+__global__ void k_fftp_rotate(const double2* __restrict__ in, double2* __restrict__ out, int A, int B, int C) {
+    const long n = (long)A * B * C;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int a = (int)(i % A);
+        const long r = i / A;
+        const int c = (int)(r % C);
+        const int b = (int)(r / C);
+        out[i] = in[((long)a * B + b) * C + c];
+    }
+}
+
+// out[(a * B + b) * C + c] = in[(b * C + c) * A + a]: the fastest axis (A) moved to the slowest
+__global__ void k_fftp_unrotate(const double2* __restrict__ in, double2* __restrict__ out, int A, int B, int C) {
+    const long n = (long)A * B * C;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long r = i / C;
+        const int b = (int)(r % B);
+        const int a = (int)(r / B);
+        out[i] = in[((long)b * C + c) * A + a];
+    }
+}
+
+// rows of C2 spectrum values -> rows of L2 values, X[L2 - k] = conj(X[k]) for k >= C2
+__global__ void k_fftp_hermitian(const double2* __restrict__ in, double2* __restrict__ out, long nrow, int C2,
+                                 int L2) {
+    const long n = nrow * L2;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int k = (int)(i % L2);
+        const long r = i / L2;
+        double2 v;
+        if (k < C2) {
+            v = in[r * C2 + k];
+        } else {
+            const double2 w = in[r * C2 + (L2 - k)];
+            v = make_double2(w.x, -w.y);
+        }
+        out[i] = v;
+    }
+}
+
+__global__ void k_fftp_real(const double2* __restrict__ s, double* __restrict__ out, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        out[i] = s[i].x;
+}
+
+// One column pass: ncol columns of nin values (stride ldi) transformed at length L, the first
+// nout kept (stride ldo).  Sets the kernel's shared-memory limit before the launch: other plans
+// set the same function's limit for their own lengths.
+template <int DIR>
+static int fftp_cols(hsb_fft_plan_s* P, const double2* in, int ldi, int nin, double2* out, int ldo, int nout,
+                     int L, long ncol) {
+    const int TB = pick_tile(L, sizeof(double2), SMEM_TILE_BUDGET, 16);
+    const int smem = 2 * TB * fpad_len(L) * (int)sizeof(double2);
+    HSB_CUDA_TRY(cudaFuncSetAttribute(k_fft_cols<double, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_fft_cols<double, DIR><<<hsb_div_up(ncol, TB), XTHREADS, smem, P->st>>>(in, ldi, nin, out, ldo, nout, L, ncol,
+                                                                            P->tw, P->twL, TB, nullptr);
+    HSB_CUDA_TRY(cudaGetLastError());
+    return HSB_OK;
+}
+
+HSB_EXPORT int hsb_fft_plan_create(const int* data_size, const int* logic_size, void* stream, hsb_fft_plan_s** out) {
+    if (!data_size || !logic_size || !out) {
+        hsb_set_error("hsb_fft_plan_create: null argument");
+        return HSB_ERR_INVALID;
+    }
+    *out = nullptr;
+    for (int a = 0; a < 3; a++) {
+        const int n = data_size[a], l = logic_size[a];
+        if (n < 1 || l < n || !is_pow2(l) || l > 4096) {
+            hsb_set_error("hsb_fft_plan_create: axis %d: data size %d, logic size %d (the logic size must be a power "
+                          "of two in [data size, 4096])", a, n, l);
+            return HSB_ERR_UNSUPPORTED;
+        }
+    }
+    if (logic_size[2] < 2) {
+        hsb_set_error("hsb_fft_plan_create: the real (last) axis needs a logic size of at least 2");
+        return HSB_ERR_UNSUPPORTED;
+    }
+    hsb_fft_plan_s* P = new hsb_fft_plan_s();
+    for (int a = 0; a < 3; a++) {
+        P->N[a] = data_size[a];
+        P->L[a] = logic_size[a];
+    }
+    P->C2 = P->L[2] / 2 + 1;
+    P->twL = std::max(P->L[0], std::max(P->L[1], P->L[2]));
+    P->st = (cudaStream_t)stream;
+    const long nscr = std::max((long)P->C2 * P->L[1] * P->L[0], (long)P->N[0] * P->N[1] * P->L[2]);
+    int rc = make_twiddles<double2>(P->twL, &P->tw);
+    if (rc == HSB_OK && (cudaMalloc(&P->s0, sizeof(double2) * nscr) != cudaSuccess ||
+                         cudaMalloc(&P->s1, sizeof(double2) * nscr) != cudaSuccess)) {
+        hsb_set_error("hsb_fft_plan_create: cudaMalloc of %ld complex scratch values failed", 2 * nscr);
+        rc = HSB_ERR_NOMEM;
+    }
+    if (rc != HSB_OK) {
+        hsb_fft_plan_destroy(P);
+        return rc;
+    }
+    *out = P;
+    return HSB_OK;
+}
+
+HSB_EXPORT int hsb_fft_plan_destroy(hsb_fft_plan_s* P) {
+    if (!P) return HSB_OK;
+    cudaFree(P->tw);
+    cudaFree(P->s0);
+    cudaFree(P->s1);
+    delete P;
+    return HSB_OK;
+}
+
+HSB_EXPORT int hsb_fft_forward(hsb_fft_plan_s* P, const double* in, double* out) {
+    if (!P || !in || !out) {
+        hsb_set_error("hsb_fft_forward: null argument");
+        return HSB_ERR_INVALID;
+    }
+    const int N0 = P->N[0], N1 = P->N[1], N2 = P->N[2], L0 = P->L[0], L1 = P->L[1], L2 = P->L[2], C2 = P->C2;
+    const long nd = (long)N0 * N1 * N2;
+    k_fftp_complexify<<<hsb_grid_1d(nd, 256), 256, 0, P->st>>>(in, P->s0, nd);
+    // x: rows (z, y) of N2 values, zero-padded to L2, C2 kept -> s1 (N0, N1, C2)
+    RC_OK(fftp_cols<-1>(P, P->s0, N2, N2, P->s1, C2, C2, L2, (long)N0 * N1));
+    // (N0, N1, C2) -> (N0, C2, N1); y: N1 values zero-padded to L1 -> s1 (N0, C2, L1)
+    k_fftp_swap<<<hsb_grid_1d((long)N0 * N1 * C2, 256), 256, 0, P->st>>>(P->s1, P->s0, N0, C2, N1);
+    RC_OK(fftp_cols<-1>(P, P->s0, N1, N1, P->s1, L1, L1, L1, (long)N0 * C2));
+    // (N0, C2, L1) -> (N0, L1, C2) -> (L1, C2, N0); z: N0 values zero-padded to L0 -> s0 (L1, C2, L0)
+    k_fftp_swap<<<hsb_grid_1d((long)N0 * C2 * L1, 256), 256, 0, P->st>>>(P->s1, P->s0, N0, L1, C2);
+    k_fftp_rotate<<<hsb_grid_1d((long)N0 * L1 * C2, 256), 256, 0, P->st>>>(P->s0, P->s1, N0, L1, C2);
+    RC_OK(fftp_cols<-1>(P, P->s1, N0, N0, P->s0, L0, L0, L0, (long)L1 * C2));
+    // (L1, C2, L0) -> (L0, L1, C2): cuFFT's packed R2C layout
+    k_fftp_unrotate<<<hsb_grid_1d((long)L0 * L1 * C2, 256), 256, 0, P->st>>>(P->s0, (double2*)out, L0, L1, C2);
+    HSB_CUDA_TRY(cudaGetLastError());
+    HSB_CUDA_TRY(cudaStreamSynchronize(P->st));
+    return HSB_OK;
+}
+
+HSB_EXPORT int hsb_fft_inverse(hsb_fft_plan_s* P, const double* in, double* out) {
+    if (!P || !in || !out) {
+        hsb_set_error("hsb_fft_inverse: null argument");
+        return HSB_ERR_INVALID;
+    }
+    const int N0 = P->N[0], N1 = P->N[1], N2 = P->N[2], L0 = P->L[0], L1 = P->L[1], L2 = P->L[2], C2 = P->C2;
+    // (L0, L1, C2) -> (L1, C2, L0); z: all L0 values, the first N0 kept -> s1 (L1, C2, N0)
+    k_fftp_rotate<<<hsb_grid_1d((long)L0 * L1 * C2, 256), 256, 0, P->st>>>((const double2*)in, P->s0, L0, L1, C2);
+    RC_OK(fftp_cols<+1>(P, P->s0, L0, L0, P->s1, N0, N0, L0, (long)L1 * C2));
+    // (L1, C2, N0) -> (N0, L1, C2)
+    k_fftp_unrotate<<<hsb_grid_1d((long)N0 * L1 * C2, 256), 256, 0, P->st>>>(P->s1, P->s0, N0, L1, C2);
+    // s0 (N0, L1, C2) -> (N0, C2, L1); y: all L1 values, the first N1 kept -> s1 (N0, C2, N1)
+    k_fftp_swap<<<hsb_grid_1d((long)N0 * L1 * C2, 256), 256, 0, P->st>>>(P->s0, P->s1, N0, C2, L1);
+    RC_OK(fftp_cols<+1>(P, P->s1, L1, L1, P->s0, N1, N1, L1, (long)N0 * C2));
+    // (N0, C2, N1) -> (N0, N1, C2); Hermitian rows of L2; x: complex inverse, N2 kept, real part
+    k_fftp_swap<<<hsb_grid_1d((long)N0 * N1 * C2, 256), 256, 0, P->st>>>(P->s0, P->s1, N0, N1, C2);
+    k_fftp_hermitian<<<hsb_grid_1d((long)N0 * N1 * L2, 256), 256, 0, P->st>>>(P->s1, P->s0, (long)N0 * N1, C2, L2);
+    RC_OK(fftp_cols<+1>(P, P->s0, L2, L2, P->s1, N2, N2, L2, (long)N0 * N1));
+    const long nd = (long)N0 * N1 * N2;
+    k_fftp_real<<<hsb_grid_1d(nd, 256), 256, 0, P->st>>>(P->s1, out, nd);
+    HSB_CUDA_TRY(cudaGetLastError());
+    HSB_CUDA_TRY(cudaStreamSynchronize(P->st));
     return HSB_OK;
 }

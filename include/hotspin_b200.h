@@ -285,7 +285,9 @@ int hsb_batch_release(hsb_batch b, int32_t slot);
 /* Demag convolution on caller-owned FP32 device arrays (SoA [3][N0][N1][N2]):
  * H (A/m) = Ms0 * K (*) (m * mask); mask may be NULL.  The plan builds the Kernel_Arne
  * tensor (kernel_magnetostatic.go:25-241) on the GPU in FP64 (accuracy as the reference,
- * normally 6).  Padded sizes must be powers of two, a2 padded >= 2. */
+ * normally 6).  A periodic axis must be a power of two; an open axis of any size is padded to
+ * twice its size or, when that is not a power of two, embedded in a grid of next_pow2(N) cells
+ * (vacuum beyond the N cells), which gives the same field. */
 typedef struct hsb_demag_plan_s* hsb_demag_plan;
 int hsb_demag_plan_create(const int* size, const double* cellsize, const int* pbc, int accuracy,
                           void* stream, hsb_demag_plan* out);
@@ -307,6 +309,22 @@ int hsb_demag_profile(hsb_demag_plan plan, const float* m, const float* mask, do
                       void* stream, int reps, double* ms3);
 /* Folded FP32 kernel spectrum, layout [kx][k1][k0][6] (XX YY ZZ YZ XZ XY). */
 int hsb_demag_kernel_copy(hsb_demag_plan plan, float* host_out, long count);
+
+/* FP64 3-D real FFT plan with the semantics of hotspin's FFTPlanX (gpu/fftplanX.go:76-104), the
+ * implementation behind hotspin's FFTInterface registry (fftPlans, gpu/fftinterface.go:16-42):
+ *   hsb_fft_forward: the data block (N0, N1, N2) zero-padded to the logic size (L0, L1, L2),
+ *     then the unnormalised real-to-complex transform into (L0, L1, L2/2 + 1) complex values
+ *     (L2 + 2 doubles per row: cuFFT's packed layout);
+ *   hsb_fft_inverse: the unnormalised complex-to-real transform of such a spectrum, cropped to
+ *     the data block (the spectrum itself is left unchanged).
+ * Device pointers, program order.  Each call runs on the plan's stream and synchronises it, as
+ * FFTPlanX does.  Logic sizes: powers of two, at least the data size, at most 4096, the last
+ * at least 2. */
+typedef struct hsb_fft_plan_s* hsb_fft_plan;
+int hsb_fft_plan_create(const int* data_size, const int* logic_size, void* stream, hsb_fft_plan* out);
+int hsb_fft_forward(hsb_fft_plan plan, const double* in, double* out);
+int hsb_fft_inverse(hsb_fft_plan plan, const double* in, double* out);
+int hsb_fft_plan_destroy(hsb_fft_plan plan);
 
 #ifdef __cplusplus
 }

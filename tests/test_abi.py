@@ -32,7 +32,7 @@ def test_python_signatures_match_the_header_prototypes():
     src = "".join(open(os.path.join(root, "include", f)).read() for f in sorted(os.listdir(os.path.join(root, "include"))))
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     src = re.sub(r"//[^\n]*", "", src)
-    handles = ("hsb_sim", "hsb_batch", "hsb_demag_plan")
+    handles = ("hsb_sim", "hsb_batch", "hsb_demag_plan", "hsb_fft_plan")
 
     def ctype_of(decl):
         d = re.sub(r"\bconst\b", "", decl).strip()

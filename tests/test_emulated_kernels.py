@@ -3,8 +3,8 @@
 A selection of the gpu tests -- the ones whose code paths have the most host logic around the
 kernels: the reference's solvers (rk12, am12, bdf-euler), the optional LLBar terms, the Newell
 tensor, grids embedded in a power-of-two demag grid, failure handling (non-finite states,
-unreachable tolerances, checkpoints, batch slot release) and the FP64 drop-ins under the Go
-call sequence -- runs in a child pytest with --emulate-cuda, where the library is the product's
+unreachable tolerances, checkpoints, batch slot release), the FP64 FFT plan and the FP64 drop-ins
+under the Go call sequence -- runs in a child pytest with --emulate-cuda, where the library is the product's
 CUDA source built as host C++ against the emulated runtime (every CUDA thread a fiber, block and
 warp barriers, graph capture and replay).  The full gpu suite runs the same way with
 ``python -m pytest tests -m gpu --emulate-cuda`` (tens of minutes).
@@ -32,6 +32,7 @@ SELECTION = [
     "tests/test_gpu_sim.py::test_nonlocal_relaxation_term",
     "tests/test_gpu_demag.py::test_demag_on_grids_that_do_not_pad_to_powers_of_two",
     "tests/test_gpu_dropin_replay.py::test_dropins_give_the_reference_rhs_under_the_go_sequence",
+    "tests/test_gpu_xfftplan.py",
 ]
 
 
