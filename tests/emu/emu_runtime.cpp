@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <vector>
 
@@ -78,6 +79,17 @@ int g_cur = -1, g_n = 0, g_done = 0, g_bar = 0;
 bool g_in_kernel = false;
 const std::function<void()>* g_body = nullptr;
 std::vector<unsigned char> g_dyn;
+
+// HSBEMU_ORDER=reverse: blocks run last to first and the threads of a block are resumed from
+// the highest index down, so a kernel that depends on an order the GPU does not promise (a
+// missing barrier, a block reading another block's output) gives different results.
+bool reverse_order() {
+    static const bool rev = [] {
+        const char* s = getenv("HSBEMU_ORDER");
+        return s && strcmp(s, "reverse") == 0;
+    }();
+    return rev;
+}
 
 char* stack_at(int i) {
     while ((int)g_stacks.size() <= i) {
@@ -159,9 +171,11 @@ void run_block(int n) {
         f.ctx.uc_link = &g_sched;
         makecontext(&f.ctx, trampoline, 0);
     }
+    const bool rev = reverse_order();
     while (g_done < n) {
         bool ran = false;
-        for (int i = 0; i < n; i++) {
+        for (int j = 0; j < n; j++) {
+            const int i = rev ? n - 1 - j : j;
             if (g_fib[i].state != READY) continue;
             g_cur = i;
             threadIdx = g_fib[i].tid;
@@ -186,9 +200,12 @@ void run_grid(const hsbemu::Cfg& c, const std::function<void()>& body) {
     // exactly the launch's dynamic shared memory (an AddressSanitizer build reports any access
     // past it); uninitialised shared memory reads as NaN / all ones
     g_dyn.assign(c.smem ? c.smem : 1, 0xFF);
-    for (unsigned z = 0; z < c.grid.z; z++)
-        for (unsigned y = 0; y < c.grid.y; y++)
-            for (unsigned x = 0; x < c.grid.x; x++) {
+    const bool rev = reverse_order();
+    for (unsigned zz = 0; zz < c.grid.z; zz++)
+        for (unsigned yy = 0; yy < c.grid.y; yy++)
+            for (unsigned xx = 0; xx < c.grid.x; xx++) {
+                const unsigned x = rev ? c.grid.x - 1 - xx : xx, y = rev ? c.grid.y - 1 - yy : yy,
+                               z = rev ? c.grid.z - 1 - zz : zz;
                 blockIdx = uint3{x, y, z};
                 memset(g_dyn.data(), 0xFF, g_dyn.size());
                 run_block(n);
