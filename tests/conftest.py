@@ -12,6 +12,11 @@ def pytest_addoption(parser):
     parser.addoption("--emulate-cuda", action="store_true",
                      help="run the gpu tests on the library's kernels built for the CPU emulation of CUDA "
                           "(tests/emu); tests of the reference's CUDA library are skipped")
+    parser.addoption("--emulate-reference", action="store_true",
+                     help="with --emulate-cuda: build the reference's own kernel library for the emulation "
+                          "(oracle/ref_emu.py) and let the replay of hotspin's call sequence drive it; runs "
+                          "every kernel in reverse scheduling order, which the reference's warp-synchronous "
+                          "max reductions need there")
     parser.addoption("--replay-dropins", action="store_true",
                      help="with --emulate-cuda: let the replay of hotspin's call sequence (oracle/replay.py) "
                           "drive the product's FP64 drop-ins in place of the reference's library, to check "
@@ -22,7 +27,15 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: longer CPU test")
     if config.getoption("--emulate-cuda"):
+        if config.getoption("--emulate-reference"):
+            os.environ["HSBEMU_ORDER"] = "reverse"      # read by both emulated runtimes at first use
         use_emulated_library(config.getoption("--replay-dropins"))
+        if config.getoption("--emulate-reference"):
+            import oracle.replay
+            from oracle import ref_emu
+            if ref_emu.available():
+                oracle.replay.REF_LIB = ref_emu.build()
+                oracle.replay.available = lambda: True
 
 
 def use_emulated_library(replay_dropins=False):

@@ -32,6 +32,8 @@ def _callee_start(s, i):
     """Start of the callee expression that ends just before position i (identifiers joined by
     ->, . or ::, each optionally followed by template arguments)."""
     j = i - 1
+    while j >= 0 and s[j] in " \t":        # `kernel <<<...>>>`
+        j -= 1
     while True:
         if j >= 0 and s[j] == ">":          # template arguments
             depth = 0

@@ -29,6 +29,7 @@
 #define __grid_constant__
 #define __shared__ static
 #define __align__(n) __attribute__((aligned(n)))
+#define __export__
 
 // ------------------------------------------------------------------ vector types
 struct dim3 {
@@ -47,6 +48,14 @@ struct __attribute__((aligned(16))) float4 {
 struct __attribute__((aligned(16))) double2 {
     double x, y;
 };
+struct double3 {
+    double x, y, z;
+};
+struct int3 {
+    int x, y, z;
+};
+inline double3 make_double3(double x, double y, double z) { return double3{x, y, z}; }
+inline int3 make_int3(int x, int y, int z) { return int3{x, y, z}; }
 inline float2 make_float2(float x, float y) { return float2{x, y}; }
 inline float4 make_float4(float x, float y, float z, float w) { return float4{x, y, z, w}; }
 inline double2 make_double2(double x, double y) { return double2{x, y}; }
@@ -126,6 +135,16 @@ cudaError_t cudaEventElapsedTime(float* ms, cudaEvent_t a, cudaEvent_t b);
 cudaError_t cudaGetLastError();
 const char* cudaGetErrorString(cudaError_t e);
 cudaError_t cudaGetDevice(int* dev);
+struct cudaDeviceProp {
+    char name[256];
+    size_t totalGlobalMem, sharedMemPerBlock, totalConstMem, textureAlignment, memPitch;
+    int regsPerBlock, warpSize, maxThreadsPerBlock, maxThreadsDim[3], maxGridSize[3], major, minor, clockRate,
+        multiProcessorCount, kernelExecTimeoutEnabled, computeMode, deviceOverlap, concurrentKernels, integrated,
+        canMapHostMemory;
+};
+cudaError_t cudaGetDeviceProperties(cudaDeviceProp* p, int dev);
+cudaError_t cudaThreadSynchronize();
+cudaError_t cudaDeviceSynchronize();
 cudaError_t cudaDeviceGetAttribute(int* v, cudaDeviceAttr a, int dev);
 template <class T>
 inline cudaError_t cudaGetSymbolAddress(void** p, const T& symbol) {
@@ -210,6 +229,7 @@ inline double __longlong_as_double(long long u) {
     return d;
 }
 inline float __fdividef(float a, float b) { return a / b; }
+inline float __expf(float x) { return expf(x); }
 inline unsigned __umulhi(unsigned a, unsigned b) { return (unsigned)(((unsigned long long)a * b) >> 32); }
 inline int __ffs(int x) { return __builtin_ffs(x); }
 inline float rsqrtf(float x) { return 1.0f / sqrtf(x); }

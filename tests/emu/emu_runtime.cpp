@@ -221,7 +221,10 @@ void __syncthreads() {
     if (!g_in_kernel || g_cur < 0) return;
     g_bar++;
     if (g_bar == g_n - g_done) {
+        // the last thread to arrive also goes back to the scheduler, so that after every
+        // barrier the block's threads resume in the scheduling order (forward or reverse)
         release_block();
+        yield_to_scheduler();
         return;
     }
     g_fib[g_cur].state = WAIT_BLOCK;
@@ -240,6 +243,7 @@ static uint64_t warp_op(unsigned mask, uint64_t v, int xor_mask, bool shuffle) {
     const unsigned part = mask & live_lanes(w);
     if ((W.arrived & part) == part) {
         release_warp(w);
+        yield_to_scheduler();     // as at a block barrier: resume in the scheduling order
     } else {
         f.state = WAIT_WARP;
         yield_to_scheduler();
@@ -417,3 +421,26 @@ cudaError_t cudaDeviceGetAttribute(int* v, cudaDeviceAttr a, int) {
     }
     return cudaErrorInvalidValue;
 }
+cudaError_t cudaGetDeviceProperties(cudaDeviceProp* p, int) {
+    memset(p, 0, sizeof(*p));
+    strcpy(p->name, "CPU emulation of CUDA");
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    p->totalGlobalMem = (size_t)64 << 30;
+    p->sharedMemPerBlock = 48 * 1024;
+    p->totalConstMem = 64 * 1024;
+    p->textureAlignment = 512;
+    p->regsPerBlock = 65536;
+    p->warpSize = 32;
+    p->maxThreadsPerBlock = 1024;
+    p->maxThreadsDim[0] = p->maxThreadsDim[1] = 1024;
+    p->maxThreadsDim[2] = 64;
+    p->maxGridSize[0] = 2147483647;
+    p->maxGridSize[1] = p->maxGridSize[2] = 65535;
+    p->major = 10;
+    p->clockRate = 1000000;
+    p->multiProcessorCount = sms;
+    return cudaSuccess;
+}
+cudaError_t cudaThreadSynchronize() { return cudaSuccess; }
+cudaError_t cudaDeviceSynchronize() { return cudaSuccess; }

@@ -31,7 +31,6 @@ SELECTION = [
     "tests/test_gpu_sim.py::test_second_order_relaxation_terms",
     "tests/test_gpu_sim.py::test_nonlocal_relaxation_term",
     "tests/test_gpu_demag.py::test_demag_on_grids_that_do_not_pad_to_powers_of_two",
-    "tests/test_gpu_dropin_replay.py::test_dropins_give_the_reference_rhs_under_the_go_sequence",
     "tests/test_gpu_xfftplan.py",
 ]
 
@@ -40,6 +39,7 @@ REPLAY_SELECTION = [
     "tests/test_gpu_reference_replay.py",
     "tests/test_gpu_rk12.py::test_rk12_matches_reference_kernels",
     "tests/test_gpu_implicit.py::test_am12_matches_reference_kernels",
+    "tests/test_gpu_dropin_replay.py",
 ]
 
 
@@ -54,14 +54,21 @@ def _run(args):
     return p, "\n".join(p.stdout.splitlines()[-30:])
 
 
-def test_replay_logic_with_the_dropins_in_place_of_the_reference_library():
-    """oracle/replay.py's restatement of hotspin's solver loops (dp45, rk12, am12) and the
-    tests built on it, with the product's FP64 drop-ins standing in for the reference's library
-    (both export the same functions): a check of the replay's logic, not of the reference's
-    kernels, which need a GPU."""
+def test_replay_tests_on_the_reference_kernels():
+    """oracle/replay.py's restatement of hotspin's solver loops (dp45, rk12, am12) on the
+    reference's own kernels built for the emulation (oracle/ref_emu.py), and the tests that
+    compare the product with them: the product's FP32 handle, its FP64 drop-ins under the Go call
+    sequence and the FP64 oracle against the reference's kernels.  Without the reference
+    checkout, the product's drop-ins stand in for the reference's library (a check of the
+    replay's logic only)."""
     if not shutil.which("g++"):
         pytest.skip("g++ is not available")
-    p, tail = _run(["--replay-dropins"] + REPLAY_SELECTION)
+    from oracle import ref_emu
+    if ref_emu.available():
+        ref_emu.build()              # here, so the child's workers reuse it
+        p, tail = _run(["--emulate-reference"] + REPLAY_SELECTION)
+    else:
+        p, tail = _run(["--replay-dropins"] + REPLAY_SELECTION[:3])
     assert p.returncode == 0, tail
     assert " passed" in tail and "failed" not in tail and "skipped" not in tail, tail
 
