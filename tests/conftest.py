@@ -26,6 +26,7 @@ def pytest_addoption(parser):
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: longer CPU test")
+    config.addinivalue_line("markers", "late: long-horizon or statistical gpu test, run after the others")
     if config.getoption("--emulate-cuda"):
         if config.getoption("--emulate-reference"):
             os.environ["HSBEMU_ORDER"] = "reverse"      # read by both emulated runtimes at first use
@@ -156,3 +157,14 @@ def host_rules(tmp_path_factory):
            "-o", out]
     subprocess.run(cmd, check=True, capture_output=True)
     return ctypes.CDLL(out)
+
+
+def pytest_collection_modifyitems(config, items):
+    """Long-horizon and statistical gpu tests (marked `late`) run after the others, so that a
+    run stopping at its first failure has checked everything else; tests/test_zz_no_alloc.py
+    stays last."""
+    def rank(it):
+        if os.path.basename(str(it.fspath)) == "test_zz_no_alloc.py":
+            return 2
+        return 1 if it.get_closest_marker("late") else 0
+    items[:] = sorted(items, key=rank)     # stable: the file order holds within each group

@@ -23,7 +23,7 @@ from hotspin_b200.sim import Simulation
 from oracle import replay
 from oracle.model import Model, Spec
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.late]
 
 MU0 = 4e-7 * math.pi
 

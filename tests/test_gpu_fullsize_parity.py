@@ -21,7 +21,7 @@ from oracle import fields as F
 from oracle import replay
 from tests.gpu_util import rel_err
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.late]
 
 MU0 = 4e-7 * math.pi
 

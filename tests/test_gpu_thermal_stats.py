@@ -88,6 +88,7 @@ def test_dp45_same_stream_ensemble_matches_oracle_3sigma(cuda, T):
         assert abs(a[1] - b[1]) < 3 * np.hypot(a[3], b[3]), (c, a, b)
 
 
+@pytest.mark.late
 @pytest.mark.parametrize("T", [150.0, 300.0, 600.0])
 def test_equilibrium_is_boltzmann_3sigma(cuda, T):
     size, B, dt = (4, 128, 128), 0.383, 2e-14
