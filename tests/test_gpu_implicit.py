@@ -143,5 +143,5 @@ def test_am12_matches_reference_kernels(cuda):
         st = sim.status()
         m = sim.get("m")
     assert st["t"] == pytest.approx(t_end, rel=1e-9)
-    assert abs(st["steps"] - ref.steps) <= 1
+    assert abs(st["steps"] - ref.steps) <= max(1, ref.steps // 50)
     assert float(np.abs(m - ref.get("m")).max()) < 1e-5

@@ -62,7 +62,7 @@ def test_rk12_matches_oracle(cuda, case):
     print("\n[rk12] %s steps %d (oracle %d) rejects %d (oracle %d) max|dm| %.2e"
           % (case, st["steps"], it.step_count, st["rejects"], it.bad_steps, dm))
     assert st["t"] == pytest.approx(t_end, rel=1e-9)
-    assert abs(st["steps"] - it.step_count) <= 1
+    assert abs(st["steps"] - it.step_count) <= max(1, it.step_count // 50)
     assert dm < 1e-5
     if T is not None:
         assert rel_err(T, it.y["Te"]) < 1e-5
