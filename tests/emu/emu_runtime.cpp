@@ -11,6 +11,7 @@
 #include <sys/mman.h>
 #include <ucontext.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -81,14 +82,36 @@ const std::function<void()>* g_body = nullptr;
 std::vector<unsigned char> g_dyn;
 
 // HSBEMU_ORDER=reverse: blocks run last to first and the threads of a block are resumed from
-// the highest index down, so a kernel that depends on an order the GPU does not promise (a
-// missing barrier, a block reading another block's output) gives different results.
-bool reverse_order() {
-    static const bool rev = [] {
+// the highest index down; HSBEMU_ORDER=shuffle: both in a random order (HSBEMU_SEED), drawn
+// anew for every launch and every pass over a block's threads.  A kernel that depends on an
+// order the GPU does not promise (a missing barrier, a block reading another block's output)
+// then gives different results.
+enum { ORDER_FORWARD = 0, ORDER_REVERSE = 1, ORDER_SHUFFLE = 2 };
+int schedule_order() {
+    static const int o = [] {
         const char* s = getenv("HSBEMU_ORDER");
-        return s && strcmp(s, "reverse") == 0;
+        if (s && strcmp(s, "reverse") == 0) return (int)ORDER_REVERSE;
+        if (s && strcmp(s, "shuffle") == 0) return (int)ORDER_SHUFFLE;
+        return (int)ORDER_FORWARD;
     }();
-    return rev;
+    return o;
+}
+bool reverse_order() { return schedule_order() == ORDER_REVERSE; }
+
+uint64_t next_random() {      // xorshift64*
+    static uint64_t x = [] {
+        const char* s = getenv("HSBEMU_SEED");
+        const uint64_t v = s ? strtoull(s, nullptr, 10) : 1;
+        return v ? v : 1;
+    }();
+    x ^= x >> 12;
+    x ^= x << 25;
+    x ^= x >> 27;
+    return x * 0x2545F4914F6CDD1DULL;
+}
+
+void shuffle(std::vector<int>& v) {
+    for (size_t i = v.size(); i > 1; i--) std::swap(v[i - 1], v[next_random() % i]);
 }
 
 char* stack_at(int i) {
@@ -171,11 +194,14 @@ void run_block(int n) {
         f.ctx.uc_link = &g_sched;
         makecontext(&f.ctx, trampoline, 0);
     }
-    const bool rev = reverse_order();
+    const bool rev = reverse_order(), shuf = schedule_order() == ORDER_SHUFFLE;
+    std::vector<int> perm(n);
+    for (int j = 0; j < n; j++) perm[j] = rev ? n - 1 - j : j;
     while (g_done < n) {
         bool ran = false;
+        if (shuf) shuffle(perm);
         for (int j = 0; j < n; j++) {
-            const int i = rev ? n - 1 - j : j;
+            const int i = perm[j];
             if (g_fib[i].state != READY) continue;
             g_cur = i;
             threadIdx = g_fib[i].tid;
@@ -200,16 +226,17 @@ void run_grid(const hsbemu::Cfg& c, const std::function<void()>& body) {
     // exactly the launch's dynamic shared memory (an AddressSanitizer build reports any access
     // past it); uninitialised shared memory reads as NaN / all ones
     g_dyn.assign(c.smem ? c.smem : 1, 0xFF);
-    const bool rev = reverse_order();
-    for (unsigned zz = 0; zz < c.grid.z; zz++)
-        for (unsigned yy = 0; yy < c.grid.y; yy++)
-            for (unsigned xx = 0; xx < c.grid.x; xx++) {
-                const unsigned x = rev ? c.grid.x - 1 - xx : xx, y = rev ? c.grid.y - 1 - yy : yy,
-                               z = rev ? c.grid.z - 1 - zz : zz;
-                blockIdx = uint3{x, y, z};
-                memset(g_dyn.data(), 0xFF, g_dyn.size());
-                run_block(n);
-            }
+    const long nb = (long)c.grid.x * c.grid.y * c.grid.z;
+    std::vector<int> order(nb);
+    for (long b = 0; b < nb; b++) order[b] = (int)(reverse_order() ? nb - 1 - b : b);
+    if (schedule_order() == ORDER_SHUFFLE) shuffle(order);
+    for (long q = 0; q < nb; q++) {
+        const long b = order[q];
+        blockIdx = uint3{(unsigned)(b % c.grid.x), (unsigned)((b / c.grid.x) % c.grid.y),
+                         (unsigned)(b / ((long)c.grid.x * c.grid.y))};
+        memset(g_dyn.data(), 0xFF, g_dyn.size());
+        run_block(n);
+    }
     g_in_kernel = false;
     g_body = nullptr;
 }
