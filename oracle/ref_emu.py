@@ -13,7 +13,7 @@ threads of a block one after another between barriers, which gives those reducti
 result in the forward order; in reverse order (HSBEMU_ORDER=reverse, lane 31 first) every lane
 reads the finished values of the higher lanes, a superset of what it reads in lockstep, which
 gives the right result for the max reductions the replay uses (partialMaxAbs / partialMaxDiff)
-but not for sums.  Tests on this build therefore run in reverse order.
+but not for sums.  Tests on the emulated reference library therefore run in reverse order.
 
     python oracle/ref_emu.py
 """

@@ -8,7 +8,7 @@
 // copies, streams, events, graph capture and replay, function attributes) are served from
 // host memory in stream order.  The launch checks of the real runtime that the library's
 // host code could trip (block size, grid size, dynamic shared memory above a kernel's
-// attribute) are made here too.  The product never loads this build: hotspin_b200/_lib.py
+// attribute) are made here too.  The product never loads the emulated library: hotspin_b200/_lib.py
 // loads only the nvcc-built libhsb200.so; tests swap the emulated library in explicitly.
 #pragma once
 #include <math.h>
